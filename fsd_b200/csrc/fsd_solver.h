@@ -1,0 +1,26 @@
+// Solver-level declarations (solver.cu, precond.cu, brownian.cu, integrator.cu).
+#pragma once
+
+#include "fsd_internal.h"
+
+namespace fsd {
+
+constexpr int kMaxRestart = 100;
+constexpr int kPrunedCap = 32;  // pruned (r < rp) neighbours per particle, self included
+
+int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin);
+int precond_apply(fsd_handle* h, const float* b, float* x);
+int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, float tol, int* iters, float* resid);
+int gmres_alloc(fsd_handle* h);
+
+// precond.cu: G ~ (R_FU^pruned + relaxer D)^-1 on 6N vectors.
+int precond_alloc(fsd_handle* h);
+void precond_free(fsd_handle* h);
+int precond_build(fsd_handle* h, const float4* pos);
+int precond_G(fsd_handle* h, const float* t, float* y);
+
+// Host reverse Cuthill-McKee ordering of a symmetric graph in CSR form
+// (adjacency may include self loops).  perm[new] = old.
+void rcm_order(int n, const std::vector<int>& rowptr, const std::vector<int>& col, std::vector<int>& perm);
+
+}  // namespace fsd

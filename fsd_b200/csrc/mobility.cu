@@ -1,0 +1,907 @@
+// Far-field grand mobility by the Positively Split Ewald method
+// (Mobility.cu, Helper_Mobility.cu of the reference):
+//
+//   wave space:  spread F and couplet C to 11 real grids with Gaussians of
+//                support P^3, 3D FFT, scale by the Hasimoto/RPY Green's
+//                function, inverse FFT, contract back to particles;
+//   real space:  tabulated pair sum within ewald_cut plus the self term.
+//
+// B200 layout choices:
+//   * the 11 real grids are carried as 6 complex grids (two real grids per
+//     complex grid: F_x+iF_y, C_xx+iC_xy, C_xz+iC_yx, C_yy+iC_yz, C_zx+iC_zy,
+//     F_z), so forward and inverse transforms are 6 complex FFTs each instead
+//     of the reference's 11 + 11 (the grids are real before the forward
+//     transform and only real parts are read after the inverse one);
+//   * spreading is a per-tile gather over particles binned by stencil origin,
+//     so every grid node is written exactly once with a fixed summation order
+//     (no atomics, deterministic);
+//   * the FFT is a shared-memory mixed-radix Stockham transform along each
+//     axis over batches of lines; the whole 72^3 working set (18 MB) stays in
+//     the 126 MB L2.
+#include <algorithm>
+#include <cmath>
+
+#include "fsd_device.cuh"
+#include "fsd_kernels.cuh"
+
+namespace fsd {
+
+namespace {
+constexpr float kPiRef = 3.1415926536f;  // the reference's pi literal
+}
+
+// ------------------------------------------------------------------ FFT plan
+FFTPlan make_fft_plan(int n) {
+    FFTPlan p{};
+    p.n = n;
+    int m = n, k = 0;
+    const int radices[] = {8, 5, 4, 3, 2};
+    while (m > 1) {
+        bool found = false;
+        for (int r : radices) {
+            if (m % r == 0) {
+                p.radix[k++] = r;
+                m /= r;
+                found = true;
+                break;
+            }
+        }
+        if (!found) {
+            p.nst = -1;
+            return p;
+        }
+    }
+    p.nst = k;
+    return p;
+}
+
+// Twiddle tables w_n^m = exp(-2 pi i m / n), m in [0, n), for the three axes,
+// computed in double on the host.
+void fill_twiddles(fsd_handle* h) {
+    const int ns[3] = {h->g.Nx, h->g.Ny, h->g.Nz};
+    std::vector<float2> tw(ns[0] + ns[1] + ns[2]);
+    int off = 0;
+    for (int a = 0; a < 3; ++a) {
+        for (int m = 0; m < ns[a]; ++m) {
+            const double ang = -2.0 * M_PI * (double)m / (double)ns[a];
+            tw[off + m] = make_float2((float)cos(ang), (float)sin(ang));
+        }
+        off += ns[a];
+    }
+    cudaMemcpyAsync(h->w.twiddle, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice, h->stream);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+
+// Radix-p DFT of y[0..p) in place, w_p^1 = wp (forward convention handled by caller).
+template <int P>
+__device__ __forceinline__ void small_dft(float2* y, const float2* tw, int n, bool inv) {
+    float2 z[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        float2 acc = y[0];
+#pragma unroll
+        for (int s = 1; s < P; ++s) {
+            float2 w = tw[((j * s) % P) * (n / P)];
+            if (inv) w.y = -w.y;
+            acc.x += y[s].x * w.x - y[s].y * w.y;
+            acc.y += y[s].x * w.y + y[s].y * w.x;
+        }
+        z[j] = acc;
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) y[j] = z[j];
+}
+
+template <int P>
+__device__ __forceinline__ void stockham_stage(const float2* in, float2* out, int nlines, int n, int Ls,
+                                               const float2* tw, bool inv) {
+    const int L = Ls * P, r = n / L, nb = n / P;
+    for (int w = threadIdx.x; w < nlines * nb; w += blockDim.x) {
+        const int line = w / nb, bf = w - line * nb;
+        const int k = bf % r, j1 = bf / r;
+        const float2* X = in + line * n;
+        float2* Y = out + line * n;
+        float2 y[P];
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+            float2 v = X[k + s * r + r * P * j1];
+            if (s > 0 && j1 > 0) {
+                float2 w = tw[(j1 * s * r) % n];
+                if (inv) w.y = -w.y;
+                v = cmul(v, w);
+            }
+            y[s] = v;
+        }
+        small_dft<P>(y, tw, n, inv);
+#pragma unroll
+        for (int j2 = 0; j2 < P; ++j2) Y[k + r * (j1 + Ls * j2)] = y[j2];
+    }
+}
+
+// Transforms nlines lines of length n held in a (ping-pong with b); returns
+// the buffer holding the result.
+__device__ float2* fft_lines(float2* a, float2* b, int nlines, const FFTPlan& pl, const float2* tw, bool inv) {
+    float2* in = a;
+    float2* out = b;
+    int Ls = 1;
+    for (int q = 0; q < pl.nst; ++q) {
+        const int p = pl.radix[q];
+        switch (p) {
+            case 2: stockham_stage<2>(in, out, nlines, pl.n, Ls, tw, inv); break;
+            case 3: stockham_stage<3>(in, out, nlines, pl.n, Ls, tw, inv); break;
+            case 4: stockham_stage<4>(in, out, nlines, pl.n, Ls, tw, inv); break;
+            case 5: stockham_stage<5>(in, out, nlines, pl.n, Ls, tw, inv); break;
+            default: stockham_stage<8>(in, out, nlines, pl.n, Ls, tw, inv); break;
+        }
+        __syncthreads();
+        float2* t = in;
+        in = out;
+        out = t;
+        Ls *= p;
+    }
+    return in;
+}
+
+// One axis of the 3D transform for all 6 packed grids.  axis 2 (z): batches of
+// B contiguous lines; axes 1 (y) and 0 (x): lines grouped by B consecutive z.
+__global__ void k_fft_axis(float2* __restrict__ data, int Nx, int Ny, int Nz, int axis, int B, FFTPlan pl,
+                           const float2* __restrict__ tw_global, bool inv, int ngrids) {
+    extern __shared__ float2 smem[];
+    const int n = pl.n;
+    float2* tw = smem;
+    float2* a = smem + n;
+    float2* b = a + B * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_global[i];
+    const size_t G = (size_t)Nx * Ny * Nz;
+    size_t base;
+    int nl, es, ls;  // valid lines, element stride, line stride
+    if (axis == 2) {
+        const size_t lines_total = (size_t)ngrids * Nx * Ny;
+        const size_t l0 = (size_t)blockIdx.x * B;
+        nl = (int)min((size_t)B, lines_total - l0);
+        const size_t g = l0 / ((size_t)Nx * Ny);
+        const size_t xy = l0 % ((size_t)Nx * Ny);
+        base = g * G + xy * Nz;  // lines of one batch never straddle grids: (Nx*Ny) % B handled by host
+        es = 1;
+        ls = Nz;
+    } else {
+        const int nch = (Nz + B - 1) / B;
+        const int outer = (axis == 1) ? Nx : Ny;
+        int bid = blockIdx.x;
+        const int ch = bid % nch;
+        bid /= nch;
+        const int o = bid % outer;
+        const int g = bid / outer;
+        const int z0 = ch * B;
+        nl = min(B, Nz - z0);
+        es = (axis == 1) ? Nz : Ny * Nz;
+        base = (size_t)g * G + (axis == 1 ? (size_t)o * Ny * Nz : (size_t)o * Nz) + z0;
+        ls = 1;
+    }
+    const int tot = nl * n;
+    if (axis == 2) {
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+            const int line = i / n, t = i - line * n;
+            a[line * n + t] = data[base + (size_t)line * ls + t];
+        }
+    } else {
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+            const int t = i / nl, line = i - t * nl;
+            a[line * n + t] = data[base + (size_t)t * es + line];
+        }
+    }
+    __syncthreads();
+    float2* res = fft_lines(a, b, nl, pl, tw, inv);
+    if (axis == 2) {
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+            const int line = i / n, t = i - line * n;
+            data[base + (size_t)line * ls + t] = res[line * n + t];
+        }
+    } else {
+        for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+            const int t = i / nl, line = i - t * nl;
+            data[base + (size_t)t * es + line] = res[line * n + t];
+        }
+    }
+}
+
+static int fft_batch_z(int Nx, int Ny, int Nz) {
+    // Batches must not straddle two grids: pick B dividing Nx*Ny.
+    int B = std::max(1, 2048 / Nz);
+    while (B > 1 && (Nx * Ny) % B != 0) --B;
+    return B;
+}
+
+static void fft3d(fsd_handle* h, bool inv, int ngrids) {
+    const int Nx = h->g.Nx, Ny = h->g.Ny, Nz = h->g.Nz;
+    const FFTPlan px = make_fft_plan(Nx), py = make_fft_plan(Ny), pz = make_fft_plan(Nz);
+    const float2* twx = h->w.twiddle;
+    const float2* twy = twx + Nx;
+    const float2* twz = twy + Ny;
+    const int Bxy = 16;
+    const int Bz = fft_batch_z(Nx, Ny, Nz);
+    auto launch = [&](int axis) {
+        const FFTPlan& pl = axis == 0 ? px : (axis == 1 ? py : pz);
+        const float2* tw = axis == 0 ? twx : (axis == 1 ? twy : twz);
+        const int B = axis == 2 ? Bz : Bxy;
+        int nblocks;
+        if (axis == 2)
+            nblocks = (int)(((size_t)ngrids * Nx * Ny + B - 1) / B);
+        else
+            nblocks = ngrids * (axis == 1 ? Nx : Ny) * ((Nz + B - 1) / B);
+        const size_t shm = sizeof(float2) * ((size_t)pl.n + 2 * (size_t)B * pl.n);
+        k_fft_axis<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, Ny, Nz, axis, B, pl, tw, inv, ngrids);
+    };
+    if (!inv) {
+        launch(2);
+        launch(1);
+        launch(0);
+    } else {
+        launch(0);
+        launch(1);
+        launch(2);
+    }
+}
+
+// ------------------------------------------------------------- wave vectors
+// Wave vector and Green's scale per grid point (Mobility_SetGridk_kernel,
+// Helper_Mobility.cu:351-410), keeping its mixed float/double arithmetic.
+__global__ void k_gridk(float4* gridk, int Nx, int Ny, int Nz, Box b, float xi, float eta, double two_pi) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = Nx * Ny * Nz;
+    if (tid >= G) return;
+    const int i = tid / (Ny * Nz);
+    const int j = (tid - i * Ny * Nz) / Nz;
+    const int k = tid % Nz;
+    float4 v;
+    v.x = (float)((i < (Nx + 1) / 2) ? i : i - Nx);
+    v.y = ((float)((j < (Ny + 1) / 2) ? j : j - Ny) - b.xy * v.x * b.Ly / b.Lx) / b.Ly;
+    v.x = v.x / b.Lx;
+    v.z = (float)((k < (Nz + 1) / 2) ? k : k - Nz) / b.Lz;
+    v.x = (float)(v.x * two_pi);
+    v.y = (float)(v.y * two_pi);
+    v.z = (float)(v.z * two_pi);
+    const float k2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    const float xisq = xi * xi;
+    if (tid == 0) {
+        v.w = 0.0f;
+    } else {
+        const float e = (float)(-(1 - eta) * (double)k2 / 4.0 / (double)xisq);
+        v.w = (float)(6.0 * 3.1415926536 * (1.0 + (double)k2 / 4.0 / (double)xisq) * (double)expf(e) / (double)k2 /
+                      (double)G);
+    }
+    gridk[tid] = v;
+}
+
+void mobility_set_gridk(fsd_handle* h) {
+    const int G = h->g.Nx * h->g.Ny * h->g.Nz;
+    const double two_pi = h->p.kgrid_pi_ref ? 2.0 * 3.1416926536 : 2.0 * M_PI;
+    k_gridk<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz, h->box, h->p.xi, h->g.eta,
+                                                    two_pi);
+}
+
+// ---------------------------------------------------------------- Green step
+// Spectra order: X Y Z XX XY XZ YX YY YZ ZX ZY (force then couplet / velocity
+// then velocity gradient), as Mobility_WaveSpace_Green_kernel (Mobility.cu:315).
+// sgn = +1 applies the operator at wave vector tk; sgn = -1 applies the
+// operator with its imaginary-unit couplings conjugated (used to average with
+// the mirror point on Nyquist planes).
+__device__ __forceinline__ void green_apply(const float4 tk, const float2* f, float2* o, float sgn) {
+    const float2 fX = f[0], fY = f[1], fZ = f[2];
+    const float2 cXX = f[3], cXY = f[4], cXZ = f[5], cYX = f[6], cYY = f[7], cYZ = f[8], cZX = f[9], cZY = f[10];
+    const float2 cZZ = make_float2(-(cXX.x + cYY.x), -(cXX.y + cYY.y));
+    const float ksq = tk.x * tk.x + tk.y * tk.y + tk.z * tk.z;
+    const float k = sqrtf(ksq);
+    const float2 kdF = make_float2((tk.x * fX.x + tk.y * fY.x + tk.z * fZ.x) / ksq,
+                                   (tk.x * fX.y + tk.y * fY.y + tk.z * fZ.y) / ksq);
+    const float2 Cdkx = make_float2(cXX.x * tk.x + cXY.x * tk.y + cXZ.x * tk.z, cXX.y * tk.x + cXY.y * tk.y + cXZ.y * tk.z);
+    const float2 Cdky = make_float2(cYX.x * tk.x + cYY.x * tk.y + cYZ.x * tk.z, cYX.y * tk.x + cYY.y * tk.y + cYZ.y * tk.z);
+    const float2 Cdkz = make_float2(cZX.x * tk.x + cZY.x * tk.y + cZZ.x * tk.z, cZX.y * tk.x + cZY.y * tk.y + cZZ.y * tk.z);
+    const float2 kdcdk = make_float2((Cdkx.x * tk.x + Cdky.x * tk.y + Cdkz.x * tk.z) / ksq,
+                                     (Cdkx.y * tk.x + Cdky.y * tk.y + Cdkz.y * tk.z) / ksq);
+    const float sk = sinf(k), ck = cosf(k);
+    const float j0 = sk / k;
+    const float j1k = (sk - k * ck) / (ksq * k);
+    // UF: (I - kk) F, real scale.
+    const float Buf = tk.w * j0 * j0;
+    o[0] = make_float2((fX.x - tk.x * kdF.x) * Buf, (fX.y - tk.x * kdF.y) * Buf);
+    o[1] = make_float2((fY.x - tk.y * kdF.x) * Buf, (fY.y - tk.y * kdF.y) * Buf);
+    o[2] = make_float2((fZ.x - tk.z * kdF.x) * Buf, (fZ.y - tk.z * kdF.y) * Buf);
+    // UC: imaginary scale.
+    const float Buc = sgn * (float)((double)(-tk.w * j0) * (3.0 * (double)(sk - k * ck) / (double)(ksq * k)));
+    o[0].x += -(Cdkx.y - tk.x * kdcdk.y) * Buc;
+    o[1].x += -(Cdky.y - tk.y * kdcdk.y) * Buc;
+    o[2].x += -(Cdkz.y - tk.z * kdcdk.y) * Buc;
+    o[0].y += (Cdkx.x - tk.x * kdcdk.x) * Buc;
+    o[1].y += (Cdky.x - tk.y * kdcdk.x) * Buc;
+    o[2].y += (Cdkz.x - tk.z * kdcdk.x) * Buc;
+    // DF: imaginary scale, D_ab = i B (F_a k_b - k_a k_b k.F/k^2).
+    const float Bdf = sgn * (float)((double)(tk.w * j0) * (3.0 * (double)(sk - k * ck) / (double)(ksq * k)));
+    const float fa[3][2] = {{fX.x, fX.y}, {fY.x, fY.y}, {fZ.x, fZ.y}};
+    const float kv[3] = {tk.x, tk.y, tk.z};
+    const int ia[8] = {0, 0, 0, 1, 1, 1, 2, 2};
+    const int ib[8] = {0, 1, 2, 0, 1, 2, 0, 1};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float kk = kv[ia[c]] * kv[ib[c]];
+        const float Fkr = fa[ia[c]][0] * kv[ib[c]], Fki = fa[ia[c]][1] * kv[ib[c]];
+        o[3 + c] = make_float2(-(Fki - kk * kdF.y) * Bdf, (Fkr - kk * kdF.x) * Bdf);
+    }
+    // DC: real scale.
+    const float Bdc = (float)((double)tk.w * (-1.0) * (-9.0) * (double)j1k * (double)j1k);
+    const float2 Cdk[3] = {Cdkx, Cdky, Cdkz};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float kk = kv[ia[c]] * kv[ib[c]];
+        o[3 + c].x += (Cdk[ia[c]].x * kv[ib[c]] - kk * kdcdk.x) * Bdc;
+        o[3 + c].y += (Cdk[ia[c]].y * kv[ib[c]] - kk * kdcdk.y) * Bdc;
+    }
+}
+
+// Packed pair p holds spectra (pa[p], pb[p]).
+__constant__ int kPackA[6] = {0, 3, 5, 7, 9, 2};
+__constant__ int kPackB[6] = {1, 4, 6, 8, 10, -1};
+
+// One thread per mirror pair {k, -k}: unpack the 11 spectra of the real grids,
+// apply the Green's function (averaged with the mirror operator where the
+// mirror wave vector is not -k, i.e. on Nyquist planes, which reproduces the
+// real part the reference keeps after its complex inverse transform), repack.
+__global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gridk, int Nx, int Ny, int Nz) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int G = Nx * Ny * Nz;
+    if (idx >= G) return;
+    const int i = idx / (Ny * Nz), j = (idx / Nz) % Ny, l = idx % Nz;
+    const int im = (Nx - i) % Nx, jm = (Ny - j) % Ny, lm = (Nz - l) % Nz;
+    const int m = (im * Ny + jm) * Nz + lm;
+    if (m < idx) return;
+    float2 f[11], o[11];
+    float2 cm[6], ck[6];
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        ck[p] = grid[(size_t)p * G + idx];
+        cm[p] = grid[(size_t)p * G + m];
+    }
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        // A = (C(k) + conj C(m)) / 2 ; B = -i (C(k) - conj C(m)) / 2
+        const float2 A = make_float2(0.5f * (ck[p].x + cm[p].x), 0.5f * (ck[p].y - cm[p].y));
+        const float2 Bv = make_float2(0.5f * (ck[p].y + cm[p].y), -0.5f * (ck[p].x - cm[p].x));
+        f[kPackA[p]] = A;
+        if (kPackB[p] >= 0) f[kPackB[p]] = Bv;
+    }
+    if (idx == 0) {
+#pragma unroll
+        for (int p = 0; p < 6; ++p) grid[(size_t)p * G] = make_float2(0.f, 0.f);
+        return;
+    }
+    green_apply(gridk[idx], f, o, 1.0f);
+    const bool nyq = (2 * i == Nx) || (2 * j == Ny) || (2 * l == Nz);
+    if (nyq) {
+        float2 o2[11];
+        green_apply(gridk[m], f, o2, -1.0f);
+#pragma unroll
+        for (int c = 0; c < 11; ++c) o[c] = make_float2(0.5f * (o[c].x + o2[c].x), 0.5f * (o[c].y + o2[c].y));
+    }
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        const float2 A = o[kPackA[p]];
+        const float2 Bv = (kPackB[p] >= 0) ? o[kPackB[p]] : make_float2(0.f, 0.f);
+        // C_out(k) = A + i B ; C_out(m) = conj A + i conj B
+        grid[(size_t)p * G + idx] = make_float2(A.x - Bv.y, A.y + Bv.x);
+        if (m != idx) grid[(size_t)p * G + m] = make_float2(A.x + Bv.y, -A.y + Bv.x);
+    }
+}
+
+// ------------------------------------------------------ particle preparation
+// Split the generalized force and map torque + stresslet to the couplet
+// (Saddle_SplitGeneralizedF_kernel, Helper_Saddle.cu:108; Mobility_TS2C_kernel,
+// Helper_Mobility.cu:294-336, including its torque sign flip).
+__global__ void k_prep(const float* __restrict__ genF, int N, float4* f4, float4* c4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float* a = genF + 6 * i;
+    const float* s = genF + 6 * N + 5 * i;
+    f4[i] = make_float4(a[0], a[1], a[2], 0.0f);
+    const float Lx = -a[3], Ly = -a[4], Lz = -a[5];
+    const float Sxx = s[0], Sxy = s[1], Sxz = s[2], Syz = s[3], Syy = s[4];
+    c4[2 * i] = make_float4(Sxx, Sxy + 0.5f * Lz, Sxz - 0.5f * Ly, Syz + 0.5f * Lx);
+    c4[2 * i + 1] = make_float4(Syy, Sxy - 0.5f * Lz, Sxz + 0.5f * Ly, Syz - 0.5f * Lx);
+}
+
+// Stencil origin of each particle: the reference's first node
+// x + 0 - P/2 + 1 - (P%2)(frac < 0.5) (Mobility.cu:242-248), wrapped.
+__device__ __forceinline__ int3 stencil_origin(float4 p, const Box& b, int Nx, int Ny, int Nz, int P, float3* fr) {
+    float3 f = make_fraction(make_float3(p.x, p.y, p.z), b);
+    f.x *= (float)Nx;
+    f.y *= (float)Ny;
+    f.z *= (float)Nz;
+    const int x = (int)f.x, y = (int)f.y, z = (int)f.z;
+    const int Pd2 = P / 2;
+    int sx = x - Pd2 + 1 - (P % 2) * ((f.x - (float)x) < 0.5f);
+    int sy = y - Pd2 + 1 - (P % 2) * ((f.y - (float)y) < 0.5f);
+    int sz = z - Pd2 + 1 - (P % 2) * ((f.z - (float)z) < 0.5f);
+    if (fr) *fr = f;
+    sx = ((sx % Nx) + Nx) % Nx;
+    sy = ((sy % Ny) + Ny) % Ny;
+    sz = ((sz % Nz) + Nz) % Nz;
+    return make_int3(sx, sy, sz);
+}
+
+__global__ void k_origin_key(const float4* __restrict__ pos, int N, Box b, int Nx, int Ny, int Nz, int P, unsigned* key,
+                             int* origin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int3 s = stencil_origin(pos[i], b, Nx, Ny, Nz, P, nullptr);
+    key[i] = (unsigned)((s.x * Ny + s.y) * Nz + s.z);
+    origin[3 * i] = s.x;
+    origin[3 * i + 1] = s.y;
+    origin[3 * i + 2] = s.z;
+}
+
+int mobility_bin_particles(fsd_handle* h, const float4* pos) {
+    Workspace& w = h->w;
+    const int N = h->p.N, Nx = h->g.Nx, Ny = h->g.Ny, Nz = h->g.Nz;
+    k_origin_key<<<(N + 255) / 256, 256, 0, h->stream>>>(pos, N, h->box, Nx, Ny, Nz, h->g.P, w.part_origin_key,
+                                                        w.part_origin);
+    counting_sort(w.part_origin_key, N, Nx * Ny * Nz, w.bin_count, w.bin_start, w.bin_fill, w.bin_parts,
+                  w.scan_scratch, h->stream);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// --------------------------------------------------------------- spreading
+struct SpreadArgs {
+    const float4* pos;
+    const float4* f4;
+    const float4* c4;
+    const unsigned* bin_start;
+    const unsigned* bin_parts;
+    const int* origin;
+    float2* grid;
+    Box box;
+    int Nx, Ny, Nz, P;
+    int TX, TY, TZ;
+    float hx, hy, hz;
+    float prefac, expfac;
+};
+
+constexpr int kSpreadCap = 384;  // staged particles per pass
+
+struct StagedParticle {
+    float x, y, z;
+    int o;  // origin within the extended tile, packed (ox | oy << 10 | oz << 20)
+    float v[12];
+};
+
+__global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
+    __shared__ StagedParticle sp[kSpreadCap];
+    __shared__ unsigned scan_sh[32];
+    __shared__ unsigned s_total;
+    const int P = a.P;
+    const int ntx = (a.Nx + a.TX - 1) / a.TX, nty = (a.Ny + a.TY - 1) / a.TY;
+    int bid = blockIdx.x;
+    const int tx = bid % ntx;
+    bid /= ntx;
+    const int ty = bid % nty;
+    const int tz = bid / nty;
+    const int x0 = tx * a.TX, y0 = ty * a.TY, z0 = tz * a.TZ;
+    const int EX = a.TX + P - 1, EY = a.TY + P - 1, EZ = a.TZ + P - 1;
+    const int ex0 = x0 - (P - 1), ey0 = y0 - (P - 1), ez0 = z0 - (P - 1);
+    const int ncell = EX * EY * EZ;
+    const int nth = blockDim.x;
+    const int cpt = (ncell + nth - 1) / nth;  // extended cells per thread, contiguous
+    // Count staged particles per thread (deterministic order: cell order, then bin order).
+    unsigned mycount = 0;
+    for (int c = threadIdx.x * cpt; c < min(ncell, (threadIdx.x + 1) * cpt); ++c) {
+        const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
+        const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
+        const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
+        mycount += a.bin_start[bin + 1] - a.bin_start[bin];
+    }
+    // Block exclusive scan of counts.
+    unsigned x = mycount;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scan_sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned s = (lane < (nth >> 5)) ? scan_sh[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        scan_sh[lane] = s;
+        if (lane == 31) s_total = s;
+    }
+    __syncthreads();
+    const unsigned myoff = (wid ? scan_sh[wid - 1] : 0u) + x - mycount;
+    const unsigned total = s_total;
+
+    // This thread's node.
+    const int lz = threadIdx.x % a.TZ, ly = (threadIdx.x / a.TZ) % a.TY, lx = threadIdx.x / (a.TZ * a.TY);
+    const int nx = x0 + lx, ny = y0 + ly, nz = z0 + lz;
+    const bool active = (lx < a.TX) && nx < a.Nx && ny < a.Ny && nz < a.Nz;
+    const float Ld2x = a.box.Lx / 2.0f, Ld2y = a.box.Ly / 2.0f, Ld2z = a.box.Lz / 2.0f;
+    float3 pg;
+    pg.x = a.hx * nx - Ld2x;
+    pg.y = a.hy * ny - Ld2y;
+    pg.z = a.hz * nz - Ld2z;
+    pg.x = pg.x + a.box.xy * pg.y;
+    float acc[11];
+#pragma unroll
+    for (int c = 0; c < 11; ++c) acc[c] = 0.0f;
+
+    for (unsigned chunk = 0; chunk < total; chunk += kSpreadCap) {
+        // Stage this thread's particles that fall in [chunk, chunk + cap).
+        unsigned k = myoff;
+        for (int c = threadIdx.x * cpt; c < min(ncell, (threadIdx.x + 1) * cpt); ++c) {
+            const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
+            const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
+            const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
+            for (unsigned q = a.bin_start[bin]; q < a.bin_start[bin + 1]; ++q, ++k) {
+                if (k < chunk || k >= chunk + kSpreadCap) continue;
+                const unsigned p = a.bin_parts[q];
+                StagedParticle& s = sp[k - chunk];
+                const float4 ps = a.pos[p];
+                s.x = ps.x;
+                s.y = ps.y;
+                s.z = ps.z;
+                s.o = cx | (cy << 10) | (cz << 20);
+                const float4 f = a.f4[p], c0 = a.c4[2 * p], c1 = a.c4[2 * p + 1];
+                // pairs: (Fx,Fy) (Cxx,Cxy) (Cxz,Cyx) (Cyy,Cyz) (Czx,Czy) (Fz,0)
+                s.v[0] = f.x; s.v[1] = f.y; s.v[2] = c0.x; s.v[3] = c0.y; s.v[4] = c0.z; s.v[5] = c1.y;
+                s.v[6] = c1.x; s.v[7] = c0.w; s.v[8] = c1.z; s.v[9] = c1.w; s.v[10] = f.z; s.v[11] = 0.0f;
+            }
+        }
+        __syncthreads();
+        const int nst = (int)min((unsigned)kSpreadCap, total - chunk);
+        if (active) {
+            for (int q = 0; q < nst; ++q) {
+                const int o = sp[q].o;
+                const int dx = lx + P - 1 - (o & 1023), dy = ly + P - 1 - ((o >> 10) & 1023),
+                          dz = lz + P - 1 - (o >> 20);
+                if ((unsigned)dx < (unsigned)P && (unsigned)dy < (unsigned)P && (unsigned)dz < (unsigned)P) {
+                    const float3 r = min_image(make_float3(pg.x - sp[q].x, pg.y - sp[q].y, pg.z - sp[q].z), a.box);
+                    const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
+                    const float wgt = a.prefac * expf(-a.expfac * rsq);
+#pragma unroll
+                    for (int c = 0; c < 11; ++c) acc[c] += wgt * sp[q].v[c];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (active) {
+        const size_t G = (size_t)a.Nx * a.Ny * a.Nz;
+        const size_t g = ((size_t)nx * a.Ny + ny) * a.Nz + nz;
+        a.grid[g] = make_float2(acc[0], acc[1]);
+        a.grid[G + g] = make_float2(acc[2], acc[3]);
+        a.grid[2 * G + g] = make_float2(acc[4], acc[5]);
+        a.grid[3 * G + g] = make_float2(acc[6], acc[7]);
+        a.grid[4 * G + g] = make_float2(acc[8], acc[9]);
+        a.grid[5 * G + g] = make_float2(acc[10], 0.0f);
+    }
+}
+
+// ------------------------------------------------------------- contraction
+// One warp per particle: interpolate velocity (3) and velocity gradient (8)
+// from the P^3 stencil (Mobility_WaveSpace_ContractU / ContractD,
+// Mobility.cu:503-841).  Output per particle, 11 floats: u then the velocity
+// gradient in the reference's transposed storage
+// {XX, YX, ZX, ZY, YY, XY, XZ, YZ}.
+__global__ void __launch_bounds__(256) k_contract(const float4* __restrict__ pos, const float2* __restrict__ grid, int N,
+                                                  Box b, int Nx, int Ny, int Nz, int P, float hx, float hy, float hz,
+                                                  float prefac, float expfac, float* __restrict__ out) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    const float4 p = pos[i];
+    const int3 s = stencil_origin(p, b, Nx, Ny, Nz, P, nullptr);
+    const size_t G = (size_t)Nx * Ny * Nz;
+    const float Ld2x = b.Lx / 2.0f, Ld2y = b.Ly / 2.0f, Ld2z = b.Lz / 2.0f;
+    float acc[11];
+#pragma unroll
+    for (int c = 0; c < 11; ++c) acc[c] = 0.0f;
+    const int P3 = P * P * P;
+    for (int t = lane; t < P3; t += 32) {
+        const int tz = t % P, ty = (t / P) % P, tx = t / (P * P);
+        int ix = s.x + tx, iy = s.y + ty, iz = s.z + tz;
+        ix -= (ix >= Nx) ? Nx : 0;
+        iy -= (iy >= Ny) ? Ny : 0;
+        iz -= (iz >= Nz) ? Nz : 0;
+        float3 pg;
+        pg.x = hx * ix - Ld2x;
+        pg.y = hy * iy - Ld2y;
+        pg.z = hz * iz - Ld2z;
+        pg.x = pg.x + b.xy * pg.y;
+        const float3 r = min_image(make_float3(pg.x - p.x, pg.y - p.y, pg.z - p.z), b);
+        const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
+        const float wgt = prefac * expf(-expfac * rsq);
+        const size_t g = ((size_t)ix * Ny + iy) * Nz + iz;
+        const float2 q0 = __ldg(grid + g), q1 = __ldg(grid + G + g), q2 = __ldg(grid + 2 * G + g),
+                     q3 = __ldg(grid + 3 * G + g), q4 = __ldg(grid + 4 * G + g), q5 = __ldg(grid + 5 * G + g);
+        // q0=(Ux,Uy) q1=(XX,XY) q2=(XZ,YX) q3=(YY,YZ) q4=(ZX,ZY) q5=(Uz,-)
+        acc[0] += wgt * q0.x;
+        acc[1] += wgt * q0.y;
+        acc[2] += wgt * q5.x;
+        acc[3] += wgt * q1.x;  // XX
+        acc[4] += wgt * q2.y;  // YX
+        acc[5] += wgt * q4.x;  // ZX
+        acc[6] += wgt * q4.y;  // ZY
+        acc[7] += wgt * q3.x;  // YY
+        acc[8] += wgt * q1.y;  // XY
+        acc[9] += wgt * q2.x;  // XZ
+        acc[10] += wgt * q3.y; // YZ
+    }
+#pragma unroll
+    for (int c = 0; c < 11; ++c) acc[c] = group_sum<32>(acc[c]);
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < 11; ++c) out[11 * i + c] = acc[c];
+    }
+}
+
+// ------------------------------------------- real space, self and combine
+// Group of 8 lanes per particle: real-space Ewald pair sum with linear table
+// interpolation (Mobility_RealSpace_kernel, Mobility.cu:1046-1226), the self
+// term, the optional wave-space part, then velocity gradient -> (W, E)
+// (Mobility_D2WE_kernel) and generalized packing
+// (Saddle_MakeGeneralizedU_kernel).
+struct RealArgs {
+    const float4* pos;
+    const float4* f4;
+    const float4* c4;
+    const float* uwave;     // may be null
+    const unsigned* nneigh;
+    const unsigned* nlist;
+    int stride;
+    const float4* table;
+    float self_x, self_y;
+    float ewald_cut, ewald_dr;
+    int ewald_n;
+    Box box;
+    int N;
+    bool real;
+    const float* saddle_x;  // may be null: adds x[11N + 6i + c] to U_i
+    float* genU;
+};
+
+constexpr int kRealGroup = 8;
+
+__global__ void __launch_bounds__(128) k_real_combine(RealArgs a) {
+    const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kRealGroup;
+    const int gl = threadIdx.x % kRealGroup;
+    const int N = a.N;
+    const bool valid = gid < N;
+    const int i = valid ? gid : N - 1;
+    float u[3] = {0, 0, 0}, D[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (a.real) {
+        const float4 pi = a.pos[i];
+        const float mindistSq = a.ewald_dr * a.ewald_dr, maxdistSq = a.ewald_cut * a.ewald_cut;
+        const unsigned nn = valid ? a.nneigh[i] : 0u;
+        const unsigned* row = a.nlist + (size_t)i * a.stride;
+        for (unsigned q = gl; q < nn; q += kRealGroup) {
+            const unsigned j = row[q];
+            const float4 pj = a.pos[j];
+            const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), a.box);
+            const float distSqr = r.x * r.x + r.y * r.y + r.z * r.z;
+            if (!(distSqr < maxdistSq && distSqr >= mindistSq)) continue;
+            const float dist = sqrtf(distSqr);
+            const float4 Fj = a.f4[j];
+            const float4 C0 = a.c4[2 * j], C1 = a.c4[2 * j + 1];
+            const int r_ind = __float2int_rd(a.ewald_n * (dist - a.ewald_dr) / (a.ewald_cut - a.ewald_dr));
+            const float4 t1m = __ldg(a.table + 2 * r_ind), t2m = __ldg(a.table + 2 * r_ind + 1);
+            const float4 t1p = __ldg(a.table + 2 * r_ind + 2), t2p = __ldg(a.table + 2 * r_ind + 3);
+            const float fac = dist / a.ewald_dr - r_ind - 1.0f;
+            const float f1 = t1m.x + (t1p.x - t1m.x) * fac;
+            const float f2 = t1m.y + (t1p.y - t1m.y) * fac;
+            const float g1 = -(t1m.z + (t1p.z - t1m.z) * fac);
+            const float g2 = -(t1m.w + (t1p.w - t1m.w) * fac);
+            const float h1 = t2m.x + (t2p.x - t2m.x) * fac;
+            const float h2 = t2m.y + (t2p.y - t2m.y) * fac;
+            const float h3 = t2m.z + (t2p.z - t2m.z) * fac;
+            const float Rx = r.x / dist, Ry = r.y / dist, Rz = r.z / dist;
+            const float rdotf = Rx * Fj.x + Ry * Fj.y + Rz * Fj.z;
+            const float Czz = -(C0.x + C1.x);
+            // C.r and r.C with C = [[XX XY XZ][YX YY YZ][ZX ZY ZZ]] = [[c0x c0y c0z][c1y c1x c0w][c1z c1w Czz]]
+            const float Cr_x = C0.x * Rx + C0.y * Ry + C0.z * Rz;
+            const float Cr_y = C1.y * Rx + C1.x * Ry + C0.w * Rz;
+            const float Cr_z = C1.z * Rx + C1.w * Ry + Czz * Rz;
+            const float rC_x = C0.x * Rx + C1.y * Ry + C1.z * Rz;
+            const float rC_y = C0.y * Rx + C1.x * Ry + C1.w * Rz;
+            const float rC_z = C0.z * Rx + C0.w * Ry + Czz * Rz;
+            const float rCr = Rx * Cr_x + Ry * Cr_y + Rz * Cr_z;
+            u[0] += f1 * Fj.x + (f2 - f1) * rdotf * Rx;
+            u[1] += f1 * Fj.y + (f2 - f1) * rdotf * Ry;
+            u[2] += f1 * Fj.z + (f2 - f1) * rdotf * Rz;
+            u[0] += g1 * (Cr_x - rCr * Rx) + g2 * (rC_x - 4.f * rCr * Rx);
+            u[1] += g1 * (Cr_y - rCr * Ry) + g2 * (rC_y - 4.f * rCr * Ry);
+            u[2] += g1 * (Cr_z - rCr * Rz) + g2 * (rC_z - 4.f * rCr * Rz);
+            // Velocity gradient from force (Mobility.cu:1177-1184).
+            D[0] += -g1 * (Rx * Fj.x - rdotf * Rx * Rx) - g2 * (rdotf + Fj.x * Rx - 4.f * rdotf * Rx * Rx);
+            D[1] += -g1 * (Rx * Fj.y - rdotf * Rx * Ry) - g2 * (Fj.x * Ry - 4.f * rdotf * Rx * Ry);
+            D[2] += -g1 * (Rx * Fj.z - rdotf * Rx * Rz) - g2 * (Fj.x * Rz - 4.f * rdotf * Rx * Rz);
+            D[3] += -g1 * (Ry * Fj.z - rdotf * Ry * Rz) - g2 * (Fj.y * Rz - 4.f * rdotf * Ry * Rz);
+            D[4] += -g1 * (Ry * Fj.y - rdotf * Ry * Ry) - g2 * (rdotf + Fj.y * Ry - 4.f * rdotf * Ry * Ry);
+            D[5] += -g1 * (Ry * Fj.x - rdotf * Ry * Rx) - g2 * (Fj.y * Rx - 4.f * rdotf * Ry * Rx);
+            D[6] += -g1 * (Rz * Fj.x - rdotf * Rz * Rx) - g2 * (Fj.z * Rx - 4.f * rdotf * Rz * Rx);
+            D[7] += -g1 * (Rz * Fj.y - rdotf * Rz * Ry) - g2 * (Fj.z * Ry - 4.f * rdotf * Rz * Ry);
+            // Velocity gradient from couplet (Mobility.cu:1186-1193).
+            D[0] += h1 * (C0.x - 4.f * C0.x) + h2 * (Rx * Cr_x - rCr * Rx * Rx) +
+                    h3 * (rCr + Cr_x * Rx + Rx * rC_x + rC_x * Rx - 6.f * rCr * Rx * Rx - C0.x);
+            D[1] += h1 * (C0.y - 4.f * C1.y) + h2 * (Rx * Cr_y - rCr * Rx * Ry) +
+                    h3 * (Cr_x * Ry + Rx * rC_y + rC_x * Ry - 6.f * rCr * Rx * Ry - C1.y);
+            D[2] += h1 * (C0.z - 4.f * C1.z) + h2 * (Rx * Cr_z - rCr * Rx * Rz) +
+                    h3 * (Cr_x * Rz + Rx * rC_z + rC_x * Rz - 6.f * rCr * Rx * Rz - C1.z);
+            D[3] += h1 * (C0.w - 4.f * C1.w) + h2 * (Ry * Cr_z - rCr * Ry * Rz) +
+                    h3 * (Cr_y * Rz + Ry * rC_z + rC_y * Rz - 6.f * rCr * Ry * Rz - C1.w);
+            D[4] += h1 * (C1.x - 4.f * C1.x) + h2 * (Ry * Cr_y - rCr * Ry * Ry) +
+                    h3 * (rCr + Cr_y * Ry + Ry * rC_y + rC_y * Ry - 6.f * rCr * Ry * Ry - C1.x);
+            D[5] += h1 * (C1.y - 4.f * C0.y) + h2 * (Ry * Cr_x - rCr * Ry * Rx) +
+                    h3 * (Cr_y * Rx + Ry * rC_x + rC_y * Rx - 6.f * rCr * Ry * Rx - C0.y);
+            D[6] += h1 * (C1.z - 4.f * C0.z) + h2 * (Rz * Cr_x - rCr * Rz * Rx) +
+                    h3 * (Cr_z * Rx + Rz * rC_x + rC_z * Rx - 6.f * rCr * Rz * Rx - C0.z);
+            D[7] += h1 * (C1.w - 4.f * C0.w) + h2 * (Rz * Cr_y - rCr * Rz * Ry) +
+                    h3 * (Cr_z * Ry + Rz * rC_y + rC_z * Ry - 6.f * rCr * Rz * Ry - C0.w);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) u[c] = group_sum<kRealGroup>(u[c]);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) D[c] = group_sum<kRealGroup>(D[c]);
+    }
+    if (!valid || gl != 0) return;
+    if (a.real) {
+        const float4 F = a.f4[i], C0 = a.c4[2 * i], C1 = a.c4[2 * i + 1];
+        u[0] += a.self_x * F.x;
+        u[1] += a.self_x * F.y;
+        u[2] += a.self_x * F.z;
+        D[0] += a.self_y * (C0.x - 4.f * C0.x);
+        D[1] += a.self_y * (C0.y - 4.f * C1.y);
+        D[2] += a.self_y * (C0.z - 4.f * C1.z);
+        D[3] += a.self_y * (C0.w - 4.f * C1.w);
+        D[4] += a.self_y * (C1.x - 4.f * C1.x);
+        D[5] += a.self_y * (C1.y - 4.f * C0.y);
+        D[6] += a.self_y * (C1.z - 4.f * C0.z);
+        D[7] += a.self_y * (C1.w - 4.f * C0.w);
+    }
+    if (a.uwave) {
+        const float* w = a.uwave + 11 * i;
+        u[0] = w[0] + u[0];
+        u[1] = w[1] + u[1];
+        u[2] = w[2] + u[2];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) D[c] = w[3 + c] + D[c];
+    }
+    // D2WE (Helper_Mobility.cu:235-283): D0 = (Exx, Exy+Wz, Exz-Wy, Eyz+Wx), D1 = (Eyy, Exy-Wz, Exz+Wy, Eyz-Wx).
+    const float W0 = 0.5f * (D[3] - D[7]);
+    const float W1 = 0.5f * (D[6] - D[2]);
+    const float W2 = 0.5f * (D[1] - D[5]);
+    const float E0 = D[0];
+    const float E1 = 0.5f * (D[1] + D[5]);
+    const float E2 = 0.5f * (D[2] + D[6]);
+    const float E3 = 0.5f * (D[3] + D[7]);
+    const float E4 = D[4];
+    float* o = a.genU + 6 * i;
+    float add[6] = {0, 0, 0, 0, 0, 0};
+    if (a.saddle_x) {
+        const float* xs = a.saddle_x + 11 * N + 6 * i;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) add[c] = xs[c];
+    }
+    o[0] = u[0] + add[0];
+    o[1] = u[1] + add[1];
+    o[2] = u[2] + add[2];
+    o[3] = W0 + add[3];
+    o[4] = W1 + add[4];
+    o[5] = W2 + add[5];
+    float* e = a.genU + 6 * N + 5 * i;
+    e[0] = 2 * E0 + E4;
+    e[1] = 2 * E1;
+    e[2] = 2 * E2;
+    e[3] = 2 * E3;
+    e[4] = 2 * E4 + E0;
+}
+
+// ------------------------------------------------------------------ drivers
+static void spread(fsd_handle* h, const float4* pos) {
+    const GridParams& g = h->g;
+    SpreadArgs a;
+    a.pos = pos;
+    a.f4 = h->w.f4;
+    a.c4 = h->w.c4;
+    a.bin_start = h->w.bin_start;
+    a.bin_parts = h->w.bin_parts;
+    a.origin = h->w.part_origin;
+    a.grid = h->w.grid;
+    a.box = h->box;
+    a.Nx = g.Nx;
+    a.Ny = g.Ny;
+    a.Nz = g.Nz;
+    a.P = g.P;
+    a.TZ = std::min(8, g.Nz - g.P + 1);
+    a.TY = std::min(8, g.Ny - g.P + 1);
+    a.TX = std::min(4, g.Nx - g.P + 1);
+    a.hx = g.hx;
+    a.hy = g.hy;
+    a.hz = g.hz;
+    const float xisq = h->p.xi * h->p.xi;
+    a.prefac = (2.0 * xisq / kPiRef / g.eta) * sqrtf(2.0 * xisq / kPiRef / g.eta);
+    a.expfac = 2.0 * xisq / g.eta;
+    const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
+    k_spread<<<ntiles, a.TX * a.TY * a.TZ, 0, h->stream>>>(a);
+}
+
+static void contract(fsd_handle* h, const float4* pos) {
+    const GridParams& g = h->g;
+    const float xisq = h->p.xi * h->p.xi;
+    const float prefac = (2.0 * xisq / kPiRef / g.eta) * sqrtf(2.0 * xisq / kPiRef / g.eta);
+    const float expfac = 2.0 * xisq / g.eta;
+    const float quadW = g.hx * g.hy * g.hz;
+    const int N = h->p.N;
+    k_contract<<<(N * 32 + 255) / 256, 256, 0, h->stream>>>(pos, h->w.grid, N, h->box, g.Nx, g.Ny, g.Nz, g.P, g.hx,
+                                                            g.hy, g.hz, quadW * prefac, expfac, h->w.uwave);
+}
+
+void mobility_wave_from_spectrum(fsd_handle* h, const float4* pos) {
+    fft3d(h, true, 6);
+    contract(h, pos);
+}
+
+void mobility_combine(fsd_handle* h, const float4* pos, const float* genF, float* genU, bool wave, bool real,
+                      const float* saddle_x) {
+    (void)genF;
+    RealArgs r;
+    r.pos = pos;
+    r.f4 = h->w.f4;
+    r.c4 = h->w.c4;
+    r.uwave = wave ? h->w.uwave : nullptr;
+    r.nneigh = h->w.nneigh;
+    r.nlist = h->w.nlist;
+    r.stride = h->w.nl_stride;
+    r.table = h->d_ewald;
+    r.self_x = h->self_x;
+    r.self_y = h->self_y;
+    r.ewald_cut = h->ewald_cut;
+    r.ewald_dr = h->ewald_dr;
+    r.ewald_n = h->ewald_n;
+    r.box = h->box;
+    r.N = h->p.N;
+    r.real = real;
+    r.saddle_x = saddle_x;
+    r.genU = genU;
+    const int N = h->p.N;
+    k_real_combine<<<(N * kRealGroup + 127) / 128, 128, 0, h->stream>>>(r);
+}
+
+int mobility_apply(fsd_handle* h, const float4* pos, const float* genF, float* genU, int parts, const float* saddle_x,
+                   bool rebin) {
+    const int N = h->p.N;
+    k_prep<<<(N + 255) / 256, 256, 0, h->stream>>>(genF, N, h->w.f4, h->w.c4);
+    const bool wave = parts & 1, real = parts & 2;
+    if (wave) {
+        if (rebin) {
+            int st = mobility_bin_particles(h, pos);
+            if (st != FSD_OK) return st;
+        }
+        spread(h, pos);
+        fft3d(h, false, 6);
+        const int G = h->g.Nx * h->g.Ny * h->g.Nz;
+        k_green<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.grid, h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz);
+        fft3d(h, true, 6);
+        contract(h, pos);
+    }
+    mobility_combine(h, pos, genF, genU, wave, real, saddle_x);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+}  // namespace fsd

@@ -1,0 +1,240 @@
+// Neighbour list: every pair within r_list = ewald_cut + buffer, both
+// directions, no self.  Replaces HOOMD's NeighborListGPUBinned as configured by
+// PSEv3 (integrate.py:80-85: cell list, r_buff 0.4, rebuilt every step).
+//
+// Particles are binned into cells no narrower than r_list (measured between
+// opposite faces of the sheared box), each cell's members are sorted by index,
+// and each particle scans its 27 neighbouring cells in a fixed order, so row
+// contents and order are deterministic.  Boxes with fewer than three cells
+// along an axis fall back to an all-pairs scan.
+#include "fsd_device.cuh"
+#include "fsd_kernels.cuh"
+
+namespace fsd {
+
+// ---------------------------------------------------------------- scan utility
+// Exclusive scan of n unsigned values, out may alias in.  out[n] receives the
+// total.  Uses block-level scans plus one pass over the block sums.
+namespace {
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* sh, unsigned* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned s = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        sh[lane] = s;
+    }
+    __syncthreads();
+    const unsigned warp_off = wid ? sh[wid - 1] : 0u;
+    if (total) *total = sh[(blockDim.x >> 5) - 1];
+    return warp_off + x - v;
+}
+
+__global__ void scan_tiles(const unsigned* in, unsigned* out, unsigned* sums, int n) {
+    __shared__ unsigned sh[32];
+    const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    unsigned v[kScanItems], s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        v[i] = (base + i < n) ? in[base + i] : 0u;
+        s += v[i];
+    }
+    unsigned total;
+    unsigned off = block_exclusive_scan(s, sh, &total);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < n) out[base + i] = off;
+        off += v[i];
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void scan_sums(unsigned* sums, int nb, unsigned* out_total) {
+    __shared__ unsigned sh[32];
+    unsigned carry = 0;
+    for (int base = 0; base < nb; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const unsigned v = (i < nb) ? sums[i] : 0u;
+        unsigned total;
+        const unsigned ex = block_exclusive_scan(v, sh, &total);
+        if (i < nb) sums[i] = ex + carry;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out_total = carry;
+}
+
+__global__ void scan_add(unsigned* out, const unsigned* sums, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += sums[i / kScanTile];
+}
+}  // namespace
+
+size_t scan_scratch_elems(int n) { return (size_t)(n + kScanTile - 1) / kScanTile + 1; }
+
+void exclusive_scan(const unsigned* in, unsigned* out, int n, unsigned* scratch, cudaStream_t st) {
+    const int nb = (n + kScanTile - 1) / kScanTile;
+    scan_tiles<<<nb, kScanThreads, 0, st>>>(in, out, scratch, n);
+    scan_sums<<<1, kScanThreads, 0, st>>>(scratch, nb, out + n);
+    scan_add<<<(n + 255) / 256, 256, 0, st>>>(out, scratch, n);
+}
+
+// ----------------------------------------------------------- counting sort bins
+__global__ void k_bin_fill(const unsigned* key, int n, const unsigned* start, unsigned* fill, unsigned* items) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned c = key[i];
+    const unsigned slot = atomicAdd(&fill[c], 1u);
+    items[start[c] + slot] = i;
+}
+
+// Sort each bin's members by particle index (bins hold few members).
+__global__ void k_bin_sort(const unsigned* start, int nbins, unsigned* items) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nbins) return;
+    const unsigned b = start[c], e = start[c + 1];
+    for (unsigned i = b + 1; i < e; ++i) {
+        const unsigned key = items[i];
+        unsigned j = i;
+        while (j > b && items[j - 1] > key) {
+            items[j] = items[j - 1];
+            --j;
+        }
+        items[j] = key;
+    }
+}
+
+__global__ void k_bin_count(const unsigned* key, int n, unsigned* count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(&count[key[i]], 1u);
+}
+
+void counting_sort(const unsigned* key, int n, int nbins, unsigned* count, unsigned* start, unsigned* fill,
+                   unsigned* items, unsigned* scan_scratch, cudaStream_t st) {
+    cudaMemsetAsync(count, 0, sizeof(unsigned) * nbins, st);
+    cudaMemsetAsync(fill, 0, sizeof(unsigned) * nbins, st);
+    k_bin_count<<<(n + 255) / 256, 256, 0, st>>>(key, n, count);
+    exclusive_scan(count, start, nbins, scan_scratch, st);
+    k_bin_fill<<<(n + 255) / 256, 256, 0, st>>>(key, n, start, fill, items);
+    k_bin_sort<<<(nbins + 255) / 256, 256, 0, st>>>(start, nbins, items);
+}
+
+// ------------------------------------------------------------------ cell list
+__global__ void k_cell_key(const float4* pos, int n, Box b, int3 nc, unsigned* key) {
+    const int i = blockIdx.x * blockIdx.y * 0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const float3 f = make_fraction(make_float3(p.x, p.y, p.z), b);
+    int cx = (int)floorf(f.x * nc.x), cy = (int)floorf(f.y * nc.y), cz = (int)floorf(f.z * nc.z);
+    cx = ((cx % nc.x) + nc.x) % nc.x;
+    cy = ((cy % nc.y) + nc.y) % nc.y;
+    cz = ((cz % nc.z) + nc.z) % nc.z;
+    key[i] = (unsigned)((cx * nc.y + cy) * nc.z + cz);
+}
+
+__global__ void k_nlist_cells(const float4* __restrict__ pos, int n, Box b, int3 nc, const unsigned* __restrict__ key,
+                              const unsigned* __restrict__ cstart, const unsigned* __restrict__ cparts, float rlist2,
+                              unsigned* nneigh, unsigned* nlist, int stride, int* max_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 pi = pos[i];
+    const unsigned c = key[i];
+    const int cz = c % nc.z, cy = (c / nc.z) % nc.y, cx = c / (nc.z * nc.y);
+    unsigned cnt = 0;
+    unsigned* row = nlist + (size_t)i * stride;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int x = (cx + dx + nc.x) % nc.x;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int y = (cy + dy + nc.y) % nc.y;
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = (cz + dz + nc.z) % nc.z;
+                const unsigned cc = (unsigned)((x * nc.y + y) * nc.z + z);
+                for (unsigned k = cstart[cc]; k < cstart[cc + 1]; ++k) {
+                    const unsigned j = cparts[k];
+                    if (j == (unsigned)i) continue;
+                    const float4 pj = pos[j];
+                    const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
+                    if (r.x * r.x + r.y * r.y + r.z * r.z < rlist2) {
+                        if (cnt < (unsigned)stride) row[cnt] = j;
+                        ++cnt;
+                    }
+                }
+            }
+        }
+    }
+    nneigh[i] = cnt < (unsigned)stride ? cnt : (unsigned)stride;
+    atomicMax(max_count, (int)cnt);
+}
+
+__global__ void k_nlist_allpairs(const float4* __restrict__ pos, int n, Box b, float rlist2, unsigned* nneigh,
+                                 unsigned* nlist, int stride, int* max_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 pi = pos[i];
+    unsigned cnt = 0;
+    unsigned* row = nlist + (size_t)i * stride;
+    for (int j = 0; j < n; ++j) {
+        if (j == i) continue;
+        const float4 pj = pos[j];
+        const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
+        if (r.x * r.x + r.y * r.y + r.z * r.z < rlist2) {
+            if (cnt < (unsigned)stride) row[cnt] = j;
+            ++cnt;
+        }
+    }
+    nneigh[i] = cnt < (unsigned)stride ? cnt : (unsigned)stride;
+    atomicMax(max_count, (int)cnt);
+}
+
+// Cells per axis so that a cell is at least r_list wide between faces.
+int3 cell_dims(const Box& b, float rlist) {
+    const float wx = b.Lx / sqrtf(1.0f + b.xy * b.xy);
+    int3 nc;
+    nc.x = (int)floorf(wx / rlist);
+    nc.y = (int)floorf(b.Ly / rlist);
+    nc.z = (int)floorf(b.Lz / rlist);
+    return nc;
+}
+
+// Builds the list; returns the largest neighbour count in *max_count_host.
+int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host) {
+    Workspace& w = h->w;
+    const int n = h->p.N;
+    const float rlist = h->ewald_cut + h->p.nlist_buffer;
+    const float rlist2 = rlist * rlist;
+    const int3 nc = cell_dims(h->box, rlist);
+    cudaStream_t st = h->stream;
+    FSD_CHECK_CUDA(cudaMemsetAsync(w.nl_overflow, 0, sizeof(int), st));
+    if (nc.x >= 3 && nc.y >= 3 && nc.z >= 3 && (size_t)nc.x * nc.y * nc.z <= w.ncell_cap) {
+        const int ncells = nc.x * nc.y * nc.z;
+        k_cell_key<<<(n + 255) / 256, 256, 0, st>>>(pos, n, h->box, nc, w.part_cell);
+        counting_sort(w.part_cell, n, ncells, w.cell_count, w.cell_start, w.cell_fill, w.cell_parts, w.scan_scratch, st);
+        k_nlist_cells<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, nc, w.part_cell, w.cell_start, w.cell_parts,
+                                                       rlist2, w.nneigh, w.nlist, w.nl_stride, w.nl_overflow);
+    } else {
+        k_nlist_allpairs<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, rlist2, w.nneigh, w.nlist, w.nl_stride,
+                                                          w.nl_overflow);
+    }
+    FSD_CHECK_CUDA(cudaGetLastError());
+    FSD_CHECK_CUDA(cudaMemcpyAsync(w.host_flag, w.nl_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    *max_count_host = *w.host_flag;
+    return FSD_OK;
+}
+
+}  // namespace fsd

@@ -1,0 +1,357 @@
+// Saddle-point operator, its block preconditioner and restarted GMRES
+// (Saddle.cu, Solvers.cu, Wrappers.cuh of the reference).
+//
+// Unknown x = [F^ff (6N) | S^ff (5N) | U - U_inf (6N)];
+//   A x = [ M^ff x[0:11N] + (x[11N:17N]; 0) ;  x[0:6N] - R_FU x[11N:17N] ].
+// Preconditioner (Saddle.cu:171-264) with M ~ I and G ~ (R_FU^pruned + relaxer D)^-1:
+//   y = G (b[0:6N] - b[11N:17N]);  x = [ b[0:6N] - y ; b[6N:11N] ; y ].
+// GMRES(m) is right-preconditioned, so the Givens residual is the true residual
+// ||b - A x||; Arnoldi coefficients, Givens rotations and the least-squares
+// solve are FP64; basis vectors are FP32.  Orthogonalisation is classical
+// Gram-Schmidt with one re-orthogonalisation pass.  Everything stays on the
+// device; the host polls a converged flag every few iterations.
+#include <cmath>
+#include <cstddef>
+
+#include "fsd_device.cuh"
+#include "fsd_kernels.cuh"
+#include "fsd_solver.h"
+
+namespace fsd {
+
+int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin) {
+    const int N = h->p.N;
+    int st = mobility_apply(h, pos, x, b, 3, x, rebin);
+    if (st != FSD_OK) return st;
+    lub_rfu(h, pos, x + 11 * N, b + 11 * N, x);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+__global__ void k_pc_pre(const float* __restrict__ b, float* __restrict__ t, int N) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 6 * N) t[k] = b[k] - b[11 * N + k];
+}
+
+__global__ void k_pc_post(const float* __restrict__ b, const float* __restrict__ y, float* __restrict__ x, int N) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 6 * N) {
+        const float yk = y[k];
+        x[k] = b[k] - yk;
+        x[11 * N + k] = yk;
+    } else if (k < 11 * N) {
+        x[k] = b[k];
+    }
+}
+
+int precond_apply(fsd_handle* h, const float* b, float* x) {
+    const int N = h->p.N;
+    float* t = h->w.pc_t;
+    float* y = h->w.pc_y;
+    k_pc_pre<<<(6 * N + 255) / 256, 256, 0, h->stream>>>(b, t, N);
+    int st = precond_G(h, t, y);
+    if (st != FSD_OK) return st;
+    k_pc_post<<<(11 * N + 255) / 256, 256, 0, h->stream>>>(b, y, x, N);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// ------------------------------------------------------------- BLAS pieces
+constexpr int kRedBlocks = 296;  // two per SM
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum_d(double v, double* sh) {
+    v = group_sum_d<32>(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        s = group_sum_d<32>(s);
+    }
+    __syncthreads();
+    return s;
+}
+
+// part[i * nblocks + block] = sum over this block's slice of V_i . w, i < nv.
+__global__ void __launch_bounds__(kRedThreads) k_multidot(const float* __restrict__ V, size_t ld, int nv,
+                                                          const float* __restrict__ w, size_t n, double* part,
+                                                          const int* done) {
+    if (done && *done) return;
+    __shared__ double sh[32];
+    const size_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const size_t b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+    for (int i = 0; i < nv; ++i) {
+        const float* vi = V + (size_t)i * ld;
+        double s = 0.0;
+        for (size_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) s += (double)vi[k] * (double)w[k];
+        s = block_sum_d(s, sh);
+        if (threadIdx.x == 0) part[(size_t)i * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// out[i] (+)= sum_b part[i * nb + b], one warp per i.
+__global__ void k_finish_dots(const double* part, int nb, int nv, double* out, bool accumulate, const int* done) {
+    if (done && *done) return;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= nv) return;
+    double s = 0.0;
+    for (int b = lane; b < nb; b += 32) s += part[(size_t)i * nb + b];
+    s = group_sum_d<32>(s);
+    if (lane == 0) out[i] = accumulate ? out[i] + s : s;
+}
+
+// w -= sum_i c[i] V_i.
+__global__ void k_multiaxpy(const float* __restrict__ V, size_t ld, int nv, const double* __restrict__ c, float* w,
+                            size_t n, const int* done) {
+    if (done && *done) return;
+    __shared__ float cs[128];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cs[i] = (float)c[i];
+    __syncthreads();
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        float acc = w[k];
+        for (int i = 0; i < nv; ++i) acc -= cs[i] * V[(size_t)i * ld + k];
+        w[k] = acc;
+    }
+}
+
+// y = sum_i c[i] V_i.
+__global__ void k_combine(const float* __restrict__ V, size_t ld, int nv, const double* __restrict__ c,
+                          float* __restrict__ y, size_t n) {
+    __shared__ float cs[128];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cs[i] = (float)c[i];
+    __syncthreads();
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (int i = 0; i < nv; ++i) acc += cs[i] * V[(size_t)i * ld + k];
+        y[k] = acc;
+    }
+}
+
+__global__ void k_scale_copy(const float* __restrict__ src, float* __restrict__ dst, size_t n, const double* norm,
+                             const int* done) {
+    if (done && *done) return;
+    const double nv = *norm;
+    const float s = nv > 0.0 ? (float)(1.0 / sqrt(nv)) : 0.0f;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        dst[k] = src[k] * s;
+}
+
+__global__ void k_residual(const float* __restrict__ b, const float* __restrict__ Ax, float* __restrict__ r, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        r[k] = b[k] - Ax[k];
+}
+
+__global__ void k_axpy(float* __restrict__ x, const float* __restrict__ u, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        x[k] += u[k];
+}
+
+__global__ void k_add_dots(double* a, const double* b, int n, const int* done) {
+    if (done && *done) return;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] += b[i];
+}
+
+// --------------------------------------------------------- Arnoldi control
+// State (FP64) for one restart cycle.
+struct GmresState {
+    double H[kMaxRestart + 1][kMaxRestart];  // column-major by iteration: H[row][col]
+    double cs[kMaxRestart], sn[kMaxRestart];
+    double g[kMaxRestart + 1];
+    double y[kMaxRestart];
+    double bnorm2;     // ||b||^2
+    double beta2;      // ||r0||^2 at cycle start
+    double resid;      // current relative residual estimate
+    double tol;
+    int j;             // completed iterations this cycle
+    int total;         // total iterations
+    int done;          // converged or broke down this cycle
+    int breakdown;
+};
+
+// Start of a cycle: r0 norm is in dots[0].
+__global__ void k_cycle_start(GmresState* s, const double* dots, double tol, int first) {
+    const double beta2 = dots[0];
+    if (first) {
+        s->total = 0;
+        s->bnorm2 = dots[1];
+    }
+    s->tol = tol;
+    s->beta2 = beta2;
+    s->j = 0;
+    s->breakdown = 0;
+    for (int i = 0; i <= kMaxRestart; ++i) s->g[i] = 0.0;
+    s->g[0] = sqrt(beta2);
+    const double bn = s->bnorm2 > 0.0 ? sqrt(s->bnorm2) : 1.0;
+    s->resid = sqrt(beta2) / bn;
+    s->done = (s->resid <= tol || beta2 == 0.0 || !(beta2 == beta2)) ? 1 : 0;
+}
+
+// After orthogonalising column j: h[0..j] in hcol, ||w||^2 in hcol[j+1].
+__global__ void k_arnoldi_update(GmresState* s, const double* hcol, int m) {
+    if (s->done) return;
+    const int j = s->j;
+    for (int i = 0; i <= j; ++i) s->H[i][j] = hcol[i];
+    const double hn2 = hcol[j + 1];
+    double hj1 = sqrt(hn2 > 0.0 ? hn2 : 0.0);
+    s->H[j + 1][j] = hj1;
+    for (int i = 0; i < j; ++i) {
+        const double a = s->H[i][j], b = s->H[i + 1][j];
+        s->H[i][j] = s->cs[i] * a + s->sn[i] * b;
+        s->H[i + 1][j] = -s->sn[i] * a + s->cs[i] * b;
+    }
+    const double a = s->H[j][j], b = s->H[j + 1][j];
+    const double r = hypot(a, b);
+    const double c = r > 0.0 ? a / r : 1.0, sv = r > 0.0 ? b / r : 0.0;
+    s->cs[j] = c;
+    s->sn[j] = sv;
+    s->H[j][j] = r;
+    s->H[j + 1][j] = 0.0;
+    s->g[j + 1] = -sv * s->g[j];
+    s->g[j] = c * s->g[j];
+    s->j = j + 1;
+    s->total += 1;
+    const double bn = s->bnorm2 > 0.0 ? sqrt(s->bnorm2) : 1.0;
+    s->resid = fabs(s->g[j + 1]) / bn;
+    if (!(hj1 > 1e-300) || !(s->resid == s->resid)) s->breakdown = (hj1 > 1e-300) ? 2 : 1;
+    if (s->resid <= s->tol || s->j >= m || s->breakdown) s->done = 1;
+}
+
+// Least-squares solve H y = g (upper triangular, size j).
+__global__ void k_lsq(GmresState* s) {
+    const int j = s->j;
+    for (int i = j - 1; i >= 0; --i) {
+        double v = s->g[i];
+        for (int k = i + 1; k < j; ++k) v -= s->H[i][k] * s->y[k];
+        s->y[i] = (s->H[i][i] != 0.0) ? v / s->H[i][i] : 0.0;
+    }
+}
+
+struct GmresHost {
+    int j, total, done, breakdown;
+    double resid;
+};
+
+__global__ void k_export(const GmresState* s, GmresHost* o) {
+    o->j = s->j;
+    o->total = s->total;
+    o->done = s->done;
+    o->breakdown = s->breakdown;
+    o->resid = s->resid;
+}
+
+static const double* gs_y(const GmresState* s) {
+    return reinterpret_cast<const double*>(reinterpret_cast<const char*>(s) + offsetof(GmresState, y));
+}
+
+int gmres_alloc(fsd_handle* h) {
+    FSD_CHECK_CUDA(cudaMalloc(&h->w.gmres_state, sizeof(GmresState)));
+    FSD_CHECK_CUDA(cudaMallocHost(&h->w.gmres_host, sizeof(GmresHost)));
+    return FSD_OK;
+}
+
+// Solve A x = b; x holds the initial guess.  Returns FSD_OK or
+// FSD_ERR_GMRES_MAXIT / FSD_ERR_BREAKDOWN; iterations and the final true
+// relative residual in *iters / *resid.
+int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, float tol, int* iters, float* resid) {
+    Workspace& w = h->w;
+    const int N = h->p.N;
+    const size_t n = (size_t)17 * N;
+    const int m = std::min(h->p.gmres_restart, kMaxRestart);
+    const int maxit = h->p.gmres_max_iter;
+    cudaStream_t st = h->stream;
+    GmresState* gs = (GmresState*)w.gmres_state;
+    GmresHost* gh = (GmresHost*)w.gmres_host;
+    const size_t ld = n;
+    float* V = w.V;
+    float* r = w.sx;   // residual / work
+    float* Ax = w.sy;  // operator output
+    float* z = w.sz;   // preconditioned vector
+    double* part = w.dred;
+    double* dots = w.hcol;  // [0..m+1]
+    const int nbl = kRedBlocks;
+    const int vthreads = 256, vblocks = 4 * 148;
+    int total = 0;
+    bool first = true;
+    int status = FSD_OK;
+    // ||b||^2 into dots[1] (first cycle only).
+    for (;;) {
+        // r = b - A x
+        int e = saddle_multiply(h, pos, x, Ax, first);
+        if (e != FSD_OK) return e;
+        k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
+        k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
+        k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
+        if (first) {
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(b, n, 1, b, n, part, nullptr);
+            k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + 1, false, nullptr);
+        }
+        k_cycle_start<<<1, 1, 0, st>>>(gs, dots, (double)tol, first ? 1 : 0);
+        k_scale_copy<<<vblocks, vthreads, 0, st>>>(r, V, n, dots, &gs->done);
+        first = false;
+        for (int j = 0; j < m; ++j) {
+            // w = A M^-1 V_j
+            e = precond_apply(h, V + (size_t)j * ld, z);
+            if (e != FSD_OK) return e;
+            e = saddle_multiply(h, pos, z, Ax, false);
+            if (e != FSD_OK) return e;
+            // CGS2 against V_0..V_j.
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+            k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, dots, false, &gs->done);
+            k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, dots, Ax, n, &gs->done);
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+            k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, w.hcol2, false, &gs->done);
+            k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, w.hcol2, Ax, n, &gs->done);
+            k_add_dots<<<1, 128, 0, st>>>(dots, w.hcol2, j + 1, &gs->done);
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(Ax, n, 1, Ax, n, part, &gs->done);
+            k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + j + 1, false, &gs->done);
+            k_arnoldi_update<<<1, 1, 0, st>>>(gs, dots, m);
+            k_scale_copy<<<vblocks, vthreads, 0, st>>>(Ax, V + (size_t)(j + 1) * ld, n, dots + j + 1, &gs->done);
+            if ((j % 4) == 3 || j == m - 1) {
+                k_export<<<1, 1, 0, st>>>(gs, gh);
+                FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+                if (gh->done) break;
+            }
+        }
+        k_export<<<1, 1, 0, st>>>(gs, gh);
+        FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+        const int jc = gh->j;
+        total = gh->total;
+        if (jc > 0) {
+            k_lsq<<<1, 1, 0, st>>>(gs);
+            k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
+            e = precond_apply(h, Ax, z);
+            if (e != FSD_OK) return e;
+            k_axpy<<<vblocks, vthreads, 0, st>>>(x, z, n);
+        }
+        if (gh->breakdown == 1) {
+            status = FSD_ERR_BREAKDOWN;
+            break;
+        }
+        if (gh->resid <= tol && jc < m) break;  // converged inside the cycle; confirm below
+        if (gh->resid <= tol) break;
+        if (total >= maxit) {
+            status = FSD_ERR_GMRES_MAXIT;
+            break;
+        }
+    }
+    // True residual of the returned solution.
+    int e = saddle_multiply(h, pos, x, Ax, false);
+    if (e != FSD_OK) return e;
+    k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
+    k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
+    k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
+    double host[2];
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host, dots, sizeof(double), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host + 1, &gs->bnorm2, sizeof(double), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    const double rel = host[1] > 0 ? sqrt(host[0] / host[1]) : sqrt(host[0]);
+    if (iters) *iters = total;
+    if (resid) *resid = (float)rel;
+    if (!(rel == rel)) status = FSD_ERR_BREAKDOWN;
+    return status;
+}
+
+}  // namespace fsd

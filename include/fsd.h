@@ -1,0 +1,201 @@
+/*
+ * fsd.h -- C ABI of the B200 Fast Stokesian Dynamics velocity path.
+ *
+ * A drop-in for the deterministic + Brownian velocity path of the PSEv3
+ * HOOMD-blue plugin (GeZhouyang/FSD).  Every entry point takes plain device
+ * pointers and sizes; no C++ or torch types cross this boundary.  Pointers
+ * named d_* are device pointers and are borrowed: the caller owns them.  All
+ * work is enqueued on the stream given to fsd_create (or fsd_set_stream);
+ * entry points that report a solver outcome synchronise that stream.
+ *
+ * Data layouts follow the reference exactly (DataStruct.h, Stokes.h:189-190):
+ *   positions      float4 x N   (x, y, z, unused), box centred on the origin
+ *   orientations   float3 x N
+ *   images         int3   x N
+ *   generalized force  (11N): [F_i, L_i] (6 per particle) then S_i (5 per particle)
+ *   generalized velocity (11N): [U_i, W_i] then E_i, same ordering
+ *   stresslet / strain order: (xx-zz, 2xy, 2xz, 2yz, yy-zz) for strain,
+ *                             (Sxx, Sxy, Sxz, Syz, Syy) for stresslets
+ *   saddle vectors (17N): [F^ff (6N) | S^ff (5N) | U - U_inf (6N)]
+ *
+ * Errors: every function returns an fsd_status.  Nothing calls exit().
+ * Threading: a handle is not re-entrant; use one handle per host thread.
+ */
+#ifndef FSD_H
+#define FSD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fsd_handle fsd_handle;
+
+enum fsd_status {
+    FSD_OK = 0,
+    FSD_ERR_BAD_PARAMS = 1,     /* parameters the reference rejects with exit() (Stokes.cc:140-261) */
+    FSD_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    FSD_ERR_GMRES_MAXIT = 3,    /* GMRES hit its iteration limit (Solvers.cu:121) */
+    FSD_ERR_LANCZOS_MAXIT = 4,  /* Lanczos did not reach its tolerance (Brownian_FarField.cu:787) */
+    FSD_ERR_ICHOL = 5,          /* incomplete Cholesky failed even after relaxation (Precondition.cu:1246) */
+    FSD_ERR_NLIST_OVERFLOW = 6, /* more neighbours than the list capacity even after growing it */
+    FSD_ERR_DEVICE_WAIT = 7,    /* a bounded device-side wait ran out */
+    FSD_ERR_ALLOC = 8,          /* device allocation failed */
+    FSD_ERR_BREAKDOWN = 9       /* Krylov breakdown or a non-finite value */
+};
+
+enum fsd_precond_kind {
+    FSD_PRECOND_NONE = 0,    /* identity (Saddle.cu:258 debug path) */
+    FSD_PRECOND_ICHOL = 1,   /* block preconditioner with RCM + IC(0) of pruned R_FU (Saddle.cu:171) */
+    FSD_PRECOND_LEARNED = 2  /* learned block-sparse approximate inverse of the same block */
+};
+
+enum fsd_force_mode {
+    FSD_FORCE_INTERPARTICLE = 0, /* overwrite applied force with the built-in pair force (Helper_Stokes.cu:65) */
+    FSD_FORCE_USER = 1           /* keep the caller's applied force/torque untouched */
+};
+
+/* Integrator parameters.  Defaults (fsd_default_params) are the reference
+ * defaults of PSEv3.__init__ (integrate.py:40-55). */
+typedef struct fsd_params {
+    int N;                       /* number of particles (radius a = 1) */
+    float Lx, Ly, Lz, xy;        /* box edges and xy tilt */
+    float xi;                    /* Ewald splitting parameter (0.5) */
+    float error;                 /* Ewald / spreading accuracy (1e-3) */
+    float max_strain;            /* maximum box strain, widens the Gaussian support (0.5) */
+    float solver_tol;            /* GMRES relative residual; the reference uses `error` (Stokes.cc:1449) */
+    float lanczos_tol;           /* Lanczos relative change; the reference uses `error` */
+    float rfd_epsilon;           /* random finite difference step; the reference uses `error` (Stokes.cc:125) */
+    float T;                     /* temperature kT */
+    float dt;                    /* time step */
+    uint32_t seed;               /* random seed (hashed as Stokes.cc:74) */
+    float ndsr, kappa, k_n, beta_AF, epsq;  /* pair force (integrate.py:54) */
+    float T_ext, omega_ext;      /* external torque amplitude and frequency */
+    float sqm_B1, sqm_B2;        /* squirmer modes */
+    int N_mix;                   /* particles with tag < N_mix keep the unmasked modes */
+    float coef_B1_mask, coef_B2_mask;
+    float rot_diff;              /* rotational diffusivity of the director noise */
+    int period;                  /* stresslet output period (0 = never) */
+    int gmres_restart;           /* 50 (Solvers.cu:105) */
+    int gmres_max_iter;          /* 1000 (Solvers.cu:117) */
+    int lanczos_max;             /* 100 (Brownian_FarField.cu:618) */
+    int precond;                 /* fsd_precond_kind */
+    int force_mode;              /* fsd_force_mode */
+    int kgrid_pi_ref;            /* 1: wave vectors scaled by 2*3.1416926536 as Helper_Mobility.cu:389; 0: 2*pi */
+    float rlub;                  /* lubrication cutoff (4.0, Stokes.cc:1505) */
+    float rp;                    /* preconditioner cutoff (2.1, Stokes.cc:1506) */
+    float nlist_buffer;          /* neighbour-list skin added to the Ewald cutoff (0.4, integrate.py:83) */
+} fsd_params;
+
+/* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
+typedef struct fsd_pse_info {
+    int Nx, Ny, Nz, P;
+    float ewald_cut, gauss_m, eta, hx, hy, hz;
+    float self_x, self_y;
+    int ewald_n;
+    float ewald_dr;
+} fsd_pse_info;
+
+/* Outcome of the last solve or step. */
+typedef struct fsd_solve_info {
+    int gmres_iters[3];          /* RFD forward, RFD backward, main solve */
+    float gmres_resid[3];        /* final relative residual ||b - Ax|| / ||b|| */
+    int lanczos_ff_iters, lanczos_nf_iters;
+    float lanczos_ff_err, lanczos_nf_err;
+    int ichol_attempts;          /* factorisations tried (relaxer doubled after each failure) */
+    float ichol_relaxer;         /* relaxer the factorisation succeeded with */
+    int nlist_max;               /* largest neighbour count seen */
+    int status;                  /* fsd_status of that call */
+} fsd_solve_info;
+
+/* Arguments of one time step (Stokes_StepOne, Stokes.cuh:81-108). */
+typedef struct fsd_step_args {
+    unsigned int timestep;
+    float shear_rate;            /* current shear rate (ShearFunction::getShearRate) */
+    float* d_pos;                /* float4 x N, in/out */
+    float* d_ori;                /* float3 x N, in/out */
+    float* d_pos_gb;             /* float4 x N, unwrapped positions, in/out (may be NULL) */
+    int* d_image;                /* int3 x N, in/out */
+    float* d_force;              /* 6N applied force/torque; written when force_mode = INTERPARTICLE */
+    float* d_velocity;           /* 11N out: [U, W] (6N) then stresslet (5N, on output steps) */
+    const float* d_noise_ang;    /* float3 x N angular noise, or NULL for none */
+    const float* d_b1_mask;      /* N floats, or NULL for all ones */
+    const float* d_b2_mask;      /* N floats, or NULL for all ones */
+} fsd_step_args;
+
+void fsd_default_params(fsd_params* p);
+const char* fsd_status_string(int status);
+
+/* Host-only part of Stokes::setParams (Stokes.cc:118-696): grid, support,
+ * splitting and the real-space Ewald table (2*(ewald_n+1) float4, written to
+ * host_table when it is non-NULL and n_floats is large enough).  Touches no
+ * GPU. */
+int fsd_pse_setup(const fsd_params* p, fsd_pse_info* info, float* host_table, size_t n_floats);
+
+/* Stokes constructor + setParams + setResistanceTable + setSparseMath +
+ * AllocateWorkSpaces (Stokes.cc:47-83, 118-696, 937-1063;
+ * Stokes_ResistanceTable.cc:33; Stokes_SparseMath.cc:15).  All device memory
+ * the path needs is allocated here; nothing is allocated per step. */
+int fsd_create(const fsd_params* p, void* cuda_stream, fsd_handle** out);
+/* Stokes destructor (Stokes.cc:86-113). */
+void fsd_destroy(fsd_handle* h);
+int fsd_set_stream(fsd_handle* h, void* cuda_stream);
+/* Box update (HOOMD box_resize with shear_variant, variant.py:14-32). */
+int fsd_set_box(fsd_handle* h, float Lx, float Ly, float Lz, float xy);
+/* Stokes::setT / temperature variant value for the next step. */
+int fsd_set_temperature(fsd_handle* h, float T);
+int fsd_get_pse_info(const fsd_handle* h, fsd_pse_info* info);
+int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info);
+/* Copy the real-space Ewald table (2*(ewald_n+1) float4) to host memory. */
+int fsd_get_ewald_table(const fsd_handle* h, float* host_table, size_t n_floats);
+
+/* Full neighbour list within ewald_cut + buffer (replaces HOOMD
+ * NeighborListGPUBinned, integrate.py:80-85, computed at Stokes.cc:1216).
+ * Must precede the pair entry points below for the same positions. */
+int fsd_build_neighbor_list(fsd_handle* h, const float* d_pos);
+/* Copy the list to host: counts (N), and row entries (N x stride). */
+int fsd_get_neighbor_list(const fsd_handle* h, unsigned int* host_nneigh, unsigned int* host_nlist,
+                          size_t cap, int* stride);
+
+/* Generalized far-field mobility U = M^ff F on 11N vectors
+ * (Mobility_GeneralizedMobility, Mobility.cu:1488).  parts: 1 = wave space
+ * only, 2 = real space + self only, 3 = both (the reference). */
+int fsd_mobility(fsd_handle* h, const float* d_pos, const float* d_genF, float* d_genU, int parts);
+
+/* Lubrication pair products over the neighbour list (Lubrication.cu). */
+int fsd_lub_rfu(fsd_handle* h, const float* d_pos, const float* d_U6, float* d_F6);          /* F = R_FU U (:69) */
+int fsd_lub_rfe(fsd_handle* h, const float* d_pos, float shear_rate, const float* d_ori,
+                const float* d_b2_mask, float B2, float* d_F6);                               /* F += R_FE:E (:350) */
+int fsd_lub_rsu(fsd_handle* h, const float* d_pos, const float* d_U6, float* d_S5);          /* S -= R_SU U (:650) */
+int fsd_lub_rse(fsd_handle* h, const float* d_pos, float shear_rate, const float* d_ori,
+                const float* d_b2_mask, float B2, float* d_S5);                               /* S += R_SE:E (:953) */
+
+/* Saddle-point operator b = A x on 17N vectors (Saddle_Multiply, Saddle.cu:80). */
+int fsd_saddle_multiply(fsd_handle* h, const float* d_pos, const float* d_x, float* d_b);
+/* Build the near-field preconditioner for these positions (Precondition_Wrap, Precondition.cu:1326). */
+int fsd_precond_build(fsd_handle* h, const float* d_pos);
+/* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */
+int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x);
+/* Preconditioned GMRES on the saddle system (Solvers_Saddle, Solvers.cu:55).
+ * d_x holds the initial guess on entry and the solution on exit. */
+int fsd_saddle_solve(fsd_handle* h, const float* d_pos, const float* d_rhs, float* d_x, int* iters, float* resid);
+
+/* Brownian pieces (Brownian_FarField.cu:829, Brownian_NearField.cu:407,
+ * Integrator.cu:549).  Outputs are velocities/forces already scaled by
+ * sqrt(2 kT / dt); draws are counter-based from (seed, timestep, stream id). */
+int fsd_brownian_farfield(fsd_handle* h, const float* d_pos, unsigned int timestep, float* d_slip11);
+int fsd_brownian_nearfield(fsd_handle* h, const float* d_pos, unsigned int timestep, float* d_force6);
+int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigned int timestep, float* d_drift6);
+
+/* Velocities and stresslets for the current configuration without moving
+ * particles (Integrator_ComputeVelocity, Integrator.cu:744). */
+int fsd_compute_velocity(fsd_handle* h, const fsd_step_args* a);
+/* One full time step (Stokes_StepOne, Stokes.cu:119). */
+int fsd_step(fsd_handle* h, const fsd_step_args* a);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSD_H */
