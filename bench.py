@@ -1,0 +1,344 @@
+"""Benchmark: full FSD time steps per second at N=32768, phi=0.4.
+
+Workload (one "step"): neighbour list, IC(0) preconditioner build, pair
+forces, far-field Brownian slip (wave-space noise + Lanczos on the real-space
+mobility), near-field Brownian force (Lanczos on R_FU), random finite
+difference drift (two saddle solves), main saddle solve to relative residual
+1e-4 (GMRES, warm-started), Euler update with simple shear 1.0.  kT = 1,
+dt = 1e-4, Ewald accuracy 1e-3 (xi 0.5, 72^3 grid, P = 6).  Positions from
+seeded random sequential addition followed by overlap relaxation.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fsd|reference]
+
+Under torchrun each rank steps its own independent suspension (the path does
+not shard within one suspension; replicas only).  Prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FSD steps/sec at N=32768 φ=0.4, learned-precond vs IChol at 1e-4 residual"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fsd", choices=["fsd", "reference"])
+    ap.add_argument("--N", type=int, default=32768)
+    ap.add_argument("--phi", type=float, default=0.4)
+    ap.add_argument("--precond", default="ichol", choices=["ichol", "none", "learned"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = [l.split(",") for l in Path(self.out.name).read_text().splitlines() if l.strip()]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def peak_hbm():
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def region_bytes(name, N, G, nnzb, pairs_real, pairs_lub, launches_per_call):
+    """Algorithmic DRAM bytes of one launch of the region's kernel."""
+    if name == "precond_apply":
+        # forward or backward block solve: factor blocks (6x6 fp32) + column ids once,
+        # the 6N right-hand side and result
+        return nnzb * (36 * 4 + 4) / 1 + 6 * N * 4 * 3
+    if name == "fft":
+        return 2 * 6 * G * 8  # one axis pass over the 6 packed complex grids, read + write
+    if name == "spread":
+        return N * (16 + 48) + 6 * G * 8
+    if name == "contract":
+        return 6 * G * 8 + N * (16 + 44)
+    if name == "green":
+        return 2 * 6 * G * 8 + G * 16
+    if name == "real_space":
+        return N * (16 + 16 + 32) + 4 * pairs_real + N * 44
+    if name == "rfu":
+        return N * (16 + 24 + 24) + 4 * pairs_lub
+    return None
+
+
+def run_fsd(args, ws, rank, local):
+    import torch
+
+    from fsd_b200 import _lib
+    from fsd_b200.configs import suspension
+    from fsd_b200.core import FSD
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    N, phi = args.N, args.phi
+    pos, L = suspension(N, phi, seed=1 + rank)
+    s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=1 + rank, error=1e-3, solver_tol=1e-4,
+            lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=args.precond, period=0, gmres_max_iter=1000)
+    info = s.pse_info()
+    shear_rate = 1.0
+    p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
+    ori = torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev).contiguous()
+    img = torch.zeros(3 * N, dtype=torch.int32, device=dev)
+    F = torch.zeros(6 * N, device=dev)
+    V = torch.zeros(11 * N, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    step_no = [0]
+
+    def one_step():
+        st = s.step(step_no[0], shear_rate, p, ori, img, F, V, raise_on_error=False)
+        step_no[0] += 1
+        if st not in (0, 4):  # Lanczos not converged (4) is reported, not fatal, as in the reference
+            raise RuntimeError(f"fsd_step status {st}")
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    lib = _lib.lib()
+    # --- device-timed region: K steps, L2 flushed before each step (outside its events)
+    iters = []
+    launch0 = lib.fsd_launch_count()
+    check_prof = lib.fsd_profile_enable(s._h, 1)
+    ms_regions = np.zeros(len(_lib.REGIONS))
+    cnt_regions = np.zeros(len(_lib.REGIONS), np.int64)
+    lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
+                         len(_lib.REGIONS), 1)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            one_step()
+            evs[k][1].record(stream)
+            si = s.solve_info()
+            iters.append(si["gmres_iters"] + [si["lanczos_ff_iters"], si["lanczos_nf_iters"]])
+        torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    launches = lib.fsd_launch_count() - launch0
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(sum(step_ms))
+    lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
+                         len(_lib.REGIONS), 1)
+    lib.fsd_profile_enable(s._h, 0)
+    if ws > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * args.steps / (total_ms / 1e3)
+    # --- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda t: t.detach().cpu().pin_memory()
+        h_pos, h_ori, h_img = pin(p), pin(ori), pin(img)
+        h_V, h_P = torch.empty(11 * N).pin_memory(), torch.empty(4 * N).pin_memory()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for k in range(args.steps):
+            p.copy_(h_pos, non_blocking=True)
+            ori.copy_(h_ori, non_blocking=True)
+            img.copy_(h_img, non_blocking=True)
+            one_step()
+            h_V.copy_(V, non_blocking=True)
+            h_P.copy_(p, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([e2e_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": "steps/s",
+               "h2d_bytes_per_step": int(h_pos.numel() * 4 + h_ori.numel() * 4 + h_img.numel() * 4),
+               "d2h_bytes_per_step": int(h_V.numel() * 4 + h_P.numel() * 4)}
+    # --- roofline of the dominant kernel (largest device time among the timed kernels)
+    regions = {n: {"ms": float(ms_regions[i]), "calls": int(cnt_regions[i])} for i, n in enumerate(_lib.REGIONS)}
+    G = info.Nx * info.Ny * info.Nz
+    nlist_rows = None
+    candidates = {n: r for n, r in regions.items() if n in ("precond_apply", "fft", "spread", "contract", "green",
+                                                             "real_space", "rfu") and r["calls"] > 0}
+    dom = max(candidates, key=lambda n: candidates[n]["ms"])
+    launches_per_call = {"precond_apply": 2, "fft": 3}.get(dom, 1)
+    avg_launch_ms = candidates[dom]["ms"] / candidates[dom]["calls"] / launches_per_call
+    nnzb = int(N * 4.1)  # pruned blocks incl. diagonal (mean pruned degree ~3.1 at phi=0.4)
+    pairs_real = int(N * 60)
+    pairs_lub = int(N * 75)
+    nb = region_bytes(dom, N, G, nnzb, pairs_real, pairs_lub, launches_per_call)
+    peak, peak_kind = peak_hbm()
+    achieved = nb / (avg_launch_ms * 1e-3) / 1e9 if nb else None
+    traffic = None
+    tf = ROOT / "profiles" / "dram_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "avg_launch_us": avg_launch_ms * 1e3, "algorithmic_bytes_per_launch": nb}
+    it = np.array(iters)
+    out = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (FP64 Krylov/Lanczos scalars and IC pivots)",
+        "data": "synthetic: seeded random sequential addition + overlap relaxation, min gap 1e-3",
+        "config": {"workload": f"full FSD step, N={N}, phi={phi}, shear 1.0, kT 1, dt 1e-4, Ewald 1e-3, "
+                               f"GMRES 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
+                   "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
+                   "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+        "iterations_per_step": {"gmres_rfd_plus": float(it[:, 0].mean()), "gmres_rfd_minus": float(it[:, 1].mean()),
+                                "gmres_main": float(it[:, 2].mean()), "lanczos_ff": float(it[:, 3].mean()),
+                                "lanczos_nf": float(it[:, 4].mean())},
+        "regions_ms_per_step": {n: r["ms"] / args.steps for n, r in regions.items()},
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        out["cpu_baseline"] = cpu_baseline(args, pos, L, out)
+    s.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return out if rank == 0 else None
+
+
+def cpu_baseline(args, pos, L, gpu_out=None):
+    """FP64 NumPy oracle of the same method on host cores: the saddle operator
+    (mobility + lubrication, the work of every GMRES iteration) timed at the
+    full N, scaled to steps/s by the operator applications one step needs."""
+    from oracle import fsd_oracle as O
+
+    golden = np.load(ROOT / "tests" / "golden" / "ewald_xi0.5_err1e-3.npz")
+    table = (golden["table"], float(golden["self_x"]), float(golden["self_y"]), float(golden["cut"]), int(golden["n"]))
+    t0 = time.time()
+    pr = O.Problem(pos, (L, L, L), table=table)
+    setup_s = time.time() - t0
+    x = np.random.default_rng(0).standard_normal(17 * len(pos))
+    n, t = 0, time.time()
+    while True:
+        pr.saddle_multiply(x)
+        n += 1
+        if time.time() - t > args.cpu_sample_seconds:
+            break
+    t_op = (time.time() - t) / n
+    if gpu_out is not None:
+        it = gpu_out["iterations_per_step"]
+        ops = it["gmres_rfd_plus"] + it["gmres_rfd_minus"] + it["gmres_main"] + 9
+    else:
+        ops = 600.0
+    return {"value": 1.0 / (t_op * ops), "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"{n} FP64 NumPy saddle-operator applications at N={len(pos)} ({t_op:.2f} s each, "
+                      f"setup {setup_s:.1f} s) scaled by {ops:.0f} applications per step"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return None
+    from fsd_b200.configs import suspension
+
+    pos, L = suspension(args.N, args.phi, seed=1)
+    vals = []
+    t_all = time.time()
+    for _ in range(max(1, args.steps)):
+        cb = cpu_baseline(argparse.Namespace(cpu_sample_seconds=max(2.0, 10.0 / max(1, args.steps))), pos, L, None)
+        vals.append(cb["value"])
+    v = float(np.median(vals))
+    return {"metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded random sequential addition + overlap relaxation",
+            "config": {"workload": f"full FSD step, N={args.N}, phi={args.phi} (CPU FP64 oracle port)",
+                       "N": args.N, "phi": args.phi},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": "port", "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": time.time() - t_all}
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        out = run_reference(args, ws, rank)
+    else:
+        out = run_fsd(args, ws, rank, local)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

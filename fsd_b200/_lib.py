@@ -11,6 +11,8 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libfsd.so"
 
 FSD_OK = 0
+REGIONS = ("nlist", "precond_build", "spread", "fft", "green", "contract", "real_space", "rfu", "precond_apply",
+           "krylov", "lanczos", "brownian_wave", "lub_other", "integrate")
 STATUS = {
     0: "FSD_OK", 1: "FSD_ERR_BAD_PARAMS", 2: "FSD_ERR_CUDA", 3: "FSD_ERR_GMRES_MAXIT",
     4: "FSD_ERR_LANCZOS_MAXIT", 5: "FSD_ERR_ICHOL", 6: "FSD_ERR_NLIST_OVERFLOW",
@@ -36,6 +38,7 @@ class fsd_params(C.Structure):
         ("gmres_restart", C.c_int), ("gmres_max_iter", C.c_int), ("lanczos_max", C.c_int),
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
+        ("ichol_local_shift", C.c_int),
     ]
 
 
@@ -55,7 +58,7 @@ class fsd_solve_info(C.Structure):
         ("lanczos_ff_iters", C.c_int), ("lanczos_nf_iters", C.c_int),
         ("lanczos_ff_err", C.c_float), ("lanczos_nf_err", C.c_float),
         ("ichol_attempts", C.c_int), ("ichol_relaxer", C.c_float),
-        ("nlist_max", C.c_int), ("status", C.c_int),
+        ("nlist_max", C.c_int), ("status", C.c_int), ("ichol_shifted", C.c_int),
     ]
 
 
@@ -74,13 +77,17 @@ _SIGS = {
     "fsd_default_params": (None, [C.POINTER(fsd_params)]),
     "fsd_status_string": (C.c_char_p, [C.c_int]),
     "fsd_pse_setup": (C.c_int, [C.POINTER(fsd_params), C.POINTER(fsd_pse_info), P, C.c_size_t]),
+    "fsd_rcm_order": (C.c_int, [C.c_int, P, P, P]),
     "fsd_create": (C.c_int, [C.POINTER(fsd_params), P, C.POINTER(H)]),
     "fsd_destroy": (None, [H]),
     "fsd_set_stream": (C.c_int, [H, P]),
+    "fsd_launch_count": (C.c_ulonglong, []),
     "fsd_set_box": (C.c_int, [H, C.c_float, C.c_float, C.c_float, C.c_float]),
     "fsd_set_temperature": (C.c_int, [H, C.c_float]),
     "fsd_get_pse_info": (C.c_int, [H, C.POINTER(fsd_pse_info)]),
     "fsd_get_solve_info": (C.c_int, [H, C.POINTER(fsd_solve_info)]),
+    "fsd_profile_enable": (C.c_int, [H, C.c_int]),
+    "fsd_profile_read": (C.c_int, [H, P, P, C.c_int, C.c_int]),
     "fsd_get_ewald_table": (C.c_int, [H, P, C.c_size_t]),
     "fsd_build_neighbor_list": (C.c_int, [H, P]),
     "fsd_get_neighbor_list": (C.c_int, [H, P, P, C.c_size_t, C.POINTER(C.c_int)]),

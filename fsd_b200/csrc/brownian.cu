@@ -18,6 +18,7 @@
 #include "fsd_brownian.h"
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_profile.h"
 #include "fsd_solver.h"
 
 namespace fsd {
@@ -60,6 +61,7 @@ __global__ void k_normals(float* out, size_t n, uint32_t key, uint32_t step, uin
 
 void gaussian(fsd_handle* h, float* out, size_t n, uint32_t step, uint32_t stream, float scale) {
     const size_t nq = (n + 3) / 4;
+    count_launch();
     k_normals<<<(unsigned)((nq + 255) / 256), 256, 0, h->stream>>>(out, n, h->seed_hashed, step, stream, scale);
 }
 
@@ -169,7 +171,9 @@ constexpr int kDotBlocks = 296;
 
 // out = a.b in FP64 (device scalar).
 void dot_device(fsd_handle* h, const float* a, const float* b, size_t n, double* out) {
+    count_launch();
     k_dot2<<<kDotBlocks, 256, 0, h->stream>>>(a, b, n, h->w.dred);
+    count_launch();
     k_sum_parts<<<1, 32, 0, h->stream>>>(h->w.dred, kDotBlocks, out);
 }
 
@@ -291,6 +295,7 @@ int lanczos_sqrt(fsd_handle* h, size_t n, const float* x, float* y, int* m_io, f
         if (err_out) *err_out = 0.f;
         return FSD_OK;
     }
+    count_launch();
     k_scale<<<nb, 256, 0, st>>>(V, x, (float)(1.0 / xnorm), n);
     std::vector<double> alpha, beta(1, 0.0), z, zprev;
     int m = std::max(1, std::min(*m_io, mmax - 2));
@@ -303,12 +308,18 @@ int lanczos_sqrt(fsd_handle* h, size_t n, const float* x, float* y, int* m_io, f
         float* wv = V + (size_t)(j + 1) * n;
         int e = apply(vj, wv);
         if (e != FSD_OK) return e;
-        if (j > 0) k_axpby<<<nb, 256, 0, st>>>(wv, V + (size_t)(j - 1) * n, (float)(-beta[j]), n);
+        ProfRegion pl(h, R_LANCZOS);
+        if (j > 0) {
+            count_launch();
+            count_launch();
+            k_axpby<<<nb, 256, 0, st>>>(wv, V + (size_t)(j - 1) * n, (float)(-beta[j]), n);
+        }
         dot_device(h, vj, wv, n, w.lz_dot);
         FSD_CHECK_CUDA(cudaMemcpyAsync(hd, w.lz_dot, sizeof(double), cudaMemcpyDeviceToHost, st));
         FSD_CHECK_CUDA(cudaStreamSynchronize(st));
         const double a = hd[0];
         alpha.push_back(a);
+        count_launch();
         k_axpby<<<nb, 256, 0, st>>>(wv, vj, (float)(-a), n);
         dot_device(h, wv, wv, n, w.lz_dot);
         FSD_CHECK_CUDA(cudaMemcpyAsync(hd, w.lz_dot, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -318,6 +329,7 @@ int lanczos_sqrt(fsd_handle* h, size_t n, const float* x, float* y, int* m_io, f
         if (b < 1e-8) {
             stop = true;  // invariant subspace (Brownian_FarField.cu:571-579)
         } else {
+            count_launch();
             k_scale<<<nb, 256, 0, st>>>(wv, wv, (float)(1.0 / b), n);
         }
         return FSD_OK;
@@ -343,6 +355,7 @@ int lanczos_sqrt(fsd_handle* h, size_t n, const float* x, float* y, int* m_io, f
         zprev = z;
     }
     FSD_CHECK_CUDA(cudaMemcpyAsync(w.lz_dot, z.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+    count_launch();
     k_lincomb<<<nb, 256, 0, st>>>(V, n, k, w.lz_dot, y, n, (float)(xnorm * scale));
     FSD_CHECK_CUDA(cudaGetLastError());
     *m_io = std::max(1, k - 1);
@@ -362,11 +375,15 @@ int brownian_farfield(fsd_handle* h, const float4* pos, uint32_t step, float* ou
     const float fac = sqrtf(T / dt / quadW);
     const int G = g.Nx * g.Ny * g.Nz;
     // Wave space: random spectrum, inverse FFT, contraction.
+    {
+        ProfRegion prw(h, R_BROWNIAN_WAVE);
+    count_launch();
     k_noise_spectrum<<<(G + 255) / 256, 256, 0, h->stream>>>(w.grid, w.gridk, g.Nx, g.Ny, g.Nz, fac, h->seed_hashed,
                                                              step, kStreamFFWave);
     mobility_wave_from_spectrum(h, pos);
     // Combine into generalized layout (wave part only): needs f4/c4 unused.
     mobility_combine(h, pos, nullptr, w.lz_c, true, false, nullptr);
+    }
     // Real space: Lanczos square root of M_real on an 11N normal vector.
     float* psi = w.lz_a;
     gaussian(h, psi, n, step, kStreamFFReal, 1.0f);
@@ -379,7 +396,9 @@ int brownian_farfield(fsd_handle* h, const float4* pos, uint32_t step, float* ou
     h->info.lanczos_ff_err = err;
     if (st != FSD_OK && st != FSD_ERR_LANCZOS_MAXIT) return st;
     // out = wave + real
+    count_launch();
     k_scale<<<(int)std::min<size_t>(4 * 148, (n + 255) / 256), 256, 0, h->stream>>>(out11, w.lz_c, 1.0f, n);
+    count_launch();
     k_axpby<<<(int)std::min<size_t>(4 * 148, (n + 255) / 256), 256, 0, h->stream>>>(out11, w.lz_b, 1.0f, n);
     FSD_CHECK_CUDA(cudaGetLastError());
     return st;
@@ -434,8 +453,10 @@ int rfd_drift(fsd_handle* h, const float4* pos, uint32_t step, float* drift6) {
     const int N = h->p.N;
     const float eps = h->p.rfd_epsilon;
     gaussian(h, w.psi, 6 * (size_t)N, step, kStreamRFD, 1.0f);
+    count_launch();
     k_rfd_rhs<<<(17 * N + 255) / 256, 256, 0, h->stream>>>(w.rfd_rhs, w.psi, N);
     FSD_CHECK_CUDA(cudaMemsetAsync(w.rfd_sol, 0, sizeof(float) * 17 * N, h->stream));
+    count_launch();
     k_displace<<<(N + 127) / 128, 128, 0, h->stream>>>(pos, w.pos_prime, w.psi, N, h->box, eps / 2.0f);
     int it = 0;
     float res = 0.f;
@@ -445,11 +466,13 @@ int rfd_drift(fsd_handle* h, const float4* pos, uint32_t step, float* drift6) {
     if (st != FSD_OK) return st;
     FSD_CHECK_CUDA(cudaMemcpyAsync(w.vel, w.rfd_sol + 11 * N, sizeof(float) * 6 * N, cudaMemcpyDeviceToDevice,
                                    h->stream));
+    count_launch();
     k_displace<<<(N + 127) / 128, 128, 0, h->stream>>>(pos, w.pos_prime, w.psi, N, h->box, -eps / 2.0f);
     st = saddle_solve(h, w.pos_prime, w.rfd_rhs, w.rfd_sol, h->p.solver_tol, &it, &res);
     h->info.gmres_iters[1] = it;
     h->info.gmres_resid[1] = res;
     if (st != FSD_OK) return st;
+    count_launch();
     k_rfd_finish<<<(6 * N + 255) / 256, 256, 0, h->stream>>>(drift6, w.vel, w.rfd_sol + 11 * N, N, h->p.T / eps);
     // Positions used by the mobility bins must be rebinned for x on the next matvec.
     FSD_CHECK_CUDA(cudaGetLastError());

@@ -3,15 +3,21 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <algorithm>
+#include <atomic>
 
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_solver.h"
+#include "fsd_profile.h"
 
 namespace fsd {
 
 static thread_local char g_last_error[512] = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
     snprintf(g_last_error, sizeof(g_last_error), "%s (%s) at %s:%d: %s", cudaGetErrorName(e), what, file, line,
@@ -55,7 +61,8 @@ static int allocate(fsd_handle* h) {
     FSD_TRY(alloc_nlist(h, neighbor_stride_for(h->p, rlist)));
     FSD_TRY(dalloc(&w.nl_overflow, 1));
     FSD_CHECK_CUDA(cudaMallocHost(&w.host_flag, sizeof(int) * 4));
-    const int3 nc = cell_dims(h->box, rlist);
+    // Cell capacity for the untilted box (tilting only removes cells).
+    const int3 nc = cell_dims(Box{h->box.Lx, h->box.Ly, h->box.Lz, 0.0f}, rlist);
     w.ncell_cap = (nc.x >= 3 && nc.y >= 3 && nc.z >= 3) ? (size_t)nc.x * nc.y * nc.z : 0;
     const size_t nbins = std::max(w.ncell_cap, G);
     FSD_TRY(dalloc(&w.scan_scratch, scan_scratch_elems((int)nbins + 1)));
@@ -121,6 +128,7 @@ static void release(fsd_handle* h) {
     if (w.gmres_host) cudaFreeHost(w.gmres_host);
     if (w.lz_host) cudaFreeHost(w.lz_host);
     precond_free(h);
+    profile_destroy(h);
 }
 
 }  // namespace fsd
@@ -157,6 +165,7 @@ void fsd_default_params(fsd_params* p) {
     p->rlub = 4.0f;
     p->rp = 2.1f;
     p->nlist_buffer = 0.4f;
+    p->ichol_local_shift = 1;
 }
 
 const char* fsd_status_string(int status) {
@@ -202,6 +211,16 @@ int fsd_pse_setup(const fsd_params* p, fsd_pse_info* info, float* host_table, si
         if (n_floats < tab.size()) return FSD_ERR_BAD_PARAMS;
         memcpy(host_table, tab.data(), sizeof(float) * tab.size());
     }
+    return FSD_OK;
+}
+
+int fsd_rcm_order(int n, const int* rowptr, const int* col, int* perm) {
+    if (n < 0 || (n > 0 && (!rowptr || !col || !perm))) return FSD_ERR_BAD_PARAMS;
+    std::vector<int> rp(rowptr, rowptr + n + 1), cl(col, col + rowptr[n]), out;
+    for (int v : cl)
+        if (v < 0 || v >= n) return FSD_ERR_BAD_PARAMS;
+    rcm_order(n, rp, cl, out);
+    std::copy(out.begin(), out.end(), perm);
     return FSD_OK;
 }
 
@@ -259,6 +278,8 @@ void fsd_destroy(fsd_handle* h) {
     release(h);
     delete h;
 }
+
+unsigned long long fsd_launch_count(void) { return launch_count(); }
 
 int fsd_set_stream(fsd_handle* h, void* stream) {
     if (!h) return FSD_ERR_BAD_PARAMS;

@@ -20,6 +20,25 @@ __device__ __forceinline__ float3 min_image(float3 w, const Box& b) {
     return w;
 }
 
+// Pair separation j - i (or i - j) and its squared length evaluated without
+// fused multiply-adds, so that separations and gaps are the correctly rounded
+// single-precision values of the reference's arithmetic (minImage, dot,
+// sqrtf).  Near contact the lubrication functions are steep in the gap, so
+// this rounding is part of the result.
+__device__ __forceinline__ float3 min_image_rn(float3 w, const Box& b) {
+    float img = rintf(__fmul_rn(w.z, 1.0f / b.Lz));
+    w.z = __fsub_rn(w.z, __fmul_rn(b.Lz, img));
+    img = rintf(__fmul_rn(w.y, 1.0f / b.Ly));
+    w.x = __fsub_rn(w.x, __fmul_rn(__fmul_rn(b.Ly, b.xy), img));
+    w.y = __fsub_rn(w.y, __fmul_rn(b.Ly, img));
+    w.x = __fsub_rn(w.x, __fmul_rn(b.Lx, rintf(__fmul_rn(w.x, 1.0f / b.Lx))));
+    return w;
+}
+
+__device__ __forceinline__ float dist2_rn(float3 r) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
+}
+
 // Fractional coordinates in [0,1) of the sheared box (HOOMD BoxDim::makeFraction).
 __device__ __forceinline__ float3 make_fraction(float3 v, const Box& b) {
     float3 d = make_float3(v.x + b.Lx / 2, v.y + b.Ly / 2, v.z + b.Lz / 2);

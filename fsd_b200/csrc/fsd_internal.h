@@ -22,6 +22,10 @@ namespace fsd {
 
 void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 
+// Kernel launches issued by this library (all handles, all threads).
+void count_launch();
+unsigned long long launch_count();
+
 struct GridParams {
     int Nx = 0, Ny = 0, Nz = 0, P = 0;
     float ewald_cut = 0, gauss_m = 0, eta = 0, hx = 0, hy = 0, hz = 0;
@@ -136,5 +140,6 @@ struct fsd_handle {
     uint32_t seed_hashed = 0;
     float ichol_relaxer = 1.0f;
     int m_lanczos_ff = 2, m_lanczos_nf = 2;
-    void* ichol = nullptr;  // preconditioner state (precond.cu)
+    void* ichol = nullptr;     // preconditioner state (precond.cu)
+    void* profiler = nullptr;  // region timers (profile.cpp)
 };

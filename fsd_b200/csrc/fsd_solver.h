@@ -18,6 +18,8 @@ int precond_alloc(fsd_handle* h);
 void precond_free(fsd_handle* h);
 int precond_build(fsd_handle* h, const float4* pos);
 int precond_G(fsd_handle* h, const float* t, float* y);
+int precond_apply_ichol(fsd_handle* h, const float* b, float* x);
+int precond_wait_status(fsd_handle* h);
 
 // Host reverse Cuthill-McKee ordering of a symmetric graph in CSR form
 // (adjacency may include self loops).  perm[new] = old.

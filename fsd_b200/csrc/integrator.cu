@@ -8,6 +8,7 @@
 #include "fsd_brownian.h"
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_profile.h"
 #include "fsd_solver.h"
 
 namespace fsd {
@@ -30,8 +31,8 @@ __global__ void k_pair_force(const float4* __restrict__ pos, int N, Box b, const
     for (unsigned q = 0; q < nn; ++q) {
         const unsigned j = nlist[(size_t)i * stride + q];
         const float4 pj = pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
-        const float dist = sqrtf(R.x * R.x + R.y * R.y + R.z * R.z);
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
+        const float dist = sqrtf(dist2_rn(R));
         const float gap = dist - rcol;
         float mag = 0.f;
         if (gap >= 0.f && dist <= 2.0f + 10.0f / kappa) mag = Hamaker / (12.f * (gap * gap + epsq)) - F0 * expf(-kappa * gap);
@@ -153,6 +154,8 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
     e = precond_build(h, pos);
     if (e != FSD_OK) return e;
     if (h->p.force_mode == FSD_FORCE_INTERPARTICLE) {
+        ProfRegion pr(h, R_INTEGRATE);
+        count_launch();
         k_pair_force<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, w.nneigh, w.nlist, w.nl_stride, h->p.ndsr,
                                                       h->p.k_n, h->p.kappa, h->p.beta_AF, h->p.epsq,
                                                       h->p.T_ext * cosf(h->p.omega_ext * a->timestep * h->p.dt),
@@ -170,6 +173,7 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
         e = rfd_drift(h, pos, step, vel);
         if (e != FSD_OK) return e;
     }
+    count_launch();
     k_rhs_terms<<<(N + 127) / 128, 128, 0, st>>>(rhs, a->d_force, N, a->shear_rate, h->p.sqm_B2, a->d_b2_mask,
                                                  (const float3*)a->d_ori);
     lub_rfe(h, pos, a->shear_rate, (const float3*)a->d_ori, a->d_b2_mask, h->p.sqm_B2, rhs + 11 * N);
@@ -179,8 +183,10 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
     h->info.gmres_iters[2] = it;
     h->info.gmres_resid[2] = res;
     if (e != FSD_OK) return e;
+    count_launch();
     k_add<<<vb(6 * N), 256, 0, st>>>(vel, w.sol + 11 * N, 6 * (size_t)N);
     if (h->p.period > 0 && ((int)(a->timestep + 1) % h->p.period) == 0) {
+        count_launch();
         k_add<<<vb(5 * N), 256, 0, st>>>(vel + 6 * N, w.sol + 6 * N, 5 * (size_t)N);
         lub_rsu(h, pos, vel, vel + 6 * N);
         lub_rse(h, pos, a->shear_rate, (const float3*)a->d_ori, a->d_b2_mask, h->p.sqm_B2, vel + 6 * N);
@@ -193,11 +199,13 @@ int step(fsd_handle* h, const fsd_step_args* a) {
     const int N = h->p.N;
     int e = compute_velocity(h, a);
     if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+    ProfRegion pr(h, R_INTEGRATE);
     const float3* noise = (const float3*)a->d_noise_ang;
     if (!noise && h->p.rot_diff > 0.f) {
         gaussian(h, h->w.pc_t, 3 * (size_t)N, a->timestep, kStreamRot, sqrtf(2.0f * h->p.rot_diff / h->p.dt));
         noise = (const float3*)h->w.pc_t;
     }
+    count_launch();
     k_euler_shear<<<(N + 127) / 128, 128, 0, h->stream>>>((float4*)a->d_pos, (float3*)a->d_ori, (float4*)a->d_pos_gb,
                                                            a->d_velocity, h->p.sqm_B1, a->d_b1_mask, noise,
                                                            (int3*)a->d_image, N, h->box, h->p.dt, a->shear_rate);

@@ -6,6 +6,7 @@
 // Jeffrey-Onishi functions exactly as the reference does (res_interp).
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_profile.h"
 
 namespace fsd {
 
@@ -68,8 +69,8 @@ __global__ void __launch_bounds__(128) k_rfu(LubArgs a, const float* __restrict_
     for (unsigned q = gl; q < nn; q += kLubGroup) {
         const unsigned j = row[q];
         const float4 pj = a.pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
-        const float d2 = R.x * R.x + R.y * R.y + R.z * R.z;
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
+        const float d2 = dist2_rn(R);
         if (!(d2 < a.rlub2 && d2 > 0.f)) continue;
         const float dist = sqrtf(d2);
         float c[10];
@@ -126,8 +127,8 @@ __global__ void __launch_bounds__(128) k_rfe(LubArgs a, float shear_rate, const 
     for (unsigned q = gl; q < nn; q += kLubGroup) {
         const unsigned j = row[q];
         const float4 pj = a.pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
-        const float d2 = R.x * R.x + R.y * R.y + R.z * R.z;
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
+        const float d2 = dist2_rn(R);
         if (!(d2 < a.rlub2)) continue;
         const float dist = sqrtf(d2);
         float c[6];
@@ -183,8 +184,8 @@ __global__ void __launch_bounds__(128) k_rsu(LubArgs a, const float* __restrict_
     for (unsigned q = gl; q < nn; q += kLubGroup) {
         const unsigned j = row[q];
         const float4 pj = a.pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
-        const float d2 = R.x * R.x + R.y * R.y + R.z * R.z;
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
+        const float d2 = dist2_rn(R);
         if (!(d2 < a.rlub2)) continue;
         const float dist = sqrtf(d2);
         float c[6];
@@ -230,8 +231,8 @@ __global__ void __launch_bounds__(128) k_rse(LubArgs a, float shear_rate, const 
     for (unsigned q = gl; q < nn; q += kLubGroup) {
         const unsigned j = row[q];
         const float4 pj = a.pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
-        const float d2 = R.x * R.x + R.y * R.y + R.z * R.z;
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), a.box);
+        const float d2 = dist2_rn(R);
         if (!(d2 < 16.0f)) continue;
         const float dist = sqrtf(d2);
         float c[6];
@@ -286,17 +287,25 @@ static LubArgs lub_args(fsd_handle* h, const float4* pos) {
 static int lub_blocks(int N) { return (N * kLubGroup + 127) / 128; }
 
 void lub_rfu(fsd_handle* h, const float4* pos, const float* U, float* F, const float* saddle_x) {
+    ProfRegion pr(h, R_RFU);
+    count_launch();
     k_rfu<<<lub_blocks(h->p.N), 128, 0, h->stream>>>(lub_args(h, pos), U, F, saddle_x);
 }
 void lub_rfe(fsd_handle* h, const float4* pos, float shear_rate, const float3* ori, const float* b2mask, float B2,
              float* F) {
+    ProfRegion pr(h, R_LUB_OTHER);
+    count_launch();
     k_rfe<<<lub_blocks(h->p.N), 128, 0, h->stream>>>(lub_args(h, pos), shear_rate, ori, b2mask, B2, F);
 }
 void lub_rsu(fsd_handle* h, const float4* pos, const float* U, float* S) {
+    ProfRegion pr(h, R_LUB_OTHER);
+    count_launch();
     k_rsu<<<lub_blocks(h->p.N), 128, 0, h->stream>>>(lub_args(h, pos), U, S);
 }
 void lub_rse(fsd_handle* h, const float4* pos, float shear_rate, const float3* ori, const float* b2mask, float B2,
              float* S) {
+    ProfRegion pr(h, R_LUB_OTHER);
+    count_launch();
     k_rse<<<lub_blocks(h->p.N), 128, 0, h->stream>>>(lub_args(h, pos), shear_rate, ori, b2mask, B2, S);
 }
 

@@ -23,6 +23,7 @@
 
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_profile.h"
 
 namespace fsd {
 
@@ -234,6 +235,12 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids) {
         else
             nblocks = ngrids * (axis == 1 ? Nx : Ny) * ((Nz + B - 1) / B);
         const size_t shm = sizeof(float2) * ((size_t)pl.n + 2 * (size_t)B * pl.n);
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(k_fft_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr_set = true;
+        }
+        count_launch();
         k_fft_axis<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, Ny, Nz, axis, B, pl, tw, inv, ngrids);
     };
     if (!inv) {
@@ -280,6 +287,7 @@ __global__ void k_gridk(float4* gridk, int Nx, int Ny, int Nz, Box b, float xi, 
 void mobility_set_gridk(fsd_handle* h) {
     const int G = h->g.Nx * h->g.Ny * h->g.Nz;
     const double two_pi = h->p.kgrid_pi_ref ? 2.0 * 3.1416926536 : 2.0 * M_PI;
+    count_launch();
     k_gridk<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz, h->box, h->p.xi, h->g.eta,
                                                     two_pi);
 }
@@ -445,6 +453,7 @@ __global__ void k_origin_key(const float4* __restrict__ pos, int N, Box b, int N
 int mobility_bin_particles(fsd_handle* h, const float4* pos) {
     Workspace& w = h->w;
     const int N = h->p.N, Nx = h->g.Nx, Ny = h->g.Ny, Nz = h->g.Nz;
+    count_launch();
     k_origin_key<<<(N + 255) / 256, 256, 0, h->stream>>>(pos, N, h->box, Nx, Ny, Nz, h->g.P, w.part_origin_key,
                                                         w.part_origin);
     counting_sort(w.part_origin_key, N, Nx * Ny * Nz, w.bin_count, w.bin_start, w.bin_fill, w.bin_parts,
@@ -698,7 +707,9 @@ __global__ void __launch_bounds__(128) k_real_combine(RealArgs a) {
             const float dist = sqrtf(distSqr);
             const float4 Fj = a.f4[j];
             const float4 C0 = a.c4[2 * j], C1 = a.c4[2 * j + 1];
-            const int r_ind = __float2int_rd(a.ewald_n * (dist - a.ewald_dr) / (a.ewald_cut - a.ewald_dr));
+            // Clamped so that a distance rounding up to the cutoff stays inside the table.
+            const int r_ind = min(max(__float2int_rd(a.ewald_n * (dist - a.ewald_dr) / (a.ewald_cut - a.ewald_dr)), 0),
+                                  a.ewald_n - 1);
             const float4 t1m = __ldg(a.table + 2 * r_ind), t2m = __ldg(a.table + 2 * r_ind + 1);
             const float4 t1p = __ldg(a.table + 2 * r_ind + 2), t2p = __ldg(a.table + 2 * r_ind + 3);
             const float fac = dist / a.ewald_dr - r_ind - 1.0f;
@@ -837,6 +848,7 @@ static void spread(fsd_handle* h, const float4* pos) {
     a.prefac = (2.0 * xisq / kPiRef / g.eta) * sqrtf(2.0 * xisq / kPiRef / g.eta);
     a.expfac = 2.0 * xisq / g.eta;
     const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
+    count_launch();
     k_spread<<<ntiles, a.TX * a.TY * a.TZ, 0, h->stream>>>(a);
 }
 
@@ -847,12 +859,17 @@ static void contract(fsd_handle* h, const float4* pos) {
     const float expfac = 2.0 * xisq / g.eta;
     const float quadW = g.hx * g.hy * g.hz;
     const int N = h->p.N;
+    count_launch();
     k_contract<<<(N * 32 + 255) / 256, 256, 0, h->stream>>>(pos, h->w.grid, N, h->box, g.Nx, g.Ny, g.Nz, g.P, g.hx,
                                                             g.hy, g.hz, quadW * prefac, expfac, h->w.uwave);
 }
 
 void mobility_wave_from_spectrum(fsd_handle* h, const float4* pos) {
-    fft3d(h, true, 6);
+    {
+        ProfRegion pr(h, R_FFT);
+        fft3d(h, true, 6);
+    }
+    ProfRegion pr(h, R_CONTRACT);
     contract(h, pos);
 }
 
@@ -879,26 +896,45 @@ void mobility_combine(fsd_handle* h, const float4* pos, const float* genF, float
     r.saddle_x = saddle_x;
     r.genU = genU;
     const int N = h->p.N;
+    count_launch();
     k_real_combine<<<(N * kRealGroup + 127) / 128, 128, 0, h->stream>>>(r);
 }
 
 int mobility_apply(fsd_handle* h, const float4* pos, const float* genF, float* genU, int parts, const float* saddle_x,
                    bool rebin) {
     const int N = h->p.N;
+    count_launch();
     k_prep<<<(N + 255) / 256, 256, 0, h->stream>>>(genF, N, h->w.f4, h->w.c4);
     const bool wave = parts & 1, real = parts & 2;
     if (wave) {
-        if (rebin) {
-            int st = mobility_bin_particles(h, pos);
-            if (st != FSD_OK) return st;
+        {
+            ProfRegion pr(h, R_SPREAD);
+            if (rebin) {
+                int st = mobility_bin_particles(h, pos);
+                if (st != FSD_OK) return st;
+            }
+            spread(h, pos);
         }
-        spread(h, pos);
-        fft3d(h, false, 6);
-        const int G = h->g.Nx * h->g.Ny * h->g.Nz;
-        k_green<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.grid, h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz);
-        fft3d(h, true, 6);
-        contract(h, pos);
+        {
+            ProfRegion pr(h, R_FFT);
+            fft3d(h, false, 6);
+        }
+        {
+            ProfRegion pr(h, R_GREEN);
+            const int G = h->g.Nx * h->g.Ny * h->g.Nz;
+            count_launch();
+            k_green<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.grid, h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz);
+        }
+        {
+            ProfRegion pr(h, R_FFT);
+            fft3d(h, true, 6);
+        }
+        {
+            ProfRegion pr(h, R_CONTRACT);
+            contract(h, pos);
+        }
     }
+    ProfRegion pr(h, R_REAL);
     mobility_combine(h, pos, genF, genU, wave, real, saddle_x);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;

@@ -9,6 +9,7 @@
 // along an axis fall back to an all-pairs scan.
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_profile.h"
 
 namespace fsd {
 
@@ -89,8 +90,11 @@ size_t scan_scratch_elems(int n) { return (size_t)(n + kScanTile - 1) / kScanTil
 
 void exclusive_scan(const unsigned* in, unsigned* out, int n, unsigned* scratch, cudaStream_t st) {
     const int nb = (n + kScanTile - 1) / kScanTile;
+    count_launch();
     scan_tiles<<<nb, kScanThreads, 0, st>>>(in, out, scratch, n);
+    count_launch();
     scan_sums<<<1, kScanThreads, 0, st>>>(scratch, nb, out + n);
+    count_launch();
     scan_add<<<(n + 255) / 256, 256, 0, st>>>(out, scratch, n);
 }
 
@@ -128,15 +132,18 @@ void counting_sort(const unsigned* key, int n, int nbins, unsigned* count, unsig
                    unsigned* items, unsigned* scan_scratch, cudaStream_t st) {
     cudaMemsetAsync(count, 0, sizeof(unsigned) * nbins, st);
     cudaMemsetAsync(fill, 0, sizeof(unsigned) * nbins, st);
+    count_launch();
     k_bin_count<<<(n + 255) / 256, 256, 0, st>>>(key, n, count);
     exclusive_scan(count, start, nbins, scan_scratch, st);
+    count_launch();
     k_bin_fill<<<(n + 255) / 256, 256, 0, st>>>(key, n, start, fill, items);
+    count_launch();
     k_bin_sort<<<(nbins + 255) / 256, 256, 0, st>>>(start, nbins, items);
 }
 
 // ------------------------------------------------------------------ cell list
 __global__ void k_cell_key(const float4* pos, int n, Box b, int3 nc, unsigned* key) {
-    const int i = blockIdx.x * blockIdx.y * 0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
     const float3 f = make_fraction(make_float3(p.x, p.y, p.z), b);
@@ -168,8 +175,8 @@ __global__ void k_nlist_cells(const float4* __restrict__ pos, int n, Box b, int3
                     const unsigned j = cparts[k];
                     if (j == (unsigned)i) continue;
                     const float4 pj = pos[j];
-                    const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
-                    if (r.x * r.x + r.y * r.y + r.z * r.z < rlist2) {
+                    const float3 r = min_image_rn(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
+                    if (dist2_rn(r) < rlist2) {
                         if (cnt < (unsigned)stride) row[cnt] = j;
                         ++cnt;
                     }
@@ -191,8 +198,8 @@ __global__ void k_nlist_allpairs(const float4* __restrict__ pos, int n, Box b, f
     for (int j = 0; j < n; ++j) {
         if (j == i) continue;
         const float4 pj = pos[j];
-        const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
-        if (r.x * r.x + r.y * r.y + r.z * r.z < rlist2) {
+        const float3 r = min_image_rn(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
+        if (dist2_rn(r) < rlist2) {
             if (cnt < (unsigned)stride) row[cnt] = j;
             ++cnt;
         }
@@ -219,14 +226,18 @@ int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host) {
     const float rlist2 = rlist * rlist;
     const int3 nc = cell_dims(h->box, rlist);
     cudaStream_t st = h->stream;
+    ProfRegion pr(h, R_NLIST);
     FSD_CHECK_CUDA(cudaMemsetAsync(w.nl_overflow, 0, sizeof(int), st));
     if (nc.x >= 3 && nc.y >= 3 && nc.z >= 3 && (size_t)nc.x * nc.y * nc.z <= w.ncell_cap) {
         const int ncells = nc.x * nc.y * nc.z;
+        count_launch();
         k_cell_key<<<(n + 255) / 256, 256, 0, st>>>(pos, n, h->box, nc, w.part_cell);
         counting_sort(w.part_cell, n, ncells, w.cell_count, w.cell_start, w.cell_fill, w.cell_parts, w.scan_scratch, st);
+        count_launch();
         k_nlist_cells<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, nc, w.part_cell, w.cell_start, w.cell_parts,
                                                        rlist2, w.nneigh, w.nlist, w.nl_stride, w.nl_overflow);
     } else {
+        count_launch();
         k_nlist_allpairs<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, rlist2, w.nneigh, w.nlist, w.nl_stride,
                                                           w.nl_overflow);
     }

@@ -10,8 +10,10 @@
 //     (genrcm, rcm.cpp:1009, restated in rcm_order below);
 //  4. incomplete Cholesky with zero fill.  The scalar IC(0) of the reference
 //     on a pattern made of dense 6x6 blocks equals block IC(0), which is what
-//     is computed here, with FP64 arithmetic and pivots; a non-positive pivot
-//     doubles the relaxer and refactors (Precondition.cu:1457-1489);
+//     is computed here, with FP64 arithmetic and pivots.  A pivot block that
+//     is not positive definite either gets a local diagonal shift (default) or,
+//     as the reference does, doubles the global relaxer and refactors
+//     (Precondition.cu:1457-1489);
 //  5. forward / backward block triangular solves, scheduled by dependency
 //     level (one launch per level).
 #include <algorithm>
@@ -21,6 +23,7 @@
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_solver.h"
+#include "fsd_profile.h"
 
 namespace fsd {
 
@@ -44,6 +47,11 @@ struct IChol {
     int* blev_rows = nullptr;    // rows sorted by backward level
     float* ty = nullptr;         // permuted work vector (6N)
     float* tz = nullptr;
+    unsigned* ready_f = nullptr; // per-row completion epoch, forward solve
+    unsigned* ready_b = nullptr; // per-row completion epoch, backward solve
+    unsigned* tickets = nullptr; // row tickets [forward, backward]
+    int* wait_err = nullptr;     // set when a bounded wait gave up
+    unsigned epoch = 0;
     int nnzb_cap = 0;
     // host
     std::vector<int> lev_ptr, blev_ptr;
@@ -66,8 +74,8 @@ __global__ void k_prune(const float4* __restrict__ pos, int N, Box b, const unsi
     for (unsigned q = 0; q < nn; ++q) {
         const unsigned j = nlist[(size_t)i * stride + q];
         const float4 pj = pos[j];
-        const float3 r = min_image(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
-        if (r.x * r.x + r.y * r.y + r.z * r.z < rp2) {
+        const float3 r = min_image_rn(make_float3(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z), b);
+        if (dist2_rn(r) < rp2) {
             if (cnt < kPrunedCap) row[cnt] = j;
             ++cnt;
         }
@@ -112,8 +120,8 @@ __global__ void k_assemble(const float4* __restrict__ pos, int N, Box b, const u
             continue;
         }
         const float4 pj = pos[j];
-        const float3 R = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
-        const float d2 = R.x * R.x + R.y * R.y + R.z * R.z;
+        const float3 R = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
+        const float d2 = dist2_rn(R);
         float c[10];
         if (!(d2 < rp2)) {
 #pragma unroll
@@ -192,7 +200,8 @@ __device__ void chol6(double* A, bool* ok) {
 
 __global__ void k_factor_level(const int* __restrict__ rows, int nrows, const int* __restrict__ rowptr,
                                const int* __restrict__ col, const int* __restrict__ src, const int* __restrict__ diag,
-                               const float* __restrict__ blocks, float* L, float* Linv, int* fail) {
+                               const float* __restrict__ blocks, float* L, float* Linv, int* fail, bool local_shift,
+                               double shift0, int* shifted) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
     const int p = rows[t];
@@ -238,7 +247,22 @@ __global__ void k_factor_level(const int* __restrict__ rows, int nrows, const in
             for (int k = 0; k < 36; ++k) out[k] = (float)acc[k];
         } else {
             bool ok = true;
+            double keep[36];
+            for (int k = 0; k < 36; ++k) keep[k] = acc[k];
             chol6(acc, &ok);
+            // Pivot-local shift: a pivot block that is not positive definite
+            // gets tau * {1,1,1,4/3,4/3,4/3} added, tau doubling from
+            // `shift0`, instead of shifting the whole matrix.
+            if (!ok && local_shift) {
+                double tau = shift0;
+                for (int attempt = 0; attempt < 40 && !ok; ++attempt, tau *= 2.0) {
+                    for (int k = 0; k < 36; ++k) acc[k] = keep[k];
+                    for (int d = 0; d < 6; ++d) acc[d * 7] += tau * ((d < 3) ? 1.0 : (double)1.33333333f);
+                    ok = true;
+                    chol6(acc, &ok);
+                }
+                if (ok) atomicAdd(shifted, 1);
+            }
             if (!ok) atomicExch(fail, 1);
             for (int k = 0; k < 36; ++k) out[k] = (float)acc[k];
             // inverse of the lower-triangular factor, forward substitution on I
@@ -338,6 +362,125 @@ __global__ void k_permute(const float* __restrict__ in, float* __restrict__ out,
         out[6 * perm[p] + c] = in[k];  // back to original order
 }
 
+// ------------------------------------------------------- sync-free solves
+// One launch per triangular solve.  Warps take rows in dependency order from
+// a ticket counter, so every row a warp waits on belongs to a warp that is
+// already running; a finished row publishes its values, then its epoch flag.
+// Each wait is bounded: after kWaitLimit polls the kernel records the row in
+// *err and carries on, so a fault in the schedule cannot hang the GPU.
+constexpr int kWaitLimit = 1 << 22;
+
+__device__ __forceinline__ void wait_ready(const unsigned* flag, unsigned epoch, int* err, int row) {
+    int n = 0;
+    while (*(volatile const unsigned*)flag != epoch) {
+        if (++n > kWaitLimit) {
+            atomicExch(err, row + 1);
+            break;
+        }
+        __nanosleep(32);
+    }
+    __threadfence();
+}
+
+// Forward solve with the saddle pre-step fused: for permuted row p with
+// particle i = perm[p], t_p = b[6i:6i+6] - b[11N+6i:11N+6i+6], then
+// z_p = Linv_pp (t_p - sum_{q<p} L_pq z_q).  Also copies b[6N:11N] to x.
+__global__ void __launch_bounds__(128) k_trsv_fwd(const int* __restrict__ order, int N, const int* __restrict__ perm,
+                                                  const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                  const int* __restrict__ diag, const float* __restrict__ L,
+                                                  const float* __restrict__ Linv, const float* __restrict__ b,
+                                                  float* __restrict__ x, float* z, unsigned* ready, unsigned epoch,
+                                                  unsigned* ticket, int* err) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned tk = 0;
+        if (lane == 0) tk = atomicAdd(ticket, 1u);
+        tk = __shfl_sync(0xffffffffu, tk, 0);
+        if (tk >= (unsigned)N) return;
+        const int p = order[tk];
+        const int i = perm[p];
+        float v = 0.f;
+        if (lane < 6) v = b[6 * i + lane] - b[11 * (size_t)N + 6 * i + lane];
+        if (lane < 5) x[6 * (size_t)N + 5 * i + lane] = b[6 * (size_t)N + 5 * i + lane];
+        for (int e = rowptr[p]; e < diag[p]; ++e) {
+            const int q = col[e];
+            if (lane == 0) wait_ready(ready + q, epoch, err, q);
+            __syncwarp();
+            float zq = (lane < 6) ? __ldcg(z + 6 * q + lane) : 0.f;
+            const float* B = L + (size_t)e * 36;
+            float acc = 0.f;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                const float zd = __shfl_sync(0xffffffffu, zq, d);
+                if (lane < 6) acc += B[lane * 6 + d] * zd;
+            }
+            v -= acc;
+        }
+        const float* Li = Linv + (size_t)p * 36;
+        float out = 0.f;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+            const float vd = __shfl_sync(0xffffffffu, v, d);
+            if (lane < 6 && d <= lane) out += Li[lane * 6 + d] * vd;
+        }
+        if (lane < 6) __stcg(z + 6 * p + lane, out);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicExch(ready + p, epoch);
+    }
+}
+
+// Backward solve with the saddle post-step fused: x_p = Linv_pp^T (z_p -
+// sum_{q>p} L_qp^T x_q); particle i = perm[p] gets y = x_p:
+// out[6i:6i+6] = b[6i:6i+6] - y and out[11N+6i:11N+6i+6] = y.
+__global__ void __launch_bounds__(128) k_trsv_bwd(const int* __restrict__ order, int N, const int* __restrict__ perm,
+                                                  const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                  const int* __restrict__ diag, const int* __restrict__ tpos,
+                                                  const float* __restrict__ L, const float* __restrict__ Linv,
+                                                  const float* __restrict__ z, const float* __restrict__ b,
+                                                  float* __restrict__ out, float* xp, unsigned* ready, unsigned epoch,
+                                                  unsigned* ticket, int* err) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned tk = 0;
+        if (lane == 0) tk = atomicAdd(ticket, 1u);
+        tk = __shfl_sync(0xffffffffu, tk, 0);
+        if (tk >= (unsigned)N) return;
+        const int p = order[tk];
+        float v = (lane < 6) ? __ldcg(z + 6 * p + lane) : 0.f;
+        for (int e = diag[p] + 1; e < rowptr[p + 1]; ++e) {
+            const int q = col[e];
+            if (lane == 0) wait_ready(ready + q, epoch, err, q);
+            __syncwarp();
+            float xq = (lane < 6) ? __ldcg(xp + 6 * q + lane) : 0.f;
+            const float* B = L + (size_t)tpos[e] * 36;  // L_qp
+            float acc = 0.f;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const float xc = __shfl_sync(0xffffffffu, xq, c);
+                if (lane < 6) acc += B[c * 6 + lane] * xc;
+            }
+            v -= acc;
+        }
+        const float* Li = Linv + (size_t)p * 36;
+        float y = 0.f;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const float vc = __shfl_sync(0xffffffffu, v, c);
+            if (lane < 6 && c >= lane) y += Li[c * 6 + lane] * vc;
+        }
+        if (lane < 6) {
+            __stcg(xp + 6 * p + lane, y);
+            const int i = perm[p];
+            out[6 * i + lane] = b[6 * i + lane] - y;
+            out[11 * (size_t)N + 6 * i + lane] = y;
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicExch(ready + p, epoch);
+    }
+}
+
 // -------------------------------------------------------------- host RCM
 namespace {
 // Breadth-first level structure from root over unmasked nodes; returns the
@@ -432,11 +575,13 @@ void rcm_order(int n, const std::vector<int>& rp, const std::vector<int>& cl, st
                         perm.push_back(u);
                     }
                 }
-                // stable insertion sort of perm[fnbr..) by degree
-                for (size_t k = fnbr + 1; k < perm.size(); ++k) {
+                // Stable insertion sort by degree of the new neighbours after
+                // the first one; the first stays in place, as in the
+                // reference's genrcm (rcm.cpp, inner loop `while ( fnbr < l )`).
+                for (size_t k = fnbr + 2; k < perm.size(); ++k) {
                     const int key = perm[k];
                     size_t l = k;
-                    while (l > fnbr && deg[perm[l - 1]] > deg[key]) {
+                    while (l > fnbr + 1 && deg[perm[l - 1]] > deg[key]) {
                         perm[l] = perm[l - 1];
                         --l;
                     }
@@ -468,11 +613,18 @@ int precond_alloc(fsd_handle* h) {
     FSD_CHECK_CUDA(cudaMalloc(&ic->tpos, sizeof(int) * (size_t)ic->nnzb_cap));
     FSD_CHECK_CUDA(cudaMalloc(&ic->L, sizeof(float) * 36 * (size_t)ic->nnzb_cap));
     FSD_CHECK_CUDA(cudaMalloc(&ic->Linv, sizeof(float) * 36 * (size_t)N));
-    FSD_CHECK_CUDA(cudaMalloc(&ic->fail, sizeof(int)));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->fail, sizeof(int) * 2));
     FSD_CHECK_CUDA(cudaMalloc(&ic->lev_rows, sizeof(int) * N));
     FSD_CHECK_CUDA(cudaMalloc(&ic->blev_rows, sizeof(int) * N));
     FSD_CHECK_CUDA(cudaMalloc(&ic->ty, sizeof(float) * 6 * (size_t)N));
     FSD_CHECK_CUDA(cudaMalloc(&ic->tz, sizeof(float) * 6 * (size_t)N));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->ready_f, sizeof(unsigned) * N));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->ready_b, sizeof(unsigned) * N));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->tickets, sizeof(unsigned) * 2));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->wait_err, sizeof(int)));
+    FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_f, 0, sizeof(unsigned) * N, h->stream));
+    FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_b, 0, sizeof(unsigned) * N, h->stream));
+    FSD_CHECK_CUDA(cudaMemsetAsync(ic->wait_err, 0, sizeof(int), h->stream));
     FSD_CHECK_CUDA(cudaMallocHost(&ic->h_fail, sizeof(int) * 2));
     return FSD_OK;
 }
@@ -481,7 +633,8 @@ void precond_free(fsd_handle* h) {
     IChol* ic = (IChol*)h->ichol;
     if (!ic) return;
     void* ptrs[] = {ic->pn, ic->plist, ic->p_over, ic->blocks, ic->perm, ic->rowptr, ic->col, ic->src, ic->diag,
-                    ic->tpos, ic->L, ic->Linv, ic->fail, ic->lev_rows, ic->blev_rows, ic->ty, ic->tz};
+                    ic->tpos, ic->L, ic->Linv, ic->fail, ic->lev_rows, ic->blev_rows, ic->ty, ic->tz,
+                    ic->ready_f, ic->ready_b, ic->tickets, ic->wait_err};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ic->h_fail) cudaFreeHost(ic->h_fail);
@@ -499,7 +652,9 @@ int precond_build(fsd_handle* h, const float4* pos) {
         h->pc_valid = true;
         return FSD_OK;
     }
+    ProfRegion pr(h, R_PRECOND_BUILD);
     FSD_CHECK_CUDA(cudaMemsetAsync(ic->p_over, 0, sizeof(int), st));
+    count_launch();
     k_prune<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride,
                                              h->p.rp * h->p.rp, ic->pn, ic->plist, ic->p_over);
     ic->h_pn.resize(N);
@@ -586,18 +741,23 @@ int precond_build(fsd_handle* h, const float4* pos) {
     h->info.ichol_attempts = 0;
     // Factor, doubling the relaxer after each failure (Precondition.cu:1457-1489).
     for (int attempt = 0; attempt < 24; ++attempt) {
+        count_launch();
         k_assemble<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, ic->pn, ic->plist,
                                                    ResTable{h->d_res_dist, h->d_res_vals}, h->p.rp, h->ichol_relaxer,
                                                    ic->blocks);
-        FSD_CHECK_CUDA(cudaMemsetAsync(ic->fail, 0, sizeof(int), st));
+        FSD_CHECK_CUDA(cudaMemsetAsync(ic->fail, 0, sizeof(int) * 2, st));
         for (int l = 0; l < nlev; ++l) {
             const int n = ic->lev_ptr[l + 1] - ic->lev_ptr[l];
+            count_launch();
             k_factor_level<<<(n + 63) / 64, 64, 0, st>>>(ic->lev_rows + ic->lev_ptr[l], n, ic->rowptr, ic->col,
-                                                        ic->src, ic->diag, ic->blocks, ic->L, ic->Linv, ic->fail);
+                                                        ic->src, ic->diag, ic->blocks, ic->L, ic->Linv, ic->fail,
+                                                        h->p.ichol_local_shift != 0, (double)h->ichol_relaxer,
+                                                        ic->fail + 1);
         }
-        FSD_CHECK_CUDA(cudaMemcpyAsync(ic->h_fail, ic->fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+        FSD_CHECK_CUDA(cudaMemcpyAsync(ic->h_fail, ic->fail, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
         FSD_CHECK_CUDA(cudaStreamSynchronize(st));
         h->info.ichol_attempts = attempt + 1;
+        h->info.ichol_shifted = ic->h_fail[1];
         if (!ic->h_fail[0]) {
             h->info.ichol_relaxer = h->ichol_relaxer;
             h->pc_valid = true;
@@ -608,6 +768,45 @@ int precond_build(fsd_handle* h, const float4* pos) {
     return FSD_ERR_ICHOL;
 }
 
+// x = P^-1 b for the saddle system with the IC(0) factor, two launches.
+int precond_apply_ichol(fsd_handle* h, const float* b, float* x) {
+    IChol* ic = (IChol*)h->ichol;
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
+    ic->epoch += 1;
+    if (ic->epoch == 0) {  // wrapped: clear the flags once
+        FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_f, 0, sizeof(unsigned) * N, st));
+        FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_b, 0, sizeof(unsigned) * N, st));
+        ic->epoch = 1;
+    }
+    FSD_CHECK_CUDA(cudaMemsetAsync(ic->tickets, 0, sizeof(unsigned) * 2, st));
+    const int warps = std::min(N, 148 * 16);
+    const int blocks = (warps * 32 + 127) / 128;
+    count_launch();
+    k_trsv_fwd<<<blocks, 128, 0, st>>>(ic->lev_rows, N, ic->perm, ic->rowptr, ic->col, ic->diag, ic->L, ic->Linv, b, x,
+                                       ic->tz, ic->ready_f, ic->epoch, ic->tickets, ic->wait_err);
+    count_launch();
+    k_trsv_bwd<<<blocks, 128, 0, st>>>(ic->blev_rows, N, ic->perm, ic->rowptr, ic->col, ic->diag, ic->tpos, ic->L,
+                                       ic->Linv, ic->tz, b, x, ic->ty, ic->ready_b, ic->epoch, ic->tickets + 1,
+                                       ic->wait_err);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// Bounded-wait failures since the last call (0 = none); clears the flag.
+int precond_wait_status(fsd_handle* h) {
+    IChol* ic = (IChol*)h->ichol;
+    if (!ic || !ic->wait_err) return FSD_OK;
+    int v = 0;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(&v, ic->wait_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (v) {
+        FSD_CHECK_CUDA(cudaMemsetAsync(ic->wait_err, 0, sizeof(int), h->stream));
+        return FSD_ERR_DEVICE_WAIT;
+    }
+    return FSD_OK;
+}
+
 int precond_G(fsd_handle* h, const float* t, float* y) {
     const int N = h->p.N;
     cudaStream_t st = h->stream;
@@ -616,19 +815,23 @@ int precond_G(fsd_handle* h, const float* t, float* y) {
         return FSD_OK;
     }
     IChol* ic = (IChol*)h->ichol;
+    count_launch();
     k_permute<<<(6 * N + 255) / 256, 256, 0, st>>>(t, ic->ty, ic->perm, N, 1);
     const int nlev = (int)ic->lev_ptr.size() - 1;
     for (int l = 0; l < nlev; ++l) {
         const int n = ic->lev_ptr[l + 1] - ic->lev_ptr[l];
+        count_launch();
         k_fwd_level<<<(n + 127) / 128, 128, 0, st>>>(ic->lev_rows + ic->lev_ptr[l], n, ic->rowptr, ic->col, ic->diag,
                                                      ic->L, ic->Linv, ic->ty, ic->tz);
     }
     const int nblev = (int)ic->blev_ptr.size() - 1;
     for (int l = 0; l < nblev; ++l) {
         const int n = ic->blev_ptr[l + 1] - ic->blev_ptr[l];
+        count_launch();
         k_bwd_level<<<(n + 127) / 128, 128, 0, st>>>(ic->blev_rows + ic->blev_ptr[l], n, ic->rowptr, ic->col,
                                                      ic->diag, ic->tpos, ic->L, ic->Linv, ic->tz, ic->ty);
     }
+    count_launch();
     k_permute<<<(6 * N + 255) / 256, 256, 0, st>>>(ic->ty, y, ic->perm, N, -1);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;

@@ -12,10 +12,13 @@
 // device; the host polls a converged flag every few iterations.
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
+#include <cstdlib>
 
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_solver.h"
+#include "fsd_profile.h"
 
 namespace fsd {
 
@@ -46,11 +49,15 @@ __global__ void k_pc_post(const float* __restrict__ b, const float* __restrict__
 
 int precond_apply(fsd_handle* h, const float* b, float* x) {
     const int N = h->p.N;
+    ProfRegion pr(h, R_PRECOND_APPLY);
+    if (h->p.precond == FSD_PRECOND_ICHOL) return precond_apply_ichol(h, b, x);
     float* t = h->w.pc_t;
     float* y = h->w.pc_y;
+    count_launch();
     k_pc_pre<<<(6 * N + 255) / 256, 256, 0, h->stream>>>(b, t, N);
     int st = precond_G(h, t, y);
     if (st != FSD_OK) return st;
+    count_launch();
     k_pc_post<<<(11 * N + 255) / 256, 256, 0, h->stream>>>(b, y, x, N);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
@@ -281,49 +288,80 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
         // r = b - A x
         int e = saddle_multiply(h, pos, x, Ax, first);
         if (e != FSD_OK) return e;
+        count_launch();
         k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
+        count_launch();
         k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
+        count_launch();
         k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
         if (first) {
+            count_launch();
             k_multidot<<<nbl, kRedThreads, 0, st>>>(b, n, 1, b, n, part, nullptr);
+            count_launch();
             k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + 1, false, nullptr);
         }
+        count_launch();
         k_cycle_start<<<1, 1, 0, st>>>(gs, dots, (double)tol, first ? 1 : 0);
+        count_launch();
         k_scale_copy<<<vblocks, vthreads, 0, st>>>(r, V, n, dots, &gs->done);
         first = false;
-        for (int j = 0; j < m; ++j) {
+        count_launch();
+        k_export<<<1, 1, 0, st>>>(gs, gh);
+        FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+        const bool converged_at_start = gh->done != 0;
+        for (int j = 0; j < m && !converged_at_start; ++j) {
             // w = A M^-1 V_j
             e = precond_apply(h, V + (size_t)j * ld, z);
             if (e != FSD_OK) return e;
             e = saddle_multiply(h, pos, z, Ax, false);
             if (e != FSD_OK) return e;
             // CGS2 against V_0..V_j.
+            ProfRegion pk(h, R_KRYLOV);
+            count_launch();
             k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+            count_launch();
             k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, dots, false, &gs->done);
+            count_launch();
             k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, dots, Ax, n, &gs->done);
+            count_launch();
             k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+            count_launch();
             k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, w.hcol2, false, &gs->done);
+            count_launch();
             k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, w.hcol2, Ax, n, &gs->done);
+            count_launch();
             k_add_dots<<<1, 128, 0, st>>>(dots, w.hcol2, j + 1, &gs->done);
+            count_launch();
             k_multidot<<<nbl, kRedThreads, 0, st>>>(Ax, n, 1, Ax, n, part, &gs->done);
+            count_launch();
             k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + j + 1, false, &gs->done);
+            count_launch();
             k_arnoldi_update<<<1, 1, 0, st>>>(gs, dots, m);
+            count_launch();
             k_scale_copy<<<vblocks, vthreads, 0, st>>>(Ax, V + (size_t)(j + 1) * ld, n, dots + j + 1, &gs->done);
             if ((j % 4) == 3 || j == m - 1) {
+                count_launch();
                 k_export<<<1, 1, 0, st>>>(gs, gh);
                 FSD_CHECK_CUDA(cudaStreamSynchronize(st));
                 if (gh->done) break;
             }
         }
+        count_launch();
         k_export<<<1, 1, 0, st>>>(gs, gh);
         FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (getenv("FSD_DEBUG_GMRES"))
+            fprintf(stderr, "gmres cycle: j=%d total=%d resid=%.3e breakdown=%d\n", gh->j, gh->total, gh->resid,
+                    gh->breakdown);
         const int jc = gh->j;
         total = gh->total;
         if (jc > 0) {
+            count_launch();
             k_lsq<<<1, 1, 0, st>>>(gs);
+            count_launch();
             k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
             e = precond_apply(h, Ax, z);
             if (e != FSD_OK) return e;
+            count_launch();
             k_axpy<<<vblocks, vthreads, 0, st>>>(x, z, n);
         }
         if (gh->breakdown == 1) {
@@ -340,14 +378,19 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     // True residual of the returned solution.
     int e = saddle_multiply(h, pos, x, Ax, false);
     if (e != FSD_OK) return e;
+    count_launch();
     k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
+    count_launch();
     k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
+    count_launch();
     k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
     double host[2];
     FSD_CHECK_CUDA(cudaMemcpyAsync(host, dots, sizeof(double), cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaMemcpyAsync(host + 1, &gs->bnorm2, sizeof(double), cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaStreamSynchronize(st));
     const double rel = host[1] > 0 ? sqrt(host[0] / host[1]) : sqrt(host[0]);
+    const int ws = precond_wait_status(h);
+    if (ws != FSD_OK) return ws;
     if (iters) *iters = total;
     if (resid) *resid = (float)rel;
     if (!(rel == rel)) status = FSD_ERR_BREAKDOWN;

@@ -87,6 +87,8 @@ typedef struct fsd_params {
     float rlub;                  /* lubrication cutoff (4.0, Stokes.cc:1505) */
     float rp;                    /* preconditioner cutoff (2.1, Stokes.cc:1506) */
     float nlist_buffer;          /* neighbour-list skin added to the Ewald cutoff (0.4, integrate.py:83) */
+    int ichol_local_shift;       /* 1: shift only failing IC(0) pivot blocks (default); 0: double the global
+                                    relaxer and refactor, as Precondition.cu:1457-1489 */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
@@ -108,6 +110,7 @@ typedef struct fsd_solve_info {
     float ichol_relaxer;         /* relaxer the factorisation succeeded with */
     int nlist_max;               /* largest neighbour count seen */
     int status;                  /* fsd_status of that call */
+    int ichol_shifted;           /* pivot blocks that needed a local shift */
 } fsd_solve_info;
 
 /* Arguments of one time step (Stokes_StepOne, Stokes.cuh:81-108). */
@@ -134,6 +137,12 @@ const char* fsd_status_string(int status);
  * GPU. */
 int fsd_pse_setup(const fsd_params* p, fsd_pse_info* info, float* host_table, size_t n_floats);
 
+/* Reverse Cuthill-McKee ordering of an n-node graph given as 0-based CSR
+ * adjacency (rows may include self loops); perm[new] = old.  Replaces the
+ * host genrcm call of the preconditioner (rcm.cpp:1009, Precondition.cu:1009)
+ * and returns the same ordering.  Host only. */
+int fsd_rcm_order(int n, const int* rowptr, const int* col, int* perm);
+
 /* Stokes constructor + setParams + setResistanceTable + setSparseMath +
  * AllocateWorkSpaces (Stokes.cc:47-83, 118-696, 937-1063;
  * Stokes_ResistanceTable.cc:33; Stokes_SparseMath.cc:15).  All device memory
@@ -142,11 +151,22 @@ int fsd_create(const fsd_params* p, void* cuda_stream, fsd_handle** out);
 /* Stokes destructor (Stokes.cc:86-113). */
 void fsd_destroy(fsd_handle* h);
 int fsd_set_stream(fsd_handle* h, void* cuda_stream);
+/* Number of CUDA kernels this library has launched since it was loaded (no
+ * counterpart in the reference; used to report launches per step). */
+unsigned long long fsd_launch_count(void);
 /* Box update (HOOMD box_resize with shear_variant, variant.py:14-32). */
 int fsd_set_box(fsd_handle* h, float Lx, float Ly, float Lz, float xy);
 /* Stokes::setT / temperature variant value for the next step. */
 int fsd_set_temperature(fsd_handle* h, float T);
 int fsd_get_pse_info(const fsd_handle* h, fsd_pse_info* info);
+/* Per-region device timing with CUDA events (no counterpart in the reference,
+ * whose only timing is HOOMD's profiler around the whole step, Stokes.cc:1201).
+ * Regions, in order: neighbour list, preconditioner build, spread, FFT,
+ * Green, contract, real space, R_FU, preconditioner apply, Krylov vector ops,
+ * Lanczos vector ops, wave-space noise, other lubrication, integration.
+ * fsd_profile_read fills ms[] and counts[] (n >= 14) and optionally resets. */
+int fsd_profile_enable(fsd_handle* h, int on);
+int fsd_profile_read(fsd_handle* h, double* ms, long long* counts, int n, int reset);
 int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info);
 /* Copy the real-space Ewald table (2*(ewald_n+1) float4) to host memory. */
 int fsd_get_ewald_table(const fsd_handle* h, float* host_table, size_t n_floats);

@@ -32,6 +32,11 @@ def resistance_table():
 
 
 # ----------------------------------------------------------------- box maths
+def xyz(pos):
+    """Coordinates (N,3) of float4 or float3 positions."""
+    return np.asarray(pos, np.float64)[:, :3]
+
+
 def min_image(d, L, xy):
     """HOOMD BoxDim::minImage, device path (rint), z then y then x."""
     d = np.array(d, np.float64, copy=True)
@@ -45,9 +50,23 @@ def min_image(d, L, xy):
     return d
 
 
+def min_image32(d, L, xy):
+    """min_image in single precision, as the kernels evaluate pair separations."""
+    d = np.array(d, F32, copy=True)
+    Lx, Ly, Lz = (F32(v) for v in L)
+    xy = F32(xy)
+    img = np.rint(d[..., 2] * (F32(1) / Lz))
+    d[..., 2] -= Lz * img
+    img = np.rint(d[..., 1] * (F32(1) / Ly))
+    d[..., 0] -= Ly * xy * img
+    d[..., 1] -= Ly * img
+    d[..., 0] -= Lx * np.rint(d[..., 0] * (F32(1) / Lx))
+    return d
+
+
 def make_fraction32(pos, L, xy):
     """HOOMD BoxDim::makeFraction in single precision."""
-    p = np.asarray(pos, F32)
+    p = np.asarray(pos, F32)[:, :3]
     Lx, Ly, Lz = (F32(v) for v in L)
     d = p + np.array([Lx / F32(2), Ly / F32(2), Lz / F32(2)], F32)
     d[:, 0] = d[:, 0] - F32(xy) * p[:, 1]
@@ -90,7 +109,7 @@ def hash_seed(seed: int) -> int:
 # ------------------------------------------------------------ neighbour list
 def neighbor_list(pos, L, xy, rlist):
     """All j != i with |minImage(x_i - x_j)| < rlist, each row sorted."""
-    pos = np.asarray(pos, np.float64)
+    pos = xyz(pos)
     N = len(pos)
     rows = []
     r2 = rlist * rlist
@@ -237,7 +256,7 @@ def wave_space(pos, F, C, L, xy, gp, xi, pi_typo=True):
     expfac = 2.0 * xisq / eta
     idx = stencil(pos, L, xy, Nxyz, P)
     pg = node_positions(idx, L, xy, h)
-    r = min_image(pg - np.asarray(pos, np.float64)[:, None, :], L, xy)
+    r = min_image(pg - xyz(pos)[:, None, :], L, xy)
     wgt = prefac * np.exp(-expfac * np.einsum("npk,npk->np", r, r))
     flat = (idx[..., 0] * Nxyz[1] + idx[..., 1]) * Nxyz[2] + idx[..., 2]
     G = Nxyz[0] * Nxyz[1] * Nxyz[2]
@@ -266,7 +285,7 @@ def real_space(pos, F, C, L, xy, rows, table, self_x, self_y, ewald_cut, ewald_n
 
     Returns u (N,3) and D (N,3,3) in the real-space convention (D[a,b] gets
     R_a F_b-type terms)."""
-    pos = np.asarray(pos, np.float64)
+    pos = xyz(pos)
     N = len(pos)
     u = self_x * F.copy()
     D = self_y * (C - 4.0 * np.transpose(C, (0, 2, 1)))
@@ -358,16 +377,21 @@ def res_interp(dist, first, count, tdist, tvals, mode="lub"):
 
 
 def _lub_pairs(pos, L, xy, rows, cut2, positive=False):
-    pos = np.asarray(pos, np.float64)
+    """Pairs from i to j within the cutoff.  Separation, squared distance and
+    distance are single precision as in the kernels (Lubrication.cu:126-141):
+    near contact the tabulated functions are steep in the gap, so the gap's
+    float32 resolution is part of the result."""
+    pos = np.asarray(pos, F32)[:, :3]
     i, j = pair_arrays(rows)
-    R = min_image(pos[j] - pos[i], L, xy)  # from i to j
-    d2 = np.einsum("ij,ij->i", R, R)
-    keep = d2 < cut2
+    R = min_image32(pos[j] - pos[i], L, xy)  # from i to j
+    d2 = R[:, 0] * R[:, 0] + R[:, 1] * R[:, 1] + R[:, 2] * R[:, 2]
+    keep = d2 < F32(cut2)
     if positive:
         keep &= d2 > 0
     i, j, R, d2 = i[keep], j[keep], R[keep], d2[keep]
     dist = np.sqrt(d2)
-    return i, j, R / dist[:, None], dist
+    r = (R / dist[:, None]).astype(np.float64)
+    return i, j, r, dist
 
 
 def strain_tensor(shear_rate, N, ori=None, b2mask=None, B2=0.0):
@@ -492,7 +516,7 @@ class Problem:
 
     def __init__(self, pos, L, xy=0.0, xi=0.5, error=1e-3, max_strain=0.5, table=None, rlub=4.0, rp=2.1,
                  pi_typo=True):
-        self.pos = np.asarray(pos, np.float64)[:, :3]
+        self.pos = xyz(pos)
         self.N = len(self.pos)
         self.L = tuple(float(v) for v in L)
         self.xy = float(xy)
@@ -545,8 +569,8 @@ class Problem:
 
 def rcm(rows):
     """Reverse Cuthill-McKee as genrcm (rcm.cpp:1009): pseudo-peripheral root,
-    breadth-first with new neighbours by increasing degree, reversed per
-    component.  rows: adjacency per node (self loops allowed).  perm[new] = old."""
+    breadth-first with new neighbours (all but the first) by increasing degree,
+    reversed per component.  rows: adjacency per node (self loops allowed).  perm[new] = old."""
     n = len(rows)
     mask = np.ones(n, bool)
     perm = []
@@ -606,7 +630,10 @@ def rcm(rows):
                 if mask[u]:
                     mask[u] = False
                     new.append(int(u))
-            new.sort(key=lambda x: deg[x])  # stable
+            # Stable insertion by degree over all but the first new neighbour:
+            # the reference's loop (rcm.cpp, `while ( fnbr < l )`) never moves
+            # the first one.
+            new = new[:1] + sorted(new[1:], key=lambda x: deg[x])
             comp.extend(new)
         perm.extend(comp[::-1])
     return np.array(perm, np.int64)
@@ -616,7 +643,7 @@ def pruned_rfu_dense(pos, L, xy, rows, tdist, tvals, rp=2.1, relaxer=1.0):
     """Pruned R_FU plus relaxer * {1,1,1,4/3,4/3,4/3} on the diagonal, dense 6N x 6N
     (Precondition_RFU_kernel, Precondition.cu:530-836; AddIdentity,
     Helper_Precondition.cu:535-580).  Also returns the particle graph rows."""
-    pos = np.asarray(pos, np.float64)
+    pos = xyz(pos)
     N = len(pos)
     prow = []
     for i in range(N):
@@ -628,11 +655,12 @@ def pruned_rfu_dense(pos, L, xy, rows, tdist, tvals, rp=2.1, relaxer=1.0):
         for j in prow[i]:
             if j == i:
                 continue
-            R = min_image(pos[j] - pos[i], L, xy)
-            dist = np.sqrt(R @ R)
+            R = min_image32((pos[j] - pos[i]).astype(F32)[None], L, xy)[0]
+            dist = np.sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2])
+            R = R.astype(np.float64)
             c = res_interp(np.array([dist]), 0, 10, tdist, tvals, mode="precond")[0]
             XA11, XA12, YA11, YA12, YB11, YB12, XC11, XC12, YC11, YC12 = c
-            r = (R.astype(F32) / F32(dist)).astype(np.float64)
+            r = R / dist
             rr = np.outer(r, r)
             Im = np.eye(3) - rr
             eps = np.array([[0, r[2], -r[1]], [-r[2], 0, r[0]], [r[1], -r[0], 0]])
@@ -663,6 +691,7 @@ def ichol0_dense(A, pattern):
         L[col, k] /= L[k, k]
         for j in col:
             rows_ = col[col >= j]
+            rows_ = rows_[pattern[rows_, j]]  # zero fill: update only entries of the pattern
             L[rows_, j] -= L[rows_, k] * L[j, k]
     return L
 
@@ -675,3 +704,109 @@ def saddle_precond(b, G, N):
     x[: 6 * N] = b[: 6 * N] - y
     x[11 * N:] = y
     return x
+
+
+# ------------------------------------------------------------ forces, motion
+def pair_force(pos, L, xy, rows, ndsr=0.1, k_n=1e4, kappa=20.0, beta=0.0, epsq=1e-5, T_ext=0.0):
+    """Repulsion + van der Waals + collision force and z torque (Stokes_SetForce_manually_kernel,
+    Helper_Stokes.cu:65-172)."""
+    pos = xyz(pos)
+    N = len(pos)
+    i, j = pair_arrays(rows)
+    R = min_image(pos[j] - pos[i], L, xy)
+    dist = np.sqrt(np.einsum("ij,ij->i", R, R))
+    rcol = 2.0 + np.sqrt(epsq)
+    F0 = 1.0 / ndsr
+    H = F0 * beta
+    gap = dist - rcol
+    mag = np.zeros_like(dist)
+    m1 = (gap >= 0) & (dist <= 2.0 + 10.0 / kappa)
+    mag[m1] = H / (12.0 * (gap[m1] ** 2 + epsq)) - F0 * np.exp(-kappa * gap[m1])
+    m2 = gap < 0
+    mag[m2] = H / (12.0 * epsq) - F0 - k_n * np.abs(gap[m2])
+    out = np.zeros((N, 6))
+    np.add.at(out[:, :3], i, mag[:, None] * R / dist[:, None])
+    out[:, 5] = T_ext
+    return out.ravel()
+
+
+def strain_rhs(shear_rate, N, ori=None, b2mask=None, B2=0.0):
+    """Imposed strain minus the active strain in the stresslet rows of the
+    right-hand side (Integrator_AddStrainRate_kernel, Helper_Integrator.cu:114-158)."""
+    b = np.zeros(17 * N)
+    e = b[6 * N: 11 * N].reshape(N, 5)
+    e[:, 1] += shear_rate
+    if B2 != 0.0 and ori is not None:
+        p = np.asarray(ori, np.float64)
+        m = np.ones(N) if b2mask is None else np.asarray(b2mask, np.float64)
+        b2 = -0.6 * B2 * m
+        e[:, 0] -= b2 * (p[:, 0] ** 2 - p[:, 2] ** 2)
+        e[:, 1] -= b2 * 2 * p[:, 0] * p[:, 1]
+        e[:, 2] -= b2 * 2 * p[:, 0] * p[:, 2]
+        e[:, 3] -= b2 * 2 * p[:, 1] * p[:, 2]
+        e[:, 4] -= b2 * (p[:, 1] ** 2 - p[:, 2] ** 2)
+    return b
+
+
+def wrap(p, img, L, xy):
+    """HOOMD BoxDim::wrap with an xy tilt: one image shift per axis, x then y then z."""
+    p = p.copy()
+    img = img.copy()
+    Lx, Ly, Lz = L
+    tilt = xy * p[:, 1]
+    hi = p[:, 0] >= Lx / 2 + tilt
+    lo = p[:, 0] < -Lx / 2 + tilt
+    p[hi, 0] -= Lx
+    img[hi, 0] += 1
+    p[lo & ~hi, 0] += Lx
+    img[lo & ~hi, 0] -= 1
+    hi = p[:, 1] >= Ly / 2
+    lo = (p[:, 1] < -Ly / 2) & ~hi
+    p[hi, 1] -= Ly
+    p[hi, 0] -= Ly * xy
+    img[hi, 1] += 1
+    p[lo, 1] += Ly
+    p[lo, 0] += Ly * xy
+    img[lo, 1] -= 1
+    hi = p[:, 2] >= Lz / 2
+    lo = (p[:, 2] < -Lz / 2) & ~hi
+    p[hi, 2] -= Lz
+    img[hi, 2] += 1
+    p[lo, 2] += Lz
+    img[lo, 2] -= 1
+    return p, img
+
+
+def euler_shear(pos, ori, pos_gb, vel, image, L, xy, dt, shear_rate, B1=0.0, b1mask=None, noise=None):
+    """Explicit Euler with simple shear and director rotation
+    (Integrator_ExplicitEuler_Shear_kernel, Integrator.cu:126-228)."""
+    pos = xyz(pos)
+    N = len(pos)
+    V = np.asarray(vel, np.float64)[: 6 * N].reshape(N, 6)
+    p = pos[:, :3].copy()
+    v = V[:, :3].copy()
+    w = V[:, 3:].copy()
+    v[:, 0] += shear_rate * p[:, 1]
+    w[:, 2] -= shear_rate / 2.0
+    if noise is not None:
+        w += np.asarray(noise, np.float64)
+    aw = np.linalg.norm(w, axis=1)
+    rot = aw > 1e-6
+    q0 = np.ones(N)
+    qv = np.zeros((N, 3))
+    ang = aw * dt
+    q0[rot] = np.cos(ang[rot] / 2)
+    qv[rot] = w[rot] / aw[rot, None] * np.sin(ang[rot] / 2)[:, None]
+    pv = np.asarray(ori, np.float64)
+    m = np.ones(N) if b1mask is None else np.asarray(b1mask, np.float64)
+    v -= (-2.0 / 3.0 * B1 * m)[:, None] * pv
+    gb = np.asarray(pos_gb, np.float64).copy()
+    gb[:, 0] += (v[:, 0] - shear_rate * p[:, 1] + shear_rate * gb[:, 1]) * dt
+    gb[:, 1] += v[:, 1] * dt
+    gb[:, 2] += v[:, 2] * dt
+    p, img = wrap(p + v * dt, np.asarray(image, np.int64), L, xy)
+    qq = np.einsum("ij,ij->i", qv, qv)
+    qp = np.einsum("ij,ij->i", qv, pv)
+    pn = (q0 * q0 - qq)[:, None] * pv + 2 * qp[:, None] * qv + 2 * q0[:, None] * np.cross(qv, pv)
+    pn /= np.linalg.norm(pn, axis=1, keepdims=True)
+    return p, pn, gb, img

@@ -100,12 +100,26 @@ def d2we(delu8):
     return o.reshape(N, 8)
 
 
+def _table_like_reference(tdist, tvals):
+    """The reference's table buffers: values in a 32000-float array zero past
+    entry 22000 (Stokes_ResistanceTable.cc:46-47, HOOMD zero-fills GPUArrays)
+    and distances in an allocation padded to 256 bytes.  Pairs with
+    3.9978 <= r < 4 index one row past the table (Lubrication.cu:193-200) and
+    read those zeros."""
+    d = np.zeros(1024, np.float32)
+    d[:1000] = np.asarray(tdist, np.float32).ravel()
+    v = np.zeros(32000, np.float32)
+    v[:22000] = np.asarray(tvals, np.float32).ravel()
+    return d, v
+
+
 def _lub_common(pos4, nlist_rows, L, xy):
     nn, flat, head = _nl(nlist_rows)
     return np.ascontiguousarray(pos4, np.float32), nn, flat, head
 
 
 def rfu(pos4, U6, nlist_rows, L, xy, tdist, tvals, rlub=4.0, tmin=1e-4, tdr=0.004305):
+    tdist, tvals = _table_like_reference(tdist, tvals)
     N = len(pos4)
     pos, nn, flat, head = _lub_common(pos4, nlist_rows, L, xy)
     F6 = np.zeros(6 * N, np.float32)
@@ -116,6 +130,7 @@ def rfu(pos4, U6, nlist_rows, L, xy, tdist, tvals, rlub=4.0, tmin=1e-4, tdr=0.00
 
 def rfe(pos4, shear_rate, nlist_rows, L, xy, tdist, tvals, ori=None, b2mask=None, B2=0.0, rlub=4.0, tmin=1e-4,
         tdr=0.004305):
+    tdist, tvals = _table_like_reference(tdist, tvals)
     N = len(pos4)
     pos, nn, flat, head = _lub_common(pos4, nlist_rows, L, xy)
     ori = np.zeros((N, 3), np.float32) if ori is None else np.ascontiguousarray(ori, np.float32)
@@ -127,6 +142,7 @@ def rfe(pos4, shear_rate, nlist_rows, L, xy, tdist, tvals, ori=None, b2mask=None
 
 
 def rsu(pos4, U6, nlist_rows, L, xy, tdist, tvals, rlub=4.0, tmin=1e-4, tdr=0.004305):
+    tdist, tvals = _table_like_reference(tdist, tvals)
     N = len(pos4)
     pos, nn, flat, head = _lub_common(pos4, nlist_rows, L, xy)
     S = np.zeros(5 * N, np.float32)
@@ -136,6 +152,7 @@ def rsu(pos4, U6, nlist_rows, L, xy, tdist, tvals, rlub=4.0, tmin=1e-4, tdr=0.00
 
 
 def rse(pos4, shear_rate, nlist_rows, L, xy, tdist, tvals, ori=None, b2mask=None, B2=0.0, tmin=1e-4, tdr=0.004305):
+    tdist, tvals = _table_like_reference(tdist, tvals)
     N = len(pos4)
     pos, nn, flat, head = _lub_common(pos4, nlist_rows, L, xy)
     ori = np.zeros((N, 3), np.float32) if ori is None else np.ascontiguousarray(ori, np.float32)
@@ -159,6 +176,7 @@ def pruned_nlist(pos4, nlist_rows, L, xy, rp=2.1):
 
 
 def precond_coo(pos4, nlist_rows, L, xy, tdist, tvals, rp=2.1, tmin=1e-4, tdr=0.004305):
+    tdist, tvals = _table_like_reference(tdist, tvals)
     """Pruned R_FU in COO as the reference assembles it (before the identity shift)."""
     N = len(pos4)
     rows, nless = pruned_nlist(pos4, nlist_rows, L, xy, rp)
