@@ -147,7 +147,7 @@ def run_fsd(args, ws, rank, local):
     N, phi = args.N, args.phi
     pos, L = suspension(N, phi, seed=1 + rank)
     s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=1 + rank, error=1e-3, solver_tol=1e-4,
-            lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=args.precond, period=0, gmres_max_iter=1000)
+            lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=args.precond, period=0, gmres_max_iter=3000, gmres_restart=200)
     info = s.pse_info()
     shear_rate = 1.0
     p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
@@ -258,7 +258,7 @@ def run_fsd(args, ws, rank, local):
         "vs_baseline": None, "dtype": "f32 (FP64 Krylov/Lanczos scalars and IC pivots)",
         "data": "synthetic: seeded random sequential addition + overlap relaxation, min gap 1e-3",
         "config": {"workload": f"full FSD step, N={N}, phi={phi}, shear 1.0, kT 1, dt 1e-4, Ewald 1e-3, "
-                               f"GMRES 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
+                               f"GMRES(200) 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
                    "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
                    "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
                    "parallelism": f"replicas x{ws}"},

@@ -38,7 +38,7 @@ class fsd_params(C.Structure):
         ("gmres_restart", C.c_int), ("gmres_max_iter", C.c_int), ("lanczos_max", C.c_int),
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
-        ("ichol_local_shift", C.c_int),
+        ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
     ]
 
 
@@ -59,6 +59,7 @@ class fsd_solve_info(C.Structure):
         ("lanczos_ff_err", C.c_float), ("lanczos_nf_err", C.c_float),
         ("ichol_attempts", C.c_int), ("ichol_relaxer", C.c_float),
         ("nlist_max", C.c_int), ("status", C.c_int), ("ichol_shifted", C.c_int),
+        ("ichol_gain", C.c_float),
     ]
 
 

@@ -166,6 +166,7 @@ void fsd_default_params(fsd_params* p) {
     p->rp = 2.1f;
     p->nlist_buffer = 0.4f;
     p->ichol_local_shift = 1;
+    p->ichol_gain_limit = 100.0f;
 }
 
 const char* fsd_status_string(int status) {

@@ -5,7 +5,7 @@
 
 namespace fsd {
 
-constexpr int kMaxRestart = 100;
+constexpr int kMaxRestart = 400;
 constexpr int kPrunedCap = 32;  // pruned (r < rp) neighbours per particle, self included
 
 int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin);

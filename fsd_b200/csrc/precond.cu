@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "fsd_brownian.h"
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_solver.h"
@@ -51,6 +52,8 @@ struct IChol {
     unsigned* ready_b = nullptr; // per-row completion epoch, backward solve
     unsigned* tickets = nullptr; // row tickets [forward, backward]
     int* wait_err = nullptr;     // set when a bounded wait gave up
+    float* gv = nullptr;         // gain estimate: two 17N saddle vectors
+    double* gnrm = nullptr;      // device squared norm of the last iterate
     unsigned epoch = 0;
     int nnzb_cap = 0;
     // host
@@ -58,6 +61,7 @@ struct IChol {
     std::vector<unsigned> h_pn, h_plist;
     int nnzb = 0;
     int* h_fail = nullptr;
+    double* h_gnrm = nullptr;
 };
 
 // ------------------------------------------------------------ pruned graph
@@ -179,11 +183,19 @@ __global__ void k_assemble(const float4* __restrict__ pos, int N, Box b, const u
 //   L_pq = (B_pq - sum_{k<q} L_pk L_qk^T) L_qq^-T   for q < p in the pattern
 //   L_pp = chol(B_pp - sum_{k<p} L_pk L_pk^T)
 // FP64 throughout; a non-positive or non-finite pivot sets *fail.
-__device__ void chol6(double* A, bool* ok) {
+// Cholesky of a 6x6 pivot block.  A pivot must keep at least kPivotFloor of
+// the assembled diagonal entry `ref` it came from; smaller (or non-positive)
+// pivots mark the block as failed, since a nearly singular pivot would give
+// the preconditioner an enormous gain that swamps the FP32 Krylov basis.
+constexpr double kPivotFloor = 1e-3;
+constexpr int kGainIters = 8;  // power-iteration steps of the gain estimate
+
+__device__ void chol6(double* A, bool* ok, const float* ref) {
     for (int j = 0; j < 6; ++j) {
         double d = A[j * 6 + j];
         for (int k = 0; k < j; ++k) d -= A[j * 6 + k] * A[j * 6 + k];
-        if (!(d > 0.0)) {
+        const double floor_j = ref ? kPivotFloor * fabs((double)ref[j * 7]) : 0.0;
+        if (!(d > floor_j) || !(d > 0.0)) {
             *ok = false;
             d = 1.0;
         }
@@ -249,7 +261,7 @@ __global__ void k_factor_level(const int* __restrict__ rows, int nrows, const in
             bool ok = true;
             double keep[36];
             for (int k = 0; k < 36; ++k) keep[k] = acc[k];
-            chol6(acc, &ok);
+            chol6(acc, &ok, B);
             // Pivot-local shift: a pivot block that is not positive definite
             // gets tau * {1,1,1,4/3,4/3,4/3} added, tau doubling from
             // `shift0`, instead of shifting the whole matrix.
@@ -259,7 +271,7 @@ __global__ void k_factor_level(const int* __restrict__ rows, int nrows, const in
                     for (int k = 0; k < 36; ++k) acc[k] = keep[k];
                     for (int d = 0; d < 6; ++d) acc[d * 7] += tau * ((d < 3) ? 1.0 : (double)1.33333333f);
                     ok = true;
-                    chol6(acc, &ok);
+                    chol6(acc, &ok, B);
                 }
                 if (ok) atomicAdd(shifted, 1);
             }
@@ -625,7 +637,10 @@ int precond_alloc(fsd_handle* h) {
     FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_f, 0, sizeof(unsigned) * N, h->stream));
     FSD_CHECK_CUDA(cudaMemsetAsync(ic->ready_b, 0, sizeof(unsigned) * N, h->stream));
     FSD_CHECK_CUDA(cudaMemsetAsync(ic->wait_err, 0, sizeof(int), h->stream));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->gv, sizeof(float) * 34 * (size_t)N));
+    FSD_CHECK_CUDA(cudaMalloc(&ic->gnrm, sizeof(double)));
     FSD_CHECK_CUDA(cudaMallocHost(&ic->h_fail, sizeof(int) * 2));
+    FSD_CHECK_CUDA(cudaMallocHost(&ic->h_gnrm, sizeof(double)));
     return FSD_OK;
 }
 
@@ -634,12 +649,51 @@ void precond_free(fsd_handle* h) {
     if (!ic) return;
     void* ptrs[] = {ic->pn, ic->plist, ic->p_over, ic->blocks, ic->perm, ic->rowptr, ic->col, ic->src, ic->diag,
                     ic->tpos, ic->L, ic->Linv, ic->fail, ic->lev_rows, ic->blev_rows, ic->ty, ic->tz,
-                    ic->ready_f, ic->ready_b, ic->tickets, ic->wait_err};
+                    ic->ready_f, ic->ready_b, ic->tickets, ic->wait_err, ic->gv, ic->gnrm};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (ic->h_fail) cudaFreeHost(ic->h_fail);
+    if (ic->h_gnrm) cudaFreeHost(ic->h_gnrm);
     delete ic;
     h->ichol = nullptr;
+}
+
+// y = x / sqrt(*nrm) (a zero norm leaves y = x).
+__global__ void k_normalize(float* __restrict__ y, const float* __restrict__ x, const double* __restrict__ nrm,
+                            size_t n) {
+    const double s = *nrm;
+    const float f = s > 0.0 ? (float)(1.0 / sqrt(s)) : 1.0f;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        y[k] = f * x[k];
+}
+
+// Power-iteration estimate of lambda_max(G) for the current factor.  With the
+// saddle input b = [0; u] the preconditioner returns G u in its last 6N
+// entries, so the iteration runs on the fused solve kernels unchanged.
+// The iteration count is small: a factor that has lost stability has a gain
+// many orders of magnitude above 1/relaxer, which a few steps expose.
+double ichol_gain(fsd_handle* h, int iters) {
+    IChol* ic = (IChol*)h->ichol;
+    const int N = h->p.N;
+    const size_t n6 = 6 * (size_t)N, off = 11 * (size_t)N;
+    cudaStream_t st = h->stream;
+    float* b = ic->gv;
+    float* x = ic->gv + 17 * (size_t)N;
+    const int nb = (int)std::min<size_t>(4 * 148, (n6 + 255) / 256);
+    if (cudaMemsetAsync(b, 0, sizeof(float) * off, st) != cudaSuccess) return -1.0;
+    gaussian(h, b + off, n6, 0, kStreamGain, 1.0f);
+    dot_device(h, b + off, b + off, n6, ic->gnrm);
+    count_launch();
+    k_normalize<<<nb, 256, 0, st>>>(b + off, b + off, ic->gnrm, n6);
+    for (int it = 0; it < iters; ++it) {
+        if (precond_apply_ichol(h, b, x) != FSD_OK) return -1.0;
+        dot_device(h, x + off, x + off, n6, ic->gnrm);
+        count_launch();
+        k_normalize<<<nb, 256, 0, st>>>(b + off, x + off, ic->gnrm, n6);
+    }
+    if (cudaMemcpyAsync(ic->h_gnrm, ic->gnrm, sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -1.0;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -1.0;
+    return sqrt(*ic->h_gnrm);
 }
 
 // Build the pattern, ordering and levels from the pruned graph (host), then
@@ -759,9 +813,23 @@ int precond_build(fsd_handle* h, const float4* pos) {
         h->info.ichol_attempts = attempt + 1;
         h->info.ichol_shifted = ic->h_fail[1];
         if (!ic->h_fail[0]) {
-            h->info.ichol_relaxer = h->ichol_relaxer;
-            h->pc_valid = true;
-            return FSD_OK;
+            // Stability check: IC(0) of the pruned lubrication matrix can be
+            // positive definite yet nearly singular (dropped fill around
+            // clusters of touching spheres); its inverse then amplifies some
+            // directions by many orders of magnitude and GMRES stagnates.
+            double gain = 0.0;
+            if (h->p.ichol_gain_limit > 0.f) {
+                gain = ichol_gain(h, kGainIters);
+                if (gain < 0.0) return FSD_ERR_CUDA;
+                const int ws = precond_wait_status(h);
+                if (ws != FSD_OK) return ws;
+            }
+            h->info.ichol_gain = (float)gain;
+            if (h->p.ichol_gain_limit <= 0.f || gain * h->ichol_relaxer <= h->p.ichol_gain_limit) {
+                h->info.ichol_relaxer = h->ichol_relaxer;
+                h->pc_valid = true;
+                return FSD_OK;
+            }
         }
         h->ichol_relaxer *= 2.0f;
     }

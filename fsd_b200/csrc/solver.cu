@@ -114,7 +114,7 @@ __global__ void k_finish_dots(const double* part, int nb, int nv, double* out, b
 __global__ void k_multiaxpy(const float* __restrict__ V, size_t ld, int nv, const double* __restrict__ c, float* w,
                             size_t n, const int* done) {
     if (done && *done) return;
-    __shared__ float cs[128];
+    __shared__ float cs[kMaxRestart + 1];
     for (int i = threadIdx.x; i < nv; i += blockDim.x) cs[i] = (float)c[i];
     __syncthreads();
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
@@ -127,7 +127,7 @@ __global__ void k_multiaxpy(const float* __restrict__ V, size_t ld, int nv, cons
 // y = sum_i c[i] V_i.
 __global__ void k_combine(const float* __restrict__ V, size_t ld, int nv, const double* __restrict__ c,
                           float* __restrict__ y, size_t n) {
-    __shared__ float cs[128];
+    __shared__ float cs[kMaxRestart + 1];
     for (int i = threadIdx.x; i < nv; i += blockDim.x) cs[i] = (float)c[i];
     __syncthreads();
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
@@ -163,6 +163,8 @@ __global__ void k_add_dots(double* a, const double* b, int n, const int* done) {
 
 // --------------------------------------------------------- Arnoldi control
 // State (FP64) for one restart cycle.
+constexpr int kConfirmPasses = 3;  // true-residual confirmations per solve
+
 struct GmresState {
     double H[kMaxRestart + 1][kMaxRestart];  // column-major by iteration: H[row][col]
     double cs[kMaxRestart], sn[kMaxRestart];
@@ -283,10 +285,106 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     int total = 0;
     bool first = true;
     int status = FSD_OK;
-    // ||b||^2 into dots[1] (first cycle only).
-    for (;;) {
-        // r = b - A x
-        int e = saddle_multiply(h, pos, x, Ax, first);
+    double rel = 0.0;
+    // The Arnoldi residual estimate drifts from the true residual once the
+    // FP32 basis loses orthogonality; a solve whose true residual is still
+    // above tol restarts from it (at most kConfirmPasses times).
+    for (int pass = 0; pass < kConfirmPasses; ++pass) {
+        status = FSD_OK;
+        // ||b||^2 into dots[1] (first cycle only).
+        for (;;) {
+            // r = b - A x
+            int e = saddle_multiply(h, pos, x, Ax, first);
+            if (e != FSD_OK) return e;
+            count_launch();
+            k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
+            count_launch();
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
+            count_launch();
+            k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
+            if (first) {
+                count_launch();
+                k_multidot<<<nbl, kRedThreads, 0, st>>>(b, n, 1, b, n, part, nullptr);
+                count_launch();
+                k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + 1, false, nullptr);
+            }
+            count_launch();
+            k_cycle_start<<<1, 1, 0, st>>>(gs, dots, (double)tol, first ? 1 : 0);
+            count_launch();
+            k_scale_copy<<<vblocks, vthreads, 0, st>>>(r, V, n, dots, &gs->done);
+            first = false;
+            count_launch();
+            k_export<<<1, 1, 0, st>>>(gs, gh);
+            FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+            const bool converged_at_start = gh->done != 0;
+            for (int j = 0; j < m && !converged_at_start; ++j) {
+                // w = A M^-1 V_j
+                e = precond_apply(h, V + (size_t)j * ld, z);
+                if (e != FSD_OK) return e;
+                e = saddle_multiply(h, pos, z, Ax, false);
+                if (e != FSD_OK) return e;
+                // CGS2 against V_0..V_j.
+                ProfRegion pk(h, R_KRYLOV);
+                count_launch();
+                k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+                count_launch();
+                k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, dots, false, &gs->done);
+                count_launch();
+                k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, dots, Ax, n, &gs->done);
+                count_launch();
+                k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+                count_launch();
+                k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, w.hcol2, false, &gs->done);
+                count_launch();
+                k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, w.hcol2, Ax, n, &gs->done);
+                count_launch();
+                k_add_dots<<<1, 128, 0, st>>>(dots, w.hcol2, j + 1, &gs->done);
+                count_launch();
+                k_multidot<<<nbl, kRedThreads, 0, st>>>(Ax, n, 1, Ax, n, part, &gs->done);
+                count_launch();
+                k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + j + 1, false, &gs->done);
+                count_launch();
+                k_arnoldi_update<<<1, 1, 0, st>>>(gs, dots, m);
+                count_launch();
+                k_scale_copy<<<vblocks, vthreads, 0, st>>>(Ax, V + (size_t)(j + 1) * ld, n, dots + j + 1, &gs->done);
+                if ((j % 4) == 3 || j == m - 1) {
+                    count_launch();
+                    k_export<<<1, 1, 0, st>>>(gs, gh);
+                    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+                    if (gh->done) break;
+                }
+            }
+            count_launch();
+            k_export<<<1, 1, 0, st>>>(gs, gh);
+            FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+            if (getenv("FSD_DEBUG_GMRES"))
+                fprintf(stderr, "gmres cycle: j=%d total=%d resid=%.3e breakdown=%d\n", gh->j, gh->total, gh->resid,
+                        gh->breakdown);
+            const int jc = gh->j;
+            total = gh->total;
+            if (jc > 0) {
+                count_launch();
+                k_lsq<<<1, 1, 0, st>>>(gs);
+                count_launch();
+                k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
+                e = precond_apply(h, Ax, z);
+                if (e != FSD_OK) return e;
+                count_launch();
+                k_axpy<<<vblocks, vthreads, 0, st>>>(x, z, n);
+            }
+            if (gh->breakdown == 1) {
+                status = FSD_ERR_BREAKDOWN;
+                break;
+            }
+            if (gh->resid <= tol && jc < m) break;  // converged inside the cycle; confirm below
+            if (gh->resid <= tol) break;
+            if (total >= maxit) {
+                status = FSD_ERR_GMRES_MAXIT;
+                break;
+            }
+        }
+        // True residual of the returned solution.
+        int e = saddle_multiply(h, pos, x, Ax, false);
         if (e != FSD_OK) return e;
         count_launch();
         k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
@@ -294,106 +392,19 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
         k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
         count_launch();
         k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
-        if (first) {
-            count_launch();
-            k_multidot<<<nbl, kRedThreads, 0, st>>>(b, n, 1, b, n, part, nullptr);
-            count_launch();
-            k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + 1, false, nullptr);
-        }
-        count_launch();
-        k_cycle_start<<<1, 1, 0, st>>>(gs, dots, (double)tol, first ? 1 : 0);
-        count_launch();
-        k_scale_copy<<<vblocks, vthreads, 0, st>>>(r, V, n, dots, &gs->done);
-        first = false;
-        count_launch();
-        k_export<<<1, 1, 0, st>>>(gs, gh);
+        double host[2];
+        FSD_CHECK_CUDA(cudaMemcpyAsync(host, dots, sizeof(double), cudaMemcpyDeviceToHost, st));
+        FSD_CHECK_CUDA(cudaMemcpyAsync(host + 1, &gs->bnorm2, sizeof(double), cudaMemcpyDeviceToHost, st));
         FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-        const bool converged_at_start = gh->done != 0;
-        for (int j = 0; j < m && !converged_at_start; ++j) {
-            // w = A M^-1 V_j
-            e = precond_apply(h, V + (size_t)j * ld, z);
-            if (e != FSD_OK) return e;
-            e = saddle_multiply(h, pos, z, Ax, false);
-            if (e != FSD_OK) return e;
-            // CGS2 against V_0..V_j.
-            ProfRegion pk(h, R_KRYLOV);
-            count_launch();
-            k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
-            count_launch();
-            k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, dots, false, &gs->done);
-            count_launch();
-            k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, dots, Ax, n, &gs->done);
-            count_launch();
-            k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
-            count_launch();
-            k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, w.hcol2, false, &gs->done);
-            count_launch();
-            k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, w.hcol2, Ax, n, &gs->done);
-            count_launch();
-            k_add_dots<<<1, 128, 0, st>>>(dots, w.hcol2, j + 1, &gs->done);
-            count_launch();
-            k_multidot<<<nbl, kRedThreads, 0, st>>>(Ax, n, 1, Ax, n, part, &gs->done);
-            count_launch();
-            k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots + j + 1, false, &gs->done);
-            count_launch();
-            k_arnoldi_update<<<1, 1, 0, st>>>(gs, dots, m);
-            count_launch();
-            k_scale_copy<<<vblocks, vthreads, 0, st>>>(Ax, V + (size_t)(j + 1) * ld, n, dots + j + 1, &gs->done);
-            if ((j % 4) == 3 || j == m - 1) {
-                count_launch();
-                k_export<<<1, 1, 0, st>>>(gs, gh);
-                FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-                if (gh->done) break;
-            }
-        }
-        count_launch();
-        k_export<<<1, 1, 0, st>>>(gs, gh);
-        FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-        if (getenv("FSD_DEBUG_GMRES"))
-            fprintf(stderr, "gmres cycle: j=%d total=%d resid=%.3e breakdown=%d\n", gh->j, gh->total, gh->resid,
-                    gh->breakdown);
-        const int jc = gh->j;
-        total = gh->total;
-        if (jc > 0) {
-            count_launch();
-            k_lsq<<<1, 1, 0, st>>>(gs);
-            count_launch();
-            k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
-            e = precond_apply(h, Ax, z);
-            if (e != FSD_OK) return e;
-            count_launch();
-            k_axpy<<<vblocks, vthreads, 0, st>>>(x, z, n);
-        }
-        if (gh->breakdown == 1) {
-            status = FSD_ERR_BREAKDOWN;
-            break;
-        }
-        if (gh->resid <= tol && jc < m) break;  // converged inside the cycle; confirm below
-        if (gh->resid <= tol) break;
-        if (total >= maxit) {
-            status = FSD_ERR_GMRES_MAXIT;
-            break;
-        }
+        rel = host[1] > 0 ? sqrt(host[0] / host[1]) : sqrt(host[0]);
+        if (status != FSD_OK || !(rel > tol) || total >= maxit) break;
     }
-    // True residual of the returned solution.
-    int e = saddle_multiply(h, pos, x, Ax, false);
-    if (e != FSD_OK) return e;
-    count_launch();
-    k_residual<<<vblocks, vthreads, 0, st>>>(b, Ax, r, n);
-    count_launch();
-    k_multidot<<<nbl, kRedThreads, 0, st>>>(r, n, 1, r, n, part, nullptr);
-    count_launch();
-    k_finish_dots<<<1, 32, 0, st>>>(part, nbl, 1, dots, false, nullptr);
-    double host[2];
-    FSD_CHECK_CUDA(cudaMemcpyAsync(host, dots, sizeof(double), cudaMemcpyDeviceToHost, st));
-    FSD_CHECK_CUDA(cudaMemcpyAsync(host + 1, &gs->bnorm2, sizeof(double), cudaMemcpyDeviceToHost, st));
-    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-    const double rel = host[1] > 0 ? sqrt(host[0] / host[1]) : sqrt(host[0]);
     const int ws = precond_wait_status(h);
     if (ws != FSD_OK) return ws;
     if (iters) *iters = total;
     if (resid) *resid = (float)rel;
     if (!(rel == rel)) status = FSD_ERR_BREAKDOWN;
+    if (status == FSD_OK && rel > tol && total >= maxit) status = FSD_ERR_GMRES_MAXIT;
     return status;
 }
 

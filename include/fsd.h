@@ -89,6 +89,10 @@ typedef struct fsd_params {
     float nlist_buffer;          /* neighbour-list skin added to the Ewald cutoff (0.4, integrate.py:83) */
     int ichol_local_shift;       /* 1: shift only failing IC(0) pivot blocks (default); 0: double the global
                                     relaxer and refactor, as Precondition.cu:1457-1489 */
+    float ichol_gain_limit;      /* largest accepted relaxer * lambda_max(G) of the IC(0) inverse, estimated by
+                                    power iteration after each factorisation; above it the relaxer doubles and
+                                    the factor is rebuilt (100; 0 = no check).  The exact (R + relaxer D)^-1
+                                    has relaxer * lambda_max <= 1. */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
@@ -111,6 +115,7 @@ typedef struct fsd_solve_info {
     int nlist_max;               /* largest neighbour count seen */
     int status;                  /* fsd_status of that call */
     int ichol_shifted;           /* pivot blocks that needed a local shift */
+    float ichol_gain;            /* power-iteration estimate of lambda_max(G) of the accepted factor */
 } fsd_solve_info;
 
 /* Arguments of one time step (Stokes_StepOne, Stokes.cuh:81-108). */

@@ -810,3 +810,48 @@ def euler_shear(pos, ori, pos_gb, vel, image, L, xy, dt, shear_rate, B1=0.0, b1m
     pn = (q0 * q0 - qq)[:, None] * pv + 2 * qp[:, None] * qv + 2 * q0[:, None] * np.cross(qv, pv)
     pn /= np.linalg.norm(pn, axis=1, keepdims=True)
     return p, pn, gb, img
+
+
+def pruned_rfu_sparse(pos, L, xy, tdist, tvals, rp=2.1, relaxer=1.0):
+    """Sparse (scipy CSR) form of pruned_rfu_dense for large N (pairs from a
+    periodic k-d tree; cubic boxes without tilt only)."""
+    import scipy.sparse as sp
+    from scipy.spatial import cKDTree
+    x = xyz(pos)
+    N = len(x)
+    Lb = L[0]
+    assert xy == 0.0 and L[0] == L[1] == L[2]
+    pairs = cKDTree((x + Lb / 2) % Lb, boxsize=Lb).query_pairs(rp, output_type="ndarray")
+    i = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    j = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    R = min_image32((np.asarray(pos, F32)[j, :3] - np.asarray(pos, F32)[i, :3]), L, xy).astype(np.float64)
+    dist = np.sqrt(np.einsum("ij,ij->i", R, R))
+    c = res_interp(dist, 0, 10, tdist, tvals, mode="precond")
+    XA11, XA12, YA11, YA12, YB11, YB12, XC11, XC12, YC11, YC12 = c.T
+    r = R / dist[:, None]
+    rr = r[:, :, None] * r[:, None, :]
+    Im = np.eye(3)[None] - rr
+    eps = np.zeros((len(r), 3, 3))
+    eps[:, 0, 1], eps[:, 0, 2] = r[:, 2], -r[:, 1]
+    eps[:, 1, 0], eps[:, 1, 2] = -r[:, 2], r[:, 0]
+    eps[:, 2, 0], eps[:, 2, 1] = r[:, 1], -r[:, 0]
+    off = np.zeros((len(r), 6, 6))
+    off[:, :3, :3] = XA12[:, None, None] * rr + YA12[:, None, None] * Im
+    off[:, :3, 3:] = YB12[:, None, None] * eps
+    off[:, 3:, :3] = YB12[:, None, None] * eps
+    off[:, 3:, 3:] = XC12[:, None, None] * rr + YC12[:, None, None] * Im
+    slf = np.zeros((len(r), 6, 6))
+    slf[:, :3, :3] = XA11[:, None, None] * rr + YA11[:, None, None] * Im
+    slf[:, :3, 3:] = -YB11[:, None, None] * eps
+    slf[:, 3:, :3] = YB11[:, None, None] * eps
+    slf[:, 3:, 3:] = XC11[:, None, None] * rr + YC11[:, None, None] * Im
+    diag = np.zeros((N, 6, 6))
+    np.add.at(diag, i, slf)
+    d = np.array([1.0, 1.0, 1.0] + [float(F32(1.33333333))] * 3)
+    diag[:, np.arange(6), np.arange(6)] += relaxer * d
+    rows = np.concatenate([np.repeat(6 * i[:, None] + np.arange(6), 6, 1).reshape(-1, 36),
+                           np.repeat(6 * np.arange(N)[:, None] + np.arange(6), 6, 1).reshape(-1, 36)])
+    cols = np.concatenate([np.tile(6 * j[:, None] + np.arange(6), 6).reshape(-1, 36),
+                           np.tile(6 * np.arange(N)[:, None] + np.arange(6), 6).reshape(-1, 36)])
+    vals = np.concatenate([off.reshape(-1, 36), diag.reshape(-1, 36)])
+    return sp.csr_matrix((vals.ravel(), (rows.ravel(), cols.ravel())), shape=(6 * N, 6 * N))
