@@ -297,6 +297,9 @@ def real_space(pos, F, C, L, xy, rows, table, self_x, self_y, ewald_cut, ewald_n
     dist = np.sqrt(d2)
     d32 = dist.astype(F32)
     rind = np.floor(F32(ewald_n) * (d32 - F32(ewald_dr)) / (F32(ewald_cut) - F32(ewald_dr))).astype(np.int64)
+    # A distance that rounds up to the cutoff in float32 gives rind = n; the
+    # reference then reads one row past its table.  Clamped, as the CUDA path.
+    rind = np.clip(rind, 0, ewald_n - 1)
     fac = dist / ewald_dr - rind - 1.0
     t = np.asarray(table, np.float64).reshape(-1, 8)
     lo, hi = t[rind], t[rind + 1]
