@@ -92,6 +92,8 @@ _SIGS = {
     "fsd_get_ewald_table": (C.c_int, [H, P, C.c_size_t]),
     "fsd_build_neighbor_list": (C.c_int, [H, P]),
     "fsd_get_neighbor_list": (C.c_int, [H, P, P, C.c_size_t, C.POINTER(C.c_int)]),
+    "fsd_neighbor_list_noalloc": (C.c_int, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                            P, P, C.c_int, P, P]),
     "fsd_mobility": (C.c_int, [H, P, P, P, C.c_int]),
     "fsd_lub_rfu": (C.c_int, [H, P, P, P]),
     "fsd_lub_rfe": (C.c_int, [H, P, C.c_float, P, P, C.c_float, P]),

@@ -7,6 +7,9 @@
 // and each particle scans its 27 neighbouring cells in a fixed order, so row
 // contents and order are deterministic.  Boxes with fewer than three cells
 // along an axis fall back to an all-pairs scan.
+#include <mutex>
+
+#include "fsd.h"
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_profile.h"
@@ -248,4 +251,92 @@ int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host) {
     return FSD_OK;
 }
 
+// ------------------------------------------- allocation-free neighbour list
+// Scratch of fsd_neighbor_list_noalloc: the cell key and cell members of every
+// particle and the counting-sort arrays of every cell, in one file-scope
+// device array (about 1.25 MiB, held on each device that loads the library
+// until the process exits).  All calls on a device share it.
+namespace {
+constexpr int kNoAllocMaxN = FSD_NOALLOC_MAX_N;
+constexpr int kNoAllocMaxCells = FSD_NOALLOC_MAX_CELLS;
+constexpr size_t kNoAllocScan = (size_t)(kNoAllocMaxCells + kScanTile - 1) / kScanTile + 1;
+constexpr size_t kOffKey = 0;
+constexpr size_t kOffParts = kOffKey + kNoAllocMaxN;
+constexpr size_t kOffCount = kOffParts + kNoAllocMaxN;
+constexpr size_t kOffStart = kOffCount + kNoAllocMaxCells;
+constexpr size_t kOffFill = kOffStart + kNoAllocMaxCells + 1;
+constexpr size_t kOffScan = kOffFill + kNoAllocMaxCells;
+constexpr size_t kNoAllocElems = kOffScan + kNoAllocScan;
+
+static __device__ __align__(256) unsigned g_nlist_scratch[kNoAllocElems];
+
+// Device address of g_nlist_scratch on the current device, looked up once per
+// device.  In host code the array's name is only a host-side stand-in, so the
+// kernels are always given this address instead.
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+unsigned* g_scratch_addr[kMaxDevices] = {};
+
+int noalloc_scratch(unsigned** out) {
+    int dev = -1;
+    FSD_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return FSD_ERR_BAD_PARAMS;
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        FSD_CHECK_CUDA(cudaGetSymbolAddress(&p, g_nlist_scratch));
+        g_scratch_addr[dev] = (unsigned*)p;
+    }
+    *out = g_scratch_addr[dev];
+    return FSD_OK;
+}
+}  // namespace
+
+int neighbor_list_noalloc(const float4* pos, int n, Box b, float rlist, unsigned* nneigh, unsigned* nlist,
+                          int stride, int* max_count, cudaStream_t st) {
+    unsigned* scratch = nullptr;
+    const int e = noalloc_scratch(&scratch);
+    if (e != FSD_OK) return e;
+    const float rlist2 = rlist * rlist;
+    int3 nc = cell_dims(b, rlist);
+    // Wider cells than r_list stay correct, so a box with more cells than the
+    // scratch holds uses fewer, wider cells along its longest cell axis.
+    while ((size_t)nc.x * nc.y * nc.z > (size_t)kNoAllocMaxCells) {
+        if (nc.x >= nc.y && nc.x >= nc.z) --nc.x;
+        else if (nc.y >= nc.z) --nc.y;
+        else --nc.z;
+    }
+    FSD_CHECK_CUDA(cudaMemsetAsync(max_count, 0, sizeof(int), st));
+    if (nc.x >= 3 && nc.y >= 3 && nc.z >= 3) {
+        const int ncells = nc.x * nc.y * nc.z;
+        unsigned* key = scratch + kOffKey;
+        unsigned* parts = scratch + kOffParts;
+        unsigned* start = scratch + kOffStart;
+        count_launch();
+        k_cell_key<<<(n + 255) / 256, 256, 0, st>>>(pos, n, b, nc, key);
+        // counting_sort clears the per-cell counters it accumulates into.
+        counting_sort(key, n, ncells, scratch + kOffCount, start, scratch + kOffFill, parts, scratch + kOffScan, st);
+        count_launch();
+        k_nlist_cells<<<(n + 127) / 128, 128, 0, st>>>(pos, n, b, nc, key, start, parts, rlist2, nneigh, nlist,
+                                                       stride, max_count);
+    } else {
+        count_launch();
+        k_nlist_allpairs<<<(n + 127) / 128, 128, 0, st>>>(pos, n, b, rlist2, nneigh, nlist, stride, max_count);
+    }
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
 }  // namespace fsd
+
+extern "C" int fsd_neighbor_list_noalloc(const float* d_pos, int N, float Lx, float Ly, float Lz, float xy,
+                                         float rlist, unsigned int* d_nneigh, unsigned int* d_nlist, int stride,
+                                         int* d_max_count, void* cuda_stream) {
+    if (!d_pos || !d_nneigh || !d_nlist || !d_max_count) return FSD_ERR_BAD_PARAMS;
+    if (N < 1 || N > FSD_NOALLOC_MAX_N || stride < 1) return FSD_ERR_BAD_PARAMS;
+    if (!(rlist > 0.f) || !(Lx > 0.f) || !(Ly > 0.f) || !(Lz > 0.f) || !std::isfinite(rlist) ||
+        !std::isfinite(Lx) || !std::isfinite(Ly) || !std::isfinite(Lz) || !std::isfinite(xy))
+        return FSD_ERR_BAD_PARAMS;
+    return fsd::neighbor_list_noalloc((const float4*)d_pos, N, fsd::Box{Lx, Ly, Lz, xy}, rlist, d_nneigh, d_nlist,
+                                      stride, d_max_count, (cudaStream_t)cuda_stream);
+}

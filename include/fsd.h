@@ -184,6 +184,38 @@ int fsd_build_neighbor_list(fsd_handle* h, const float* d_pos);
 int fsd_get_neighbor_list(const fsd_handle* h, unsigned int* host_nneigh, unsigned int* host_nlist,
                           size_t cap, int* stride);
 
+/* Neighbour list that allocates nothing.  No counterpart in the reference.
+ *
+ * fsd_create allocates the handle's device workspaces, and some callers
+ * cannot do that at the point where they need a list: an integrator whose
+ * host application owns all device memory through its own pool and gives a
+ * plug-in none of its own, or a step loop in which cudaMalloc/cudaFree,
+ * which can synchronise the whole device, are not allowed.  This entry point
+ * takes only the caller's buffers and does its cell binning in one fixed
+ * file-scope device array of about 1.25 MiB that every GPU loading the
+ * library holds until the process exits.
+ *
+ * Same lists as fsd_build_neighbor_list with r_list = ewald_cut + buffer:
+ * for each particle, every j != i with |minImage(x_i - x_j)|^2 < rlist^2, in
+ * a deterministic (not sorted) order.  d_pos: float4 x N; d_nneigh: N counts;
+ * d_nlist: N x stride entries; *d_max_count (device int) receives the
+ * largest count before capping: a value above stride means rows were
+ * truncated and the call should be repeated with a larger stride.
+ * N above FSD_NOALLOC_MAX_N, stride < 1, a non-positive box length or rlist
+ * return FSD_ERR_BAD_PARAMS before any GPU work.  Boxes whose cell grid
+ * would exceed FSD_NOALLOC_MAX_CELLS use fewer, wider cells.
+ *
+ * The first call on each device looks up the array's device address (with
+ * that device current); make that first call before any stream capture.
+ * All calls on a device share the array: calls whose GPU work overlaps
+ * (different streams without ordering between them) race and corrupt each
+ * other's lists.  Order them on one stream or with events. */
+#define FSD_NOALLOC_MAX_N 65536
+#define FSD_NOALLOC_MAX_CELLS 65536
+int fsd_neighbor_list_noalloc(const float* d_pos, int N, float Lx, float Ly, float Lz, float xy, float rlist,
+                              unsigned int* d_nneigh, unsigned int* d_nlist, int stride, int* d_max_count,
+                              void* cuda_stream);
+
 /* Generalized far-field mobility U = M^ff F on 11N vectors
  * (Mobility_GeneralizedMobility, Mobility.cu:1488).  parts: 1 = wave space
  * only, 2 = real space + self only, 3 = both (the reference). */
