@@ -39,6 +39,7 @@ class fsd_params(C.Structure):
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
         ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
+        ("learned_inner", C.c_int), ("learned_rg", C.c_float),
     ]
 
 
@@ -101,6 +102,7 @@ _SIGS = {
     "fsd_lub_rse": (C.c_int, [H, P, C.c_float, P, P, C.c_float, P]),
     "fsd_saddle_multiply": (C.c_int, [H, P, P, P]),
     "fsd_precond_build": (C.c_int, [H, P]),
+    "fsd_precond_set_blocks": (C.c_int, [H, C.c_int, P, P, P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),
     "fsd_saddle_solve": (C.c_int, [H, P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "fsd_brownian_farfield": (C.c_int, [H, P, C.c_uint, P]),

@@ -191,6 +191,16 @@ class FSD:
         self._sync_stream()
         check(lib().fsd_precond_build(self._h, _ptr(pos)), "fsd_precond_build")
 
+    def precond_set_blocks(self, rowptr, col, blocks):
+        """Block-CSR G (int32 rowptr N+1, int32 col, float32 blocks nnzb x 36) for precond='learned'."""
+        self._sync_stream()
+        rowptr = torch.as_tensor(rowptr, dtype=torch.int32, device=self.device).contiguous()
+        col = torch.as_tensor(col, dtype=torch.int32, device=self.device).contiguous()
+        blocks = torch.as_tensor(blocks, dtype=torch.float32, device=self.device).contiguous()
+        check(lib().fsd_precond_set_blocks(self._h, int(col.numel()), _ptr(rowptr), _ptr(col), _ptr(blocks)),
+              "fsd_precond_set_blocks")
+        torch.cuda.synchronize(self.device)
+
     def precond_apply(self, b) -> torch.Tensor:
         self._sync_stream()
         out = self._new(17 * self.N)

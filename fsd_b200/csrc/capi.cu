@@ -8,6 +8,7 @@
 
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_learned.h"
 #include "fsd_solver.h"
 #include "fsd_profile.h"
 
@@ -89,6 +90,8 @@ static int allocate(fsd_handle* h) {
     FSD_TRY(dalloc(&w.sz, n17));
     const int m = std::min(h->p.gmres_restart, kMaxRestart);
     FSD_TRY(dalloc(&w.V, (size_t)(m + 1) * n17));
+    if (h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0)  // flexible GMRES keeps M^-1 v_j
+        FSD_TRY(dalloc(&w.Z, (size_t)m * n17));
     FSD_TRY(dalloc(&w.dred, (size_t)(kMaxRestart + 2) * 512));
     FSD_TRY(dalloc(&w.hcol, kMaxRestart + 2));
     FSD_TRY(dalloc(&w.hcol2, kMaxRestart + 2));
@@ -118,7 +121,7 @@ static void release(fsd_handle* h) {
     Workspace& w = h->w;
     void* dev[] = {w.nneigh, w.nlist, w.nl_overflow, w.scan_scratch, w.part_cell, w.cell_count, w.cell_start,
                    w.cell_fill, w.cell_parts, w.part_origin_key, w.part_origin, w.bin_count, w.bin_start, w.bin_fill,
-                   w.bin_parts, w.grid, w.gridk, w.twiddle, w.f4, w.c4, w.uwave, w.sx, w.sy, w.sz, w.V, w.dred,
+                   w.bin_parts, w.grid, w.gridk, w.twiddle, w.f4, w.c4, w.uwave, w.sx, w.sy, w.sz, w.V, w.Z, w.dred,
                    w.hcol, w.hcol2, w.gmres_state, w.pc_t, w.pc_y, w.rhs, w.sol, w.rfd_rhs, w.rfd_sol, w.psi,
                    w.pos_prime, w.vel, w.force, w.lanczos_V, w.lz_a, w.lz_b, w.lz_c, w.lz_dot, h->d_ewald,
                    h->d_res_dist, h->d_res_vals};
@@ -128,6 +131,7 @@ static void release(fsd_handle* h) {
     if (w.gmres_host) cudaFreeHost(w.gmres_host);
     if (w.lz_host) cudaFreeHost(w.lz_host);
     precond_free(h);
+    learned_free(h);
     profile_destroy(h);
 }
 
@@ -167,6 +171,8 @@ void fsd_default_params(fsd_params* p) {
     p->nlist_buffer = 0.4f;
     p->ichol_local_shift = 1;
     p->ichol_gain_limit = 100.0f;
+    p->learned_inner = 4;
+    p->learned_rg = 3.0f;
 }
 
 const char* fsd_status_string(int status) {
@@ -231,6 +237,7 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
     if (p->N < 1 || !(p->Lx > 0 && p->Ly > 0 && p->Lz > 0) || !(p->xi > 0) || !(p->error > 0 && p->error < 1))
         return FSD_ERR_BAD_PARAMS;
     if (p->gmres_restart < 1 || p->gmres_restart > kMaxRestart || p->lanczos_max < 4) return FSD_ERR_BAD_PARAMS;
+    if (p->learned_inner < 0 || p->learned_inner > kMaxInner || !(p->learned_rg > 2.0f)) return FSD_ERR_BAD_PARAMS;
     fsd_handle* h = new fsd_handle();
     h->p = *p;
     h->stream = (cudaStream_t)stream;
@@ -416,6 +423,11 @@ int fsd_saddle_multiply(fsd_handle* h, const float* d_pos, const float* d_x, flo
 int fsd_precond_build(fsd_handle* h, const float* d_pos) {
     if (!h || !h->nlist_valid || !d_pos) return FSD_ERR_BAD_PARAMS;
     return precond_build(h, (const float4*)d_pos);
+}
+
+int fsd_precond_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_blocks) {
+    if (!h || !d_rowptr || (nnzb > 0 && (!d_col || !d_blocks))) return FSD_ERR_BAD_PARAMS;
+    return learned_set_blocks(h, nnzb, d_rowptr, d_col, d_blocks);
 }
 
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x) {

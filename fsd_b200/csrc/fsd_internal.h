@@ -95,6 +95,7 @@ struct Workspace {
     float* sy = nullptr;
     float* sz = nullptr;
     float* V = nullptr;            // (restart + 1) x 17N basis
+    float* Z = nullptr;            // restart x 17N preconditioned basis (flexible GMRES only)
     double* dred = nullptr;        // per-block partial sums
     double* hcol = nullptr;        // Hessenberg column
     double* hcol2 = nullptr;       // re-orthogonalisation column
@@ -141,5 +142,6 @@ struct fsd_handle {
     float ichol_relaxer = 1.0f;
     int m_lanczos_ff = 2, m_lanczos_nf = 2;
     void* ichol = nullptr;     // preconditioner state (precond.cu)
+    void* learned = nullptr;   // block-sparse preconditioner state (learned.cu)
     void* profiler = nullptr;  // region timers (profile.cpp)
 };

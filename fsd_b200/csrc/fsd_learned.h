@@ -1,0 +1,38 @@
+// Learned block-sparse preconditioner (learned.cu).
+#pragma once
+
+#include "fsd_internal.h"
+
+namespace fsd {
+
+struct LearnedState {
+    // G in block-CSR over particles (original order), 6x6 row-major fp32 blocks
+    int* g_rowptr = nullptr;
+    int* g_col = nullptr;
+    float* g_val = nullptr;
+    int g_nnzb = 0, g_cap = 0;
+    bool g_user = false;  // blocks were set through fsd_precond_set_blocks
+    // R_FU^pruned + D operator (owned by the IC(0) state, pruned-list order)
+    const unsigned* a_pn = nullptr;
+    const unsigned* a_plist = nullptr;
+    const float* a_blocks = nullptr;
+    // inner GMRES work space
+    int inner_cap = -1;
+    float* t = nullptr;      // 6N right-hand side of the inner solve
+    float* w = nullptr;      // 6N
+    float* y = nullptr;      // 6N inner solution
+    float* Vi = nullptr;     // (kMaxInner + 1) x 6N
+    float* Zi = nullptr;     // kMaxInner x 6N
+    double* part = nullptr;  // (kMaxInner + 2) x kInnerBlocks partial sums
+    double* H = nullptr;     // (kMaxInner + 1) x kMaxInner Hessenberg, column-major by step, plus beta
+};
+
+LearnedState* learned(fsd_handle* h);
+void learned_free(fsd_handle* h);
+int learned_reserve(fsd_handle* h, int nnzb);
+int learned_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_val);
+int precond_apply_learned(fsd_handle* h, const float* b, float* x);
+int precond_build_learned(fsd_handle* h, const float4* pos);
+bool precond_is_flexible(const fsd_handle* h);
+
+}  // namespace fsd

@@ -6,6 +6,7 @@
 namespace fsd {
 
 constexpr int kMaxRestart = 400;
+constexpr int kMaxInner = 16;    // inner GMRES steps of the learned preconditioner
 constexpr int kPrunedCap = 32;  // pruned (r < rp) neighbours per particle, self included
 
 int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin);
@@ -20,6 +21,10 @@ int precond_build(fsd_handle* h, const float4* pos);
 int precond_G(fsd_handle* h, const float* t, float* y);
 int precond_apply_ichol(fsd_handle* h, const float* b, float* x);
 int precond_wait_status(fsd_handle* h);
+// Pruned R_FU + relaxer D in pruned-list order (precond.cu): pn (N), plist and
+// blocks (N x kPrunedCap, self included), no ordering or factorisation.
+int precond_assemble_pruned(fsd_handle* h, const float4* pos, float relaxer, const unsigned** pn,
+                            const unsigned** plist, const float** blocks);
 
 // Host reverse Cuthill-McKee ordering of a symmetric graph in CSR form
 // (adjacency may include self loops).  perm[new] = old.

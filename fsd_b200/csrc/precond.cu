@@ -23,6 +23,7 @@
 #include "fsd_brownian.h"
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_learned.h"
 #include "fsd_solver.h"
 #include "fsd_profile.h"
 
@@ -706,6 +707,7 @@ int precond_build(fsd_handle* h, const float4* pos) {
         h->pc_valid = true;
         return FSD_OK;
     }
+    if (h->p.precond == FSD_PRECOND_LEARNED) return precond_build_learned(h, pos);
     ProfRegion pr(h, R_PRECOND_BUILD);
     FSD_CHECK_CUDA(cudaMemsetAsync(ic->p_over, 0, sizeof(int), st));
     count_launch();
@@ -834,6 +836,29 @@ int precond_build(fsd_handle* h, const float4* pos) {
         h->ichol_relaxer *= 2.0f;
     }
     return FSD_ERR_ICHOL;
+}
+
+// Pruned matrix only (for preconditioners that use R_FU^pruned + relaxer D as
+// an operator): prune, check the list capacity, assemble.
+int precond_assemble_pruned(fsd_handle* h, const float4* pos, float relaxer, const unsigned** pn,
+                            const unsigned** plist, const float** blocks) {
+    IChol* ic = (IChol*)h->ichol;
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
+    FSD_CHECK_CUDA(cudaMemsetAsync(ic->p_over, 0, sizeof(int), st));
+    count_launch();
+    k_prune<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride,
+                                             h->p.rp * h->p.rp, ic->pn, ic->plist, ic->p_over);
+    count_launch();
+    k_assemble<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, ic->pn, ic->plist,
+                                               ResTable{h->d_res_dist, h->d_res_vals}, h->p.rp, relaxer, ic->blocks);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(ic->h_fail, ic->p_over, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (ic->h_fail[0] > 0) return FSD_ERR_NLIST_OVERFLOW;
+    *pn = ic->pn;
+    *plist = ic->plist;
+    *blocks = ic->blocks;
+    return FSD_OK;
 }
 
 // x = P^-1 b for the saddle system with the IC(0) factor, two launches.

@@ -17,6 +17,7 @@
 
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
+#include "fsd_learned.h"
 #include "fsd_solver.h"
 #include "fsd_profile.h"
 
@@ -51,6 +52,7 @@ int precond_apply(fsd_handle* h, const float* b, float* x) {
     const int N = h->p.N;
     ProfRegion pr(h, R_PRECOND_APPLY);
     if (h->p.precond == FSD_PRECOND_ICHOL) return precond_apply_ichol(h, b, x);
+    if (h->p.precond == FSD_PRECOND_LEARNED) return precond_apply_learned(h, b, x);
     float* t = h->w.pc_t;
     float* y = h->w.pc_y;
     count_launch();
@@ -95,6 +97,34 @@ __global__ void __launch_bounds__(kRedThreads) k_multidot(const float* __restric
         for (size_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) s += (double)vi[k] * (double)w[k];
         s = block_sum_d(s, sh);
         if (threadIdx.x == 0) part[(size_t)i * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// Same partial dots for the Gram-Schmidt passes, where nv is large: the
+// block's slice of w is staged in shared memory once and each warp takes
+// whole vectors, so no block-wide reduction is needed per vector.  Slices are
+// `chunk` long (the launch's dynamic shared memory is chunk floats).
+__global__ void __launch_bounds__(kRedThreads) k_multidot_ws(const float* __restrict__ V, size_t ld, int nv,
+                                                             const float* __restrict__ w, size_t n, size_t chunk,
+                                                             double* part, const int* done) {
+    if (done && *done) return;
+    extern __shared__ float ws[];
+    const size_t b0 = (size_t)blockIdx.x * chunk;
+    const size_t len = b0 < n ? min(chunk, n - b0) : 0;
+    for (size_t k = threadIdx.x; k < len; k += blockDim.x) ws[k] = w[b0 + k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i < nv; i += nw) {
+        const float* vi = V + (size_t)i * ld + b0;
+        double s = 0.0;
+        size_t k = lane;
+        for (; k + 96 < len; k += 128) {
+            const float a0 = vi[k], a1 = vi[k + 32], a2 = vi[k + 64], a3 = vi[k + 96];
+            s += (double)a0 * ws[k] + (double)a1 * ws[k + 32] + (double)a2 * ws[k + 64] + (double)a3 * ws[k + 96];
+        }
+        for (; k < len; k += 32) s += (double)vi[k] * ws[k];
+        s = group_sum_d<32>(s);
+        if (lane == 0) part[(size_t)i * gridDim.x + blockIdx.x] = s;
     }
 }
 
@@ -282,6 +312,18 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     double* dots = w.hcol;  // [0..m+1]
     const int nbl = kRedBlocks;
     const int vthreads = 256, vblocks = 4 * 148;
+    // Flexible GMRES (Saad 1993) when the preconditioner varies between
+    // applications: the preconditioned basis Z is kept and x += Z y.
+    const bool flexible = precond_is_flexible(h);
+    if (flexible && !w.Z) return FSD_ERR_BAD_PARAMS;
+    const size_t chunk = (n + nbl - 1) / nbl;
+    const bool staged = chunk * sizeof(float) <= 48 * 1024;
+    auto multidot = [&](const float* Vb, size_t ldv, int nv, const float* wv, size_t nn, double* pt, const int* dn) {
+        if (staged)
+            k_multidot_ws<<<nbl, kRedThreads, chunk * sizeof(float), st>>>(Vb, ldv, nv, wv, nn, chunk, pt, dn);
+        else
+            k_multidot<<<nbl, kRedThreads, 0, st>>>(Vb, ldv, nv, wv, nn, pt, dn);
+    };
     int total = 0;
     bool first = true;
     int status = FSD_OK;
@@ -319,20 +361,21 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
             const bool converged_at_start = gh->done != 0;
             for (int j = 0; j < m && !converged_at_start; ++j) {
                 // w = A M^-1 V_j
-                e = precond_apply(h, V + (size_t)j * ld, z);
+                float* zj = flexible ? w.Z + (size_t)j * ld : z;
+                e = precond_apply(h, V + (size_t)j * ld, zj);
                 if (e != FSD_OK) return e;
-                e = saddle_multiply(h, pos, z, Ax, false);
+                e = saddle_multiply(h, pos, zj, Ax, false);
                 if (e != FSD_OK) return e;
                 // CGS2 against V_0..V_j.
                 ProfRegion pk(h, R_KRYLOV);
                 count_launch();
-                k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+                multidot(V, ld, j + 1, Ax, n, part, &gs->done);
                 count_launch();
                 k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, dots, false, &gs->done);
                 count_launch();
                 k_multiaxpy<<<vblocks, vthreads, 0, st>>>(V, ld, j + 1, dots, Ax, n, &gs->done);
                 count_launch();
-                k_multidot<<<nbl, kRedThreads, 0, st>>>(V, ld, j + 1, Ax, n, part, &gs->done);
+                multidot(V, ld, j + 1, Ax, n, part, &gs->done);
                 count_launch();
                 k_finish_dots<<<(j + 1 + 7) / 8, 256, 0, st>>>(part, nbl, j + 1, w.hcol2, false, &gs->done);
                 count_launch();
@@ -365,10 +408,15 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
             if (jc > 0) {
                 count_launch();
                 k_lsq<<<1, 1, 0, st>>>(gs);
-                count_launch();
-                k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
-                e = precond_apply(h, Ax, z);
-                if (e != FSD_OK) return e;
+                if (flexible) {  // x += Z y
+                    count_launch();
+                    k_combine<<<vblocks, vthreads, 0, st>>>(w.Z, ld, jc, gs_y(gs), z, n);
+                } else {  // x += M^-1 V y
+                    count_launch();
+                    k_combine<<<vblocks, vthreads, 0, st>>>(V, ld, jc, gs_y(gs), Ax, n);
+                    e = precond_apply(h, Ax, z);
+                    if (e != FSD_OK) return e;
+                }
                 count_launch();
                 k_axpy<<<vblocks, vthreads, 0, st>>>(x, z, n);
             }

@@ -93,6 +93,10 @@ typedef struct fsd_params {
                                     power iteration after each factorisation; above it the relaxer doubles and
                                     the factor is rebuilt (100; 0 = no check).  The exact (R + relaxer D)^-1
                                     has relaxer * lambda_max <= 1. */
+    int learned_inner;           /* FSD_PRECOND_LEARNED: inner GMRES steps on R_FU^pruned + D per application,
+                                    right-preconditioned by the learned block-sparse G (4; 0 = apply G once).
+                                    With inner steps the outer solve is flexible GMRES. */
+    float learned_rg;            /* FSD_PRECOND_LEARNED: pair distance below which G has a block (3.0) */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
@@ -233,6 +237,13 @@ int fsd_lub_rse(fsd_handle* h, const float* d_pos, float shear_rate, const float
 int fsd_saddle_multiply(fsd_handle* h, const float* d_pos, const float* d_x, float* d_b);
 /* Build the near-field preconditioner for these positions (Precondition_Wrap, Precondition.cu:1326). */
 int fsd_precond_build(fsd_handle* h, const float* d_pos);
+/* Set the block-sparse G used by FSD_PRECOND_LEARNED in place of the IC(0)
+ * factor's (L L^T)^-1 inside the saddle preconditioner (Saddle.cu:171-264;
+ * the explicit-G slot itself has no counterpart in the reference).  Block CSR
+ * over particles in their original order: d_rowptr (N+1), d_col (nnzb),
+ * d_blocks (nnzb x 36, row-major 6x6 fp32).  The structure is checked
+ * (rowptr monotone, rowptr[N] = nnzb, 0 <= col < N) and the arrays copied. */
+int fsd_precond_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_blocks);
 /* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x);
 /* Preconditioned GMRES on the saddle system (Solvers_Saddle, Solvers.cu:55).

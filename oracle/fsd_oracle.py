@@ -681,6 +681,69 @@ def pruned_rfu_dense(pos, L, xy, rows, tdist, tvals, rp=2.1, relaxer=1.0):
     return A, prow
 
 
+def pruned_pairs(pos, L, xy, rows=None, rp=2.1):
+    """Directed pairs (i, j), i != j, of the pruned graph: float64 minimum-image
+    distance below rp (Precondition_GetPrunedNneigh_kernel, Precondition.cu:443).
+    Candidates come from `rows`, or from a periodic k-d tree for untilted boxes."""
+    x = xyz(pos)
+    if rows is None:
+        from scipy.spatial import cKDTree
+        if xy != 0.0:
+            raise ValueError("k-d tree candidates need an untilted box; pass rows")
+        Lb = np.asarray(L, np.float64)
+        pr = cKDTree(np.mod(x + Lb / 2, Lb), boxsize=Lb).query_pairs(rp + 1e-3, output_type="ndarray")
+        i = np.concatenate([pr[:, 0], pr[:, 1]]).astype(np.int64)
+        j = np.concatenate([pr[:, 1], pr[:, 0]]).astype(np.int64)
+    else:
+        i, j = pair_arrays(rows)
+    d = min_image(x[i] - x[j], L, xy)
+    keep = np.einsum("ij,ij->i", d, d) < rp * rp
+    i, j = i[keep], j[keep]
+    o = np.lexsort((j, i))
+    return i[o], j[o]
+
+
+def pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=None, rp=2.1, relaxer=1.0):
+    """pruned_rfu_dense as a SciPy CSR matrix, vectorised for large N."""
+    import scipy.sparse as sp
+    x = xyz(pos)
+    N = len(x)
+    i, j = pruned_pairs(pos, L, xy, rows, rp)
+    R = min_image32((x[j] - x[i]).astype(F32), L, xy)
+    dist = np.sqrt(R[:, 0] * R[:, 0] + R[:, 1] * R[:, 1] + R[:, 2] * R[:, 2])
+    R = R.astype(np.float64)
+    c = res_interp(dist, 0, 10, tdist, tvals, mode="precond")
+    XA11, XA12, YA11, YA12, YB11, YB12, XC11, XC12, YC11, YC12 = c.T
+    r = R / dist.astype(np.float64)[:, None]
+    rr = r[:, :, None] * r[:, None, :]
+    Im = np.eye(3)[None] - rr
+    eps = np.zeros((len(r), 3, 3))
+    eps[:, 0, 1], eps[:, 0, 2] = r[:, 2], -r[:, 1]
+    eps[:, 1, 0], eps[:, 1, 2] = -r[:, 2], r[:, 0]
+    eps[:, 2, 0], eps[:, 2, 1] = r[:, 1], -r[:, 0]
+    w = lambda a: a[:, None, None]
+    off = np.zeros((len(r), 6, 6))
+    off[:, :3, :3] = w(XA12) * rr + w(YA12) * Im
+    off[:, :3, 3:] = w(YB12) * eps
+    off[:, 3:, :3] = w(YB12) * eps
+    off[:, 3:, 3:] = w(XC12) * rr + w(YC12) * Im
+    slf = np.zeros((len(r), 6, 6))
+    slf[:, :3, :3] = w(XA11) * rr + w(YA11) * Im
+    slf[:, :3, 3:] = -w(YB11) * eps
+    slf[:, 3:, :3] = w(YB11) * eps
+    slf[:, 3:, 3:] = w(XC11) * rr + w(YC11) * Im
+    diag = np.zeros((N, 6, 6))
+    np.add.at(diag, i, slf)
+    d = np.array([1.0, 1.0, 1.0] + [float(F32(1.33333333))] * 3)
+    diag[:, np.arange(6), np.arange(6)] += relaxer * d
+    bi = np.concatenate([i, np.arange(N)])
+    bj = np.concatenate([j, np.arange(N)])
+    vals = np.concatenate([off, diag])
+    rows_ = (6 * bi[:, None, None] + np.arange(6)[None, :, None]) * np.ones((1, 1, 6), np.int64)
+    cols_ = (6 * bj[:, None, None] + np.arange(6)[None, None, :]) * np.ones((1, 6, 1), np.int64)
+    return sp.csr_matrix((vals.ravel(), (rows_.ravel(), cols_.ravel())), shape=(6 * N, 6 * N))
+
+
 def ichol0_dense(A, pattern):
     """Scalar IC(0) restricted to `pattern` (boolean), FP64.  Returns L or None on a non-positive pivot."""
     n = len(A)
@@ -813,48 +876,3 @@ def euler_shear(pos, ori, pos_gb, vel, image, L, xy, dt, shear_rate, B1=0.0, b1m
     pn = (q0 * q0 - qq)[:, None] * pv + 2 * qp[:, None] * qv + 2 * q0[:, None] * np.cross(qv, pv)
     pn /= np.linalg.norm(pn, axis=1, keepdims=True)
     return p, pn, gb, img
-
-
-def pruned_rfu_sparse(pos, L, xy, tdist, tvals, rp=2.1, relaxer=1.0):
-    """Sparse (scipy CSR) form of pruned_rfu_dense for large N (pairs from a
-    periodic k-d tree; cubic boxes without tilt only)."""
-    import scipy.sparse as sp
-    from scipy.spatial import cKDTree
-    x = xyz(pos)
-    N = len(x)
-    Lb = L[0]
-    assert xy == 0.0 and L[0] == L[1] == L[2]
-    pairs = cKDTree((x + Lb / 2) % Lb, boxsize=Lb).query_pairs(rp, output_type="ndarray")
-    i = np.concatenate([pairs[:, 0], pairs[:, 1]])
-    j = np.concatenate([pairs[:, 1], pairs[:, 0]])
-    R = min_image32((np.asarray(pos, F32)[j, :3] - np.asarray(pos, F32)[i, :3]), L, xy).astype(np.float64)
-    dist = np.sqrt(np.einsum("ij,ij->i", R, R))
-    c = res_interp(dist, 0, 10, tdist, tvals, mode="precond")
-    XA11, XA12, YA11, YA12, YB11, YB12, XC11, XC12, YC11, YC12 = c.T
-    r = R / dist[:, None]
-    rr = r[:, :, None] * r[:, None, :]
-    Im = np.eye(3)[None] - rr
-    eps = np.zeros((len(r), 3, 3))
-    eps[:, 0, 1], eps[:, 0, 2] = r[:, 2], -r[:, 1]
-    eps[:, 1, 0], eps[:, 1, 2] = -r[:, 2], r[:, 0]
-    eps[:, 2, 0], eps[:, 2, 1] = r[:, 1], -r[:, 0]
-    off = np.zeros((len(r), 6, 6))
-    off[:, :3, :3] = XA12[:, None, None] * rr + YA12[:, None, None] * Im
-    off[:, :3, 3:] = YB12[:, None, None] * eps
-    off[:, 3:, :3] = YB12[:, None, None] * eps
-    off[:, 3:, 3:] = XC12[:, None, None] * rr + YC12[:, None, None] * Im
-    slf = np.zeros((len(r), 6, 6))
-    slf[:, :3, :3] = XA11[:, None, None] * rr + YA11[:, None, None] * Im
-    slf[:, :3, 3:] = -YB11[:, None, None] * eps
-    slf[:, 3:, :3] = YB11[:, None, None] * eps
-    slf[:, 3:, 3:] = XC11[:, None, None] * rr + YC11[:, None, None] * Im
-    diag = np.zeros((N, 6, 6))
-    np.add.at(diag, i, slf)
-    d = np.array([1.0, 1.0, 1.0] + [float(F32(1.33333333))] * 3)
-    diag[:, np.arange(6), np.arange(6)] += relaxer * d
-    rows = np.concatenate([np.repeat(6 * i[:, None] + np.arange(6), 6, 1).reshape(-1, 36),
-                           np.repeat(6 * np.arange(N)[:, None] + np.arange(6), 6, 1).reshape(-1, 36)])
-    cols = np.concatenate([np.tile(6 * j[:, None] + np.arange(6), 6).reshape(-1, 36),
-                           np.tile(6 * np.arange(N)[:, None] + np.arange(6), 6).reshape(-1, 36)])
-    vals = np.concatenate([off.reshape(-1, 36), diag.reshape(-1, 36)])
-    return sp.csr_matrix((vals.ravel(), (rows.ravel(), cols.ravel())), shape=(6 * N, 6 * N))
