@@ -103,6 +103,11 @@ _SIGS = {
     "fsd_saddle_multiply": (C.c_int, [H, P, P, P]),
     "fsd_precond_build": (C.c_int, [H, P]),
     "fsd_precond_set_blocks": (C.c_int, [H, C.c_int, P, P, P]),
+    "fsd_learned_num_weights": (C.c_int, []),
+    "fsd_learned_set_weights": (C.c_int, [H, P, C.c_int]),
+    "fsd_learned_get_weights": (C.c_int, [H, P, C.c_int]),
+    "fsd_learned_tensor_cores": (C.c_int, [H, C.c_int]),
+    "fsd_learned_train_step": (C.c_int, [H, P, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float), P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),
     "fsd_saddle_solve": (C.c_int, [H, P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "fsd_brownian_farfield": (C.c_int, [H, P, C.c_uint, P]),

@@ -201,6 +201,36 @@ class FSD:
               "fsd_precond_set_blocks")
         torch.cuda.synchronize(self.device)
 
+    def learned_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        check(lib().fsd_learned_set_weights(self._h, w.ctypes.data_as(C.c_void_p), int(w.size)),
+              "fsd_learned_set_weights")
+
+    def learned_get_weights(self) -> np.ndarray:
+        w = np.zeros(lib().fsd_learned_num_weights(), np.float32)
+        check(lib().fsd_learned_get_weights(self._h, w.ctypes.data_as(C.c_void_p), int(w.size)),
+              "fsd_learned_get_weights")
+        return w
+
+    def learned_tensor_cores(self, on: bool):
+        check(lib().fsd_learned_tensor_cores(self._h, int(bool(on))), "fsd_learned_tensor_cores")
+
+    def learned_train_step(self, pos, probes=None, n_probes=4, step=0, lr=0.0, want_grad=False):
+        """Loss (and gradient as a NumPy vector when want_grad) of the approximate-inverse
+        objective for these positions; lr > 0 also takes one Adam step."""
+        self._sync_stream()
+        pp = None
+        if probes is not None:
+            probes = np.ascontiguousarray(probes, np.float32)
+            n_probes = probes.shape[0]
+            pp = probes.ctypes.data_as(C.c_void_p)
+        loss = C.c_float(0.0)
+        g = np.zeros(lib().fsd_learned_num_weights(), np.float32) if want_grad else None
+        check(lib().fsd_learned_train_step(self._h, _ptr(pos), pp, int(n_probes), int(step), float(lr),
+                                           C.byref(loss), g.ctypes.data_as(C.c_void_p) if want_grad else None),
+              "fsd_learned_train_step")
+        return (loss.value, g) if want_grad else loss.value
+
     def precond_apply(self, b) -> torch.Tensor:
         self._sync_stream()
         out = self._new(17 * self.N)

@@ -9,6 +9,7 @@
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_learned.h"
+#include "fsd_mpnn.h"
 #include "fsd_solver.h"
 #include "fsd_profile.h"
 
@@ -428,6 +429,30 @@ int fsd_precond_build(fsd_handle* h, const float* d_pos) {
 int fsd_precond_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_blocks) {
     if (!h || !d_rowptr || (nnzb > 0 && (!d_col || !d_blocks))) return FSD_ERR_BAD_PARAMS;
     return learned_set_blocks(h, nnzb, d_rowptr, d_col, d_blocks);
+}
+
+int fsd_learned_num_weights(void) { return MpLayout::total; }
+
+int fsd_learned_set_weights(fsd_handle* h, const float* host_w, int n) {
+    if (!h || !host_w) return FSD_ERR_BAD_PARAMS;
+    return learned_set_weights(h, host_w, n);
+}
+
+int fsd_learned_get_weights(fsd_handle* h, float* host_w, int n) {
+    if (!h || !host_w) return FSD_ERR_BAD_PARAMS;
+    return mpnn_get_weights(h, host_w, n);
+}
+
+int fsd_learned_tensor_cores(fsd_handle* h, int on) {
+    if (!h) return FSD_ERR_BAD_PARAMS;
+    mpnn_use_umma(h, on != 0);
+    return FSD_OK;
+}
+
+int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,
+                           unsigned int step, float lr, float* loss, float* host_grad) {
+    if (!h || !d_pos || !h->nlist_valid || n_probes < 1) return FSD_ERR_BAD_PARAMS;
+    return mpnn_train_step(h, (const float4*)d_pos, host_probes, n_probes, step, lr, loss, host_grad);
 }
 
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x) {

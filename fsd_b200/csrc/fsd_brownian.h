@@ -14,6 +14,7 @@ constexpr uint32_t kStreamNF = 3;      // near-field normals (6N)
 constexpr uint32_t kStreamRFD = 4;     // drift direction (6N)
 constexpr uint32_t kStreamRot = 5;     // rotational noise (3N)
 constexpr uint32_t kStreamGain = 6;    // start vector of the IC(0) gain estimate (6N)
+constexpr uint32_t kStreamLearned = 7; // probe vectors of the learned preconditioner's training loss
 
 void dot_device(fsd_handle* h, const float* a, const float* b, size_t n, double* out);
 void gaussian(fsd_handle* h, float* out, size_t n, uint32_t step, uint32_t stream, float scale);

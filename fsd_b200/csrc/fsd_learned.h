@@ -25,6 +25,16 @@ struct LearnedState {
     float* Zi = nullptr;     // kMaxInner x 6N
     double* part = nullptr;  // (kMaxInner + 2) x kInnerBlocks partial sums
     double* H = nullptr;     // (kMaxInner + 1) x kMaxInner Hessenberg, column-major by step, plus beta
+    void* mp = nullptr;      // message-passing network state (mpnn.cu)
+    // two-hop sparse approximate inverse (spai.cu)
+    int* sp_sets = nullptr;          // N x kSpaiCap members, particle itself first
+    unsigned* sp_size = nullptr;     // N set sizes
+    unsigned* sp_rowptr = nullptr;   // N + 1
+    unsigned* sp_scan = nullptr;
+    int* sp_bucket = nullptr;        // bucket lists
+    unsigned* sp_cnt = nullptr;      // bucket counts, truncated sets, failed rows
+    unsigned* sp_host = nullptr;
+    int sp_truncated = 0;
 };
 
 LearnedState* learned(fsd_handle* h);
@@ -33,6 +43,18 @@ int learned_reserve(fsd_handle* h, int nnzb);
 int learned_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_val);
 int precond_apply_learned(fsd_handle* h, const float* b, float* x);
 int precond_build_learned(fsd_handle* h, const float4* pos);
+int learned_set_weights(fsd_handle* h, const float* host_w, int n);
 bool precond_is_flexible(const fsd_handle* h);
+int spai_build(fsd_handle* h);
+
+// mpnn.cu
+void mpnn_free(fsd_handle* h);
+int mpnn_set_weights(fsd_handle* h, const float* host_w, int n);
+int mpnn_get_weights(fsd_handle* h, float* host_w, int n);
+bool mpnn_loaded(fsd_handle* h);
+void mpnn_use_umma(fsd_handle* h, bool on);
+int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist, const float* a_blocks);
+int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, int P, uint32_t step, float lr,
+                    float* loss_out, float* host_grad);
 
 }  // namespace fsd

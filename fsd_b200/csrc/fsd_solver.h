@@ -7,7 +7,8 @@ namespace fsd {
 
 constexpr int kMaxRestart = 400;
 constexpr int kMaxInner = 16;    // inner GMRES steps of the learned preconditioner
-constexpr int kPrunedCap = 32;  // pruned (r < rp) neighbours per particle, self included
+constexpr int kPrunedCap = 32;
+constexpr int kSpaiCap = 32;     // members of a two-hop approximate-inverse set  // pruned (r < rp) neighbours per particle, self included
 
 int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin);
 int precond_apply(fsd_handle* h, const float* b, float* x);

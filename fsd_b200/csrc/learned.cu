@@ -26,9 +26,12 @@ LearnedState* learned(fsd_handle* h) {
 void learned_free(fsd_handle* h) {
     LearnedState* s = (LearnedState*)h->learned;
     if (!s) return;
-    void* ptrs[] = {s->g_rowptr, s->g_col, s->g_val, s->t, s->w, s->y, s->Vi, s->Zi, s->part, s->H};
+    mpnn_free(h);
+    void* ptrs[] = {s->g_rowptr, s->g_col, s->g_val, s->t, s->w, s->y, s->Vi, s->Zi, s->part, s->H,
+                    s->sp_sets, s->sp_size, s->sp_rowptr, s->sp_scan, s->sp_bucket, s->sp_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (s->sp_host) cudaFreeHost(s->sp_host);
     delete s;
     h->learned = nullptr;
 }
@@ -405,18 +408,33 @@ int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
     return FSD_OK;
 }
 
+// Blocks set through fsd_precond_set_blocks are used as given.  Otherwise G
+// is the two-hop sparse approximate inverse of the pruned matrix, plus the
+// loaded network's correction on the same pattern.
 int precond_build_learned(fsd_handle* h, const float4* pos) {
     LearnedState* s = learned(h);
-    if (!s->g_user) return FSD_ERR_BAD_PARAMS;  // no blocks set and no network loaded
     ProfRegion pr(h, R_PRECOND_BUILD);
-    if (h->p.learned_inner > 0) {
-        int e = inner_alloc(h);
+    int e = FSD_OK;
+    if (h->p.learned_inner > 0) e = inner_alloc(h);
+    if (e != FSD_OK) return e;
+    e = precond_assemble_pruned(h, pos, 1.0f, &s->a_pn, &s->a_plist, &s->a_blocks);
+    if (e != FSD_OK) return e;
+    if (!s->g_user) {
+        e = spai_build(h);
         if (e != FSD_OK) return e;
-        e = precond_assemble_pruned(h, pos, 1.0f, &s->a_pn, &s->a_plist, &s->a_blocks);
-        if (e != FSD_OK) return e;
+        if (mpnn_loaded(h)) {
+            e = mpnn_infer(h, pos, s->a_pn, s->a_plist, s->a_blocks);
+            if (e != FSD_OK) return e;
+        }
     }
     h->pc_valid = true;
     return FSD_OK;
+}
+
+int learned_set_weights(fsd_handle* h, const float* host_w, int n) {
+    const int e = mpnn_set_weights(h, host_w, n);
+    if (e == FSD_OK) learned(h)->g_user = false;
+    return e;
 }
 
 }  // namespace fsd

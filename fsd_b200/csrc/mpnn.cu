@@ -1,0 +1,1090 @@
+// Message-passing network for the learned block-sparse preconditioner:
+// graph construction, features, forward pass, the equivariant block head,
+// the approximate-inverse loss E_z ||A G z - z||^2 with its gradient,
+// backward pass and Adam.  Layout and formulas: fsd_mpnn.h.
+//
+// The dense layers go through mp_gemm (one interface, two kernels): the
+// tensor-core kernel of umma_gemm.cu with BF16 operands and FP32 accumulation,
+// or an FP32 SIMT kernel used as its check.  Everything else is FP32 with
+// FP64 reductions where a sum runs over the whole graph.  Every reduction has a
+// fixed order, so a training run is reproducible bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fsd_brownian.h"
+#include "fsd_device.cuh"
+#include "fsd_kernels.cuh"
+#include "fsd_learned.h"
+#include "fsd_mpnn.h"
+#include "fsd_profile.h"
+#include "fsd_solver.h"
+#include "fsd_umma.h"
+
+namespace fsd {
+
+namespace {
+constexpr int W = kMpWidth;
+constexpr int kThreads = 256;
+
+inline int nblk(size_t n, int t = kThreads) { return (int)std::min<size_t>((n + t - 1) / t, 148 * 16); }
+}  // namespace
+
+// ------------------------------------------------------------------ graph
+__global__ void k_g_count(const float4* __restrict__ pos, int N, Box b, const unsigned* __restrict__ nneigh,
+                          const unsigned* __restrict__ nlist, int stride, float rg2, unsigned* cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 pi = pos[i];
+    unsigned c = 0;
+    for (unsigned q = 0; q < nneigh[i]; ++q) {
+        const float4 pj = pos[nlist[(size_t)i * stride + q]];
+        const float3 r = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
+        if (dist2_rn(r) < rg2) ++c;
+    }
+    cnt[i] = c;
+}
+
+// Edges of row i in neighbour-list order; rhat = (unit vector i -> j, distance).
+__global__ void k_g_fill(const float4* __restrict__ pos, int N, Box b, const unsigned* __restrict__ nneigh,
+                         const unsigned* __restrict__ nlist, int stride, float rg2,
+                         const unsigned* __restrict__ rowptr, int* src, int* dst, float4* rhat) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 pi = pos[i];
+    unsigned e = rowptr[i];
+    for (unsigned q = 0; q < nneigh[i]; ++q) {
+        const unsigned j = nlist[(size_t)i * stride + q];
+        const float4 pj = pos[j];
+        const float3 r = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
+        const float d2 = dist2_rn(r);
+        if (d2 < rg2) {
+            const float d = sqrtf(d2);
+            src[e] = i;
+            dst[e] = (int)j;
+            rhat[e] = make_float4(r.x / d, r.y / d, r.z / d, d);
+            ++e;
+        }
+    }
+}
+
+// rev[e] = position of the opposite edge j -> i (or -1 if absent).
+__global__ void k_g_rev(const unsigned* __restrict__ rowptr, const int* __restrict__ src, const int* __restrict__ dst,
+                        int E, int* rev) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int i = src[e], j = dst[e];
+    int r = -1;
+    for (unsigned f = rowptr[j]; f < rowptr[j + 1]; ++f)
+        if (dst[f] == i) {
+            r = (int)f;
+            break;
+        }
+    rev[e] = r;
+}
+
+__device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x) * 0.25f; }
+
+// Rotation-invariant edge features.
+__global__ void k_g_feat(const float4* __restrict__ rhat, int E, ResTable tab, float* x) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const float r = rhat[e].w;
+    const float h = r - 2.0f;
+    float c[10];
+    res_interp<10>(tab, r, 0, c);
+    float* o = x + (size_t)e * kMpFeat;
+    o[0] = logf(fmaxf(h, 1e-4f)) * 0.2f;
+    o[1] = h;
+    o[2] = expf(-10.0f * fmaxf(h, 0.0f));
+    o[3] = 2.0f / r;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) o[4 + k] = slog(c[k]);
+    o[14] = 1.0f;
+    o[15] = 0.0f;
+}
+
+// J_i = (A_ii)^-1 for the self block of the pruned matrix (FP64 Gauss-Jordan
+// on an SPD 6x6 block), and the row's degree in the G graph.
+__global__ void k_g_jinv(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist,
+                         const float* __restrict__ A, int N, float* J) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int s = 0;
+    for (unsigned q = 0; q < pn[i]; ++q)
+        if (plist[(size_t)i * kPrunedCap + q] == (unsigned)i) s = (int)q;
+    const float* a = A + ((size_t)i * kPrunedCap + s) * 36;
+    double m[6][12];
+    for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 12; ++c) m[r][c] = (c < 6) ? (double)a[r * 6 + c] : (c - 6 == r ? 1.0 : 0.0);
+    for (int c = 0; c < 6; ++c) {
+        int p = c;
+        for (int r = c + 1; r < 6; ++r)
+            if (fabs(m[r][c]) > fabs(m[p][c])) p = r;
+        if (p != c)
+            for (int q = 0; q < 12; ++q) {
+                const double t = m[c][q];
+                m[c][q] = m[p][q];
+                m[p][q] = t;
+            }
+        const double piv = m[c][c];
+        const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+        for (int q = 0; q < 12; ++q) m[c][q] *= inv;
+        for (int r = 0; r < 6; ++r)
+            if (r != c) {
+                const double f = m[r][c];
+                for (int q = 0; q < 12; ++q) m[r][q] -= f * m[c][q];
+            }
+    }
+    for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c) J[(size_t)i * 36 + r * 6 + c] = (float)m[r][6 + c];
+}
+
+// ------------------------------------------------------------ SIMT GEMM
+// Y[r][o] = act(sum_k X(r,k) W[o][k] + b[o]) (+ R[r][o]), with X a row-wise
+// concatenation of up to three 64-wide (or one 16-wide) parts, each part read
+// through an optional row index.  64 rows x 64 outputs per block, 4x4 per thread.
+struct GemmIn {
+    const float* p[3];
+    const int* idx[3];
+    int width;   // columns per part (64, or 16 for the input layer)
+    int parts;
+};
+
+__global__ void __launch_bounds__(256) k_gemm_simt(GemmIn in, int rows, const float* __restrict__ Wt, int O,
+                                                   const float* __restrict__ bias, int relu,
+                                                   const float* __restrict__ resid, float* __restrict__ Y,
+                                                   int ldy) {
+    __shared__ float xs[16][65];
+    __shared__ float ws[16][65];
+    const int K = in.width * in.parts;
+    const int r0 = blockIdx.x * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int kk = t & 15, rr = t >> 4;
+            const int k = k0 + kk;
+            const int part = k / in.width, col = k - part * in.width;
+            const int r = r0 + rr;
+            float v = 0.f;
+            if (r < rows) {
+                const int src = in.idx[part] ? in.idx[part][r] : r;
+                v = in.p[part][(size_t)src * in.width + col];
+            }
+            xs[kk][rr] = v;
+            ws[kk][rr] = (rr < O) ? Wt[(size_t)rr * K + k] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float xv[4], wv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) xv[a] = xs[kk][ty * 4 + a];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) wv[c] = ws[kk][tx * 4 + c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] += xv[a] * wv[c];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + ty * 4 + a;
+        if (r >= rows) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int o = tx * 4 + c;
+            if (o >= O) continue;
+            float v = acc[a][c] + bias[o];
+            if (relu) v = fmaxf(v, 0.f);
+            if (resid) v += resid[(size_t)r * ldy + o];
+            Y[(size_t)r * ldy + o] = v;
+        }
+    }
+}
+
+// dX[r][k] = sum_o dY[r][o] W[o][k]   (dX dense, K columns)
+__global__ void __launch_bounds__(256) k_gemm_dx_simt(const float* __restrict__ dY, int rows, int O,
+                                                      const float* __restrict__ Wt, int K, float* __restrict__ dX) {
+    __shared__ float ds[16][65];
+    __shared__ float ws[16][65];
+    const int r0 = blockIdx.x * 64, k0b = blockIdx.y * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4] = {};
+    for (int o0 = 0; o0 < O; o0 += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int oo = t & 15, rr = t >> 4;
+            const int o = o0 + oo, r = r0 + rr, k = k0b + rr;
+            ds[oo][rr] = (r < rows && o < O) ? dY[(size_t)r * O + o] : 0.f;
+            ws[oo][rr] = (k < K && o < O) ? Wt[(size_t)o * K + k] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int oo = 0; oo < 16; ++oo) {
+            float dv[4], wv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) dv[a] = ds[oo][ty * 4 + a];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) wv[c] = ws[oo][tx * 4 + c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[a][c] += dv[a] * wv[c];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int r = r0 + ty * 4 + a;
+        if (r >= rows) continue;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int k = k0b + tx * 4 + c;
+            if (k < K) dX[(size_t)r * K + k] = acc[a][c];
+        }
+    }
+}
+
+// Partial weight gradients: part[blk][o][k] = sum over the block's rows of
+// dY[r][o] X(r,k), and part[blk][o][K] = sum dY[r][o] (bias).  One block per
+// kRowsPerPart rows; a second kernel sums the partials in block order.
+constexpr int kRowsPerPart = 512;
+
+__global__ void __launch_bounds__(256) k_gemm_dw_part(GemmIn in, int rows, const float* __restrict__ dY, int O,
+                                                      float* __restrict__ part) {
+    const int K = in.width * in.parts;
+    const int r0 = blockIdx.x * kRowsPerPart;
+    const int r1 = min(rows, r0 + kRowsPerPart);
+    const int KK = K + 1;
+    float* out = part + (size_t)blockIdx.x * O * KK;
+    for (int t = threadIdx.x; t < O * KK; t += blockDim.x) {
+        const int o = t / KK, k = t - o * KK;
+        float s = 0.f;
+        if (k < K) {
+            const int p = k / in.width, col = k - p * in.width;
+            for (int r = r0; r < r1; ++r) {
+                const int src = in.idx[p] ? in.idx[p][r] : r;
+                s += dY[(size_t)r * O + o] * in.p[p][(size_t)src * in.width + col];
+            }
+        } else {
+            for (int r = r0; r < r1; ++r) s += dY[(size_t)r * O + o];
+        }
+        out[t] = s;
+    }
+}
+
+// dW[o][k] += sum_blk part, db[o] += sum_blk part[..][K].
+__global__ void k_gemm_dw_reduce(const float* __restrict__ part, int nparts, int O, int K, float* dW, float* db) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int KK = K + 1;
+    if (t >= O * KK) return;
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += part[(size_t)b * O * KK + t];
+    const int o = t / KK, k = t - o * KK;
+    if (k < K) dW[(size_t)o * K + k] += (float)s;
+    else db[o] += (float)s;
+}
+
+// ----------------------------------------------------------- aggregation
+// out[i] = mean over row i's edges of in[e] (64 wide).  One warp per row, two
+// columns per lane.
+__global__ void k_seg_mean(const unsigned* __restrict__ rowptr, const float* __restrict__ in, int N, float* out) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    const unsigned b = rowptr[i], e = rowptr[i + 1];
+    float s0 = 0.f, s1 = 0.f;
+    for (unsigned f = b; f < e; ++f) {
+        s0 += in[(size_t)f * W + lane];
+        s1 += in[(size_t)f * W + 32 + lane];
+    }
+    const float inv = e > b ? 1.0f / (float)(e - b) : 0.f;
+    out[(size_t)i * W + lane] = s0 * inv;
+    out[(size_t)i * W + 32 + lane] = s1 * inv;
+}
+
+// d(in)[e] (+)= d(out)[src(e)] / deg(src(e))
+__global__ void k_seg_mean_bwd(const unsigned* __restrict__ rowptr, const float* __restrict__ dout, int N,
+                               float* din, int accumulate) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    const unsigned b = rowptr[i], e = rowptr[i + 1];
+    const float inv = e > b ? 1.0f / (float)(e - b) : 0.f;
+    const float g0 = dout[(size_t)i * W + lane] * inv, g1 = dout[(size_t)i * W + 32 + lane] * inv;
+    for (unsigned f = b; f < e; ++f) {
+        if (accumulate) {
+            din[(size_t)f * W + lane] += g0;
+            din[(size_t)f * W + 32 + lane] += g1;
+        } else {
+            din[(size_t)f * W + lane] = g0;
+            din[(size_t)f * W + 32 + lane] = g1;
+        }
+    }
+}
+
+// Node gradients from a gathered-edge input gradient dX (E x ldx), parts at
+// column offsets cs (gathered by src) and cd (gathered by dst):
+// dh[i] += sum_{e in row i} dX[e][cs + :] + dX[rev(e)][cd + :].
+__global__ void k_node_from_edges(const unsigned* __restrict__ rowptr, const int* __restrict__ rev,
+                                  const float* __restrict__ dX, int ldx, int cs, int cd, int N, float* dh) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    float s0 = 0.f, s1 = 0.f;
+    for (unsigned f = rowptr[i]; f < rowptr[i + 1]; ++f) {
+        s0 += dX[(size_t)f * ldx + cs + lane];
+        s1 += dX[(size_t)f * ldx + cs + 32 + lane];
+        const int r = rev[f];
+        if (r >= 0) {
+            s0 += dX[(size_t)r * ldx + cd + lane];
+            s1 += dX[(size_t)r * ldx + cd + 32 + lane];
+        }
+    }
+    dh[(size_t)i * W + lane] += s0;
+    dh[(size_t)i * W + 32 + lane] += s1;
+}
+
+// y[r][c] = x[r][coff + c] * (mask[r][c] > 0) for a 64-wide slice (ReLU backward
+// through a stored post-activation), optionally accumulated.
+__global__ void k_relu_bwd(const float* __restrict__ g, int ldg, int goff, const float* __restrict__ act, size_t rows,
+                           float* __restrict__ out) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= rows * W) return;
+    const size_t r = t / W;
+    const int c = (int)(t - r * W);
+    out[t] = act[t] > 0.f ? g[r * ldg + goff + c] : 0.f;
+}
+
+__global__ void k_add_slice(const float* __restrict__ g, int ldg, int goff, size_t rows, float* __restrict__ out) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= rows * W) return;
+    const size_t r = t / W;
+    out[t] += g[r * ldg + goff + (int)(t - r * W)];
+}
+
+// ------------------------------------------------------------------ head
+__device__ __forceinline__ void axis_block(const float* o, float3 r, float* B) {
+    // B(o, r): [o0 rr + o1 (I - rr), o2 [r]x ; o3 [r]x, o4 rr + o5 (I - rr)]
+    const float rv[3] = {r.x, r.y, r.z};
+    // [r]x v = r x v:  rows (0, -rz, ry), (rz, 0, -rx), (-ry, rx, 0)
+    const float cx[3][3] = {{0.f, -r.z, r.y}, {r.z, 0.f, -r.x}, {-r.y, r.x, 0.f}};
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const float rr = rv[a] * rv[b];
+            const float id = (a == b) ? 1.f : 0.f;
+            B[a * 6 + b] = o[0] * rr + o[1] * (id - rr);
+            B[a * 6 + 3 + b] = o[2] * cx[a][b];
+            B[(3 + a) * 6 + b] = o[3] * cx[a][b];
+            B[(3 + a) * 6 + 3 + b] = o[4] * rr + o[5] * (id - rr);
+        }
+}
+
+// <dB, dB/do_k> for the six basis tensors of axis_block.
+__device__ __forceinline__ void axis_block_grad(const float* dB, float3 r, float* go) {
+    const float rv[3] = {r.x, r.y, r.z};
+    const float cx[3][3] = {{0.f, -r.z, r.y}, {r.z, 0.f, -r.x}, {-r.y, r.x, 0.f}};
+    float g[6] = {};
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const float rr = rv[a] * rv[b];
+            const float id = (a == b) ? 1.f : 0.f;
+            g[0] += dB[a * 6 + b] * rr;
+            g[1] += dB[a * 6 + b] * (id - rr);
+            g[2] += dB[a * 6 + 3 + b] * cx[a][b];
+            g[3] += dB[(3 + a) * 6 + b] * cx[a][b];
+            g[4] += dB[(3 + a) * 6 + 3 + b] * rr;
+            g[5] += dB[(3 + a) * 6 + 3 + b] * (id - rr);
+        }
+    for (int k = 0; k < 6; ++k) go[k] = g[k];
+}
+
+// G in block CSR: row i = [self, edges of i].  One thread per row.
+__global__ void k_head_blocks(const unsigned* __restrict__ rowptr, const float4* __restrict__ rhat,
+                              const float* __restrict__ oe, const float* __restrict__ on, const float* __restrict__ J,
+                              int N, int* g_rowptr, int* g_col, const int* __restrict__ dst, float* G) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > N) return;
+    if (i == N) {
+        g_rowptr[N] = (int)rowptr[N] + N;
+        return;
+    }
+    const unsigned b = rowptr[i], e = rowptr[i + 1];
+    const int base = (int)b + i;
+    g_rowptr[i] = base;
+    float Ji[36];
+    for (int k = 0; k < 36; ++k) Ji[k] = J[(size_t)i * 36 + k];
+    float S[36];
+    for (int k = 0; k < 36; ++k) S[k] = 0.f;
+    const float ct = on[(size_t)i * kMpHeadN + 0], cr = on[(size_t)i * kMpHeadN + 1];
+    for (int d = 0; d < 6; ++d) S[d * 7] = 1.0f + (d < 3 ? ct : cr);
+    float B[36];
+    for (unsigned f = b; f < e; ++f) {
+        const float4 rh = rhat[f];
+        const float3 r = make_float3(rh.x, rh.y, rh.z);
+        axis_block(oe + (size_t)f * kMpHeadE + 6, r, B);
+        for (int k = 0; k < 36; ++k) S[k] += B[k];
+        axis_block(oe + (size_t)f * kMpHeadE, r, B);
+        float* out = G + (size_t)(base + 1 + (f - b)) * 36;
+        for (int a = 0; a < 6; ++a)
+            for (int c = 0; c < 6; ++c) {
+                float s = 0.f;
+                for (int q = 0; q < 6; ++q) s += Ji[a * 6 + q] * B[q * 6 + c];
+                out[a * 6 + c] = s;
+            }
+        g_col[base + 1 + (f - b)] = dst[f];
+    }
+    float* out = G + (size_t)base * 36;
+    for (int a = 0; a < 6; ++a)
+        for (int c = 0; c < 6; ++c) {
+            float s = 0.f;
+            for (int q = 0; q < 6; ++q) s += Ji[a * 6 + q] * S[q * 6 + c];
+            out[a * 6 + c] = s;
+        }
+    g_col[base] = i;
+}
+
+// From dG (block CSR like G) to head gradients: dB = J_i^T dG.
+__global__ void k_head_bwd(const unsigned* __restrict__ rowptr, const float4* __restrict__ rhat,
+                           const float* __restrict__ J, const float* __restrict__ dG, int N, float* doe, float* don) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const unsigned b = rowptr[i], e = rowptr[i + 1];
+    const int base = (int)b + i;
+    float Ji[36];
+    for (int k = 0; k < 36; ++k) Ji[k] = J[(size_t)i * 36 + k];
+    float dS[36];
+    {
+        const float* g = dG + (size_t)base * 36;
+        for (int a = 0; a < 6; ++a)
+            for (int c = 0; c < 6; ++c) {
+                float s = 0.f;
+                for (int q = 0; q < 6; ++q) s += Ji[q * 6 + a] * g[q * 6 + c];
+                dS[a * 6 + c] = s;
+            }
+    }
+    don[(size_t)i * kMpHeadN + 0] = dS[0] + dS[7] + dS[14];
+    don[(size_t)i * kMpHeadN + 1] = dS[21] + dS[28] + dS[35];
+    for (int k = 2; k < kMpHeadN; ++k) don[(size_t)i * kMpHeadN + k] = 0.f;
+    float dB[36], go[6];
+    for (unsigned f = b; f < e; ++f) {
+        const float4 rh = rhat[f];
+        const float3 r = make_float3(rh.x, rh.y, rh.z);
+        const float* g = dG + (size_t)(base + 1 + (f - b)) * 36;
+        for (int a = 0; a < 6; ++a)
+            for (int c = 0; c < 6; ++c) {
+                float s = 0.f;
+                for (int q = 0; q < 6; ++q) s += Ji[q * 6 + a] * g[q * 6 + c];
+                dB[a * 6 + c] = s;
+            }
+        float* d = doe + (size_t)f * kMpHeadE;
+        axis_block_grad(dB, r, go);
+        for (int k = 0; k < 6; ++k) d[k] = go[k];
+        axis_block_grad(dS, r, go);
+        for (int k = 0; k < 6; ++k) d[6 + k] = go[k];
+        for (int k = 12; k < kMpHeadE; ++k) d[k] = 0.f;
+    }
+}
+
+// ------------------------------------------------------------------ loss
+// u = G Z for P probe columns stored probe-major (P x 6N).
+__global__ void k_bsr_multi(const int* __restrict__ rowptr, const int* __restrict__ col, const float* __restrict__ G,
+                            const float* __restrict__ Z, float* __restrict__ U, int N, int P) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid >> 3, r = threadIdx.x & 7;
+    if (i >= N) return;
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const size_t n6 = 6 * (size_t)N;
+    for (int p = 0; p < P; ++p) {
+        float acc = 0.f;
+        for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+            const int j = col[e];
+            const float xj = (r < 6) ? Z[p * n6 + 6 * j + r] : 0.f;
+            const float* Ge = G + (size_t)e * 36 + (r < 6 ? r : 0) * 6;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const float xc = __shfl_sync(gmask, xj, c, 8);
+                if (r < 6) acc += Ge[c] * xc;
+            }
+        }
+        if (r < 6) U[p * n6 + 6 * i + r] = acc;
+    }
+}
+
+__global__ void k_pruned_multi(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist,
+                               const float* __restrict__ A, const float* __restrict__ X, float* __restrict__ Y, int N,
+                               int P) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid >> 3, r = threadIdx.x & 7;
+    if (i >= N) return;
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const size_t n6 = 6 * (size_t)N;
+    for (int p = 0; p < P; ++p) {
+        float acc = 0.f;
+        for (unsigned s = 0; s < pn[i]; ++s) {
+            const size_t e = (size_t)i * kPrunedCap + s;
+            const unsigned j = plist[e];
+            const float xj = (r < 6) ? X[p * n6 + 6 * j + r] : 0.f;
+            const float* Ae = A + e * 36 + (r < 6 ? r : 0) * 6;
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const float xc = __shfl_sync(gmask, xj, c, 8);
+                if (r < 6) acc += Ae[c] * xc;
+            }
+        }
+        if (r < 6) Y[p * n6 + 6 * i + r] = acc;
+    }
+}
+
+// R = (V - Z) * scale in place of V; part[b] = partial sum (V - Z)^2.
+__global__ void __launch_bounds__(kThreads) k_resid(float* V, const float* __restrict__ Z, size_t n, float scale,
+                                                    double* part) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const float d = V[k] - Z[k];
+        s += (double)d * d;
+        V[k] = d * scale;
+    }
+    s = group_sum_d<32>(s);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        v = group_sum_d<32>(v);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_sum_part(const double* part, int nb, double scale, double* out) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nb; b += 32) s += part[b];
+    s = group_sum_d<32>(s);
+    if (threadIdx.x == 0) *out = s * scale;
+}
+
+// dG block (i, col e) = sum_p dU_p[i] Z_p[j]^T.
+__global__ void k_dG(const int* __restrict__ rowptr, const int* __restrict__ col, const float* __restrict__ dU,
+                     const float* __restrict__ Z, int N, int P, float* dG) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const size_t n6 = 6 * (size_t)N;
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+        const int j = col[e];
+        float g[36] = {};
+        for (int p = 0; p < P; ++p) {
+            const float* du = dU + p * n6 + 6 * (size_t)i;
+            const float* z = Z + p * n6 + 6 * (size_t)j;
+            for (int a = 0; a < 6; ++a)
+                for (int c = 0; c < 6; ++c) g[a * 6 + c] += du[a] * z[c];
+        }
+        float* out = dG + (size_t)e * 36;
+        for (int k = 0; k < 36; ++k) out[k] = g[k];
+    }
+}
+
+// ------------------------------------------------------------------ Adam
+__global__ void k_adam(float* w, const float* __restrict__ g, float* m, float* v, int n, float lr, float b1, float b2,
+                       float c1, float c2, float eps, float clip) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float gk = g[k];
+    gk = fminf(fmaxf(gk, -clip), clip);
+    const float mk = b1 * m[k] + (1.f - b1) * gk;
+    const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    w[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+}
+
+// ------------------------------------------------------------ host side
+struct MpState {
+    int N = 0;
+    int E = 0, E_cap = 0;
+    float rg = 0.f;
+    unsigned* cnt = nullptr;     // N+1 (scan output)
+    unsigned* scan = nullptr;
+    int* src = nullptr;
+    int* dst = nullptr;
+    int* rev = nullptr;
+    float4* rhat = nullptr;
+    float* x = nullptr;          // E x 16
+    float* J = nullptr;          // N x 36
+    // activations
+    float* e[kMpLayers + 1] = {};
+    float* m[kMpLayers] = {};
+    float* h[kMpLayers + 1] = {};
+    float* a[kMpLayers] = {};
+    float* u[kMpLayers] = {};    // relu(W_h [h, a] + b) per layer
+    float* oe = nullptr;         // E x 16
+    float* on = nullptr;         // N x 16
+    // backward
+    float* dX = nullptr;         // E x 192
+    float* dXn = nullptr;        // N x 128
+    float* de = nullptr;         // E x 64
+    float* dm = nullptr;         // E x 64
+    float* dh = nullptr;         // N x 64
+    float* dh2 = nullptr;        // N x 64
+    float* dA = nullptr;         // N x 64
+    float* du = nullptr;         // N x 64
+    float* doe = nullptr;
+    float* don = nullptr;
+    float* dG = nullptr;
+    float* dwpart = nullptr;
+    size_t dwpart_cap = 0;
+    // weights
+    float* w = nullptr;
+    float* gw = nullptr;
+    float* mw = nullptr;
+    float* vw = nullptr;
+    bool loaded = false;
+    int adam_t = 0;
+    // probes
+    float* Zp = nullptr;
+    float* Up = nullptr;
+    float* Vp = nullptr;
+    int P_cap = 0;
+    double* part = nullptr;
+    double* loss = nullptr;
+    bool use_umma = true;
+    std::vector<unsigned> h_cnt;
+};
+
+static MpState* mp(fsd_handle* h) {
+    LearnedState* s = learned(h);
+    if (!s->mp) s->mp = new MpState();
+    return (MpState*)s->mp;
+}
+
+template <class T> static int grow(T** p, size_t n) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    FSD_CHECK_CUDA(cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(n, 1)));
+    return FSD_OK;
+}
+
+#define MP_TRY(x)                   \
+    do {                            \
+        int s_ = (x);               \
+        if (s_ != FSD_OK) return s_; \
+    } while (0)
+
+void mpnn_free(fsd_handle* h) {
+    LearnedState* ls = (LearnedState*)h->learned;
+    if (!ls || !ls->mp) return;
+    MpState* s = (MpState*)ls->mp;
+    void* ptrs[] = {s->cnt, s->scan, s->src, s->dst, s->rev, s->rhat, s->x, s->J, s->oe, s->on, s->dX, s->dXn, s->de,
+                    s->dm, s->dh, s->dh2, s->dA, s->du, s->doe, s->don, s->dG, s->dwpart, s->w, s->gw, s->mw, s->vw,
+                    s->Zp, s->Up, s->Vp, s->part, s->loss};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (int l = 0; l <= kMpLayers; ++l) {
+        if (s->e[l]) cudaFree(s->e[l]);
+        if (s->h[l]) cudaFree(s->h[l]);
+    }
+    for (int l = 0; l < kMpLayers; ++l) {
+        if (s->m[l]) cudaFree(s->m[l]);
+        if (s->a[l]) cudaFree(s->a[l]);
+        if (s->u[l]) cudaFree(s->u[l]);
+    }
+    delete s;
+    ls->mp = nullptr;
+}
+
+static int mp_alloc_static(fsd_handle* h) {
+    MpState* s = mp(h);
+    if (s->N) return FSD_OK;
+    const int N = h->p.N;
+    s->N = N;
+    MP_TRY(grow(&s->cnt, N + 1));
+    MP_TRY(grow(&s->scan, scan_scratch_elems(N)));
+    MP_TRY(grow(&s->J, (size_t)N * 36));
+    for (int l = 0; l <= kMpLayers; ++l) MP_TRY(grow(&s->h[l], (size_t)N * W));
+    for (int l = 0; l < kMpLayers; ++l) {
+        MP_TRY(grow(&s->a[l], (size_t)N * W));
+        MP_TRY(grow(&s->u[l], (size_t)N * W));
+    }
+    MP_TRY(grow(&s->on, (size_t)N * kMpHeadN));
+    MP_TRY(grow(&s->w, MpLayout::total));
+    MP_TRY(grow(&s->gw, MpLayout::total));
+    MP_TRY(grow(&s->mw, MpLayout::total));
+    MP_TRY(grow(&s->vw, MpLayout::total));
+    MP_TRY(grow(&s->part, 4096));
+    MP_TRY(grow(&s->loss, 4));
+    s->h_cnt.resize(1);
+    return FSD_OK;
+}
+
+static int mp_alloc_edges(fsd_handle* h, int E) {
+    MpState* s = mp(h);
+    if (E <= s->E_cap) return FSD_OK;
+    const int cap = E + E / 8 + 1024;
+    MP_TRY(grow(&s->src, cap));
+    MP_TRY(grow(&s->dst, cap));
+    MP_TRY(grow(&s->rev, cap));
+    MP_TRY(grow(&s->rhat, cap));
+    MP_TRY(grow(&s->x, (size_t)cap * kMpFeat));
+    for (int l = 0; l <= kMpLayers; ++l) MP_TRY(grow(&s->e[l], (size_t)cap * W));
+    for (int l = 0; l < kMpLayers; ++l) MP_TRY(grow(&s->m[l], (size_t)cap * W));
+    MP_TRY(grow(&s->oe, (size_t)cap * kMpHeadE));
+    s->E_cap = cap;
+    // backward buffers are grown on first use (training only)
+    if (s->dX) {
+        cudaFree(s->dX);
+        s->dX = nullptr;
+    }
+    return FSD_OK;
+}
+
+static int mp_alloc_backward(fsd_handle* h) {
+    MpState* s = mp(h);
+    if (s->dX) return FSD_OK;
+    const int N = s->N;
+    const size_t cap = s->E_cap;
+    MP_TRY(grow(&s->dX, cap * 3 * W));
+    MP_TRY(grow(&s->dXn, (size_t)N * 2 * W));
+    MP_TRY(grow(&s->de, cap * W));
+    MP_TRY(grow(&s->dm, cap * W));
+    MP_TRY(grow(&s->dh, (size_t)N * W));
+    MP_TRY(grow(&s->dh2, (size_t)N * W));
+    MP_TRY(grow(&s->dA, (size_t)N * W));
+    MP_TRY(grow(&s->du, (size_t)N * W));
+    MP_TRY(grow(&s->doe, cap * kMpHeadE));
+    MP_TRY(grow(&s->don, (size_t)N * kMpHeadN));
+    MP_TRY(grow(&s->dG, (cap + N) * 36));
+    return FSD_OK;
+}
+
+// Dense layer through the tensor-core kernel (BF16 operands, FP32
+// accumulation) or the FP32 SIMT kernel.
+static void mp_gemm(fsd_handle* h, const GemmIn& in, int rows, const float* Wt, int O, const float* b, int relu,
+                    const float* resid, float* Y) {
+    MpState* s = mp(h);
+    if (rows <= 0) return;
+    count_launch();
+    if (s->use_umma && umma_gemm_supported(in.width * in.parts, O)) {
+        umma_gemm(in.p, in.idx, in.width, in.parts, rows, Wt, O, b, relu, resid, Y, h->stream);
+        return;
+    }
+    k_gemm_simt<<<(rows + 63) / 64, 256, 0, h->stream>>>(in, rows, Wt, O, b, relu, resid, Y, O);
+}
+
+static void mp_gemm_dx(fsd_handle* h, const float* dY, int rows, int O, const float* Wt, int K, float* dX) {
+    MpState* s = mp(h);
+    if (rows <= 0) return;
+    count_launch();
+    if (s->use_umma && umma_gemm_dx_supported(O, K)) {
+        umma_gemm_dx(dY, rows, O, Wt, K, dX, h->stream);
+        return;
+    }
+    dim3 g((rows + 63) / 64, (K + 63) / 64);
+    k_gemm_dx_simt<<<g, 256, 0, h->stream>>>(dY, rows, O, Wt, K, dX);
+}
+
+static int mp_gemm_dw(fsd_handle* h, const GemmIn& in, int rows, const float* dY, int O, float* dW, float* db) {
+    MpState* s = mp(h);
+    if (rows <= 0) return FSD_OK;
+    const int K = in.width * in.parts;
+    const int nparts = (rows + kRowsPerPart - 1) / kRowsPerPart;
+    const size_t need = (size_t)nparts * O * (K + 1);
+    if (need > s->dwpart_cap) {
+        MP_TRY(grow(&s->dwpart, need));
+        s->dwpart_cap = need;
+    }
+    count_launch();
+    k_gemm_dw_part<<<nparts, 256, 0, h->stream>>>(in, rows, dY, O, s->dwpart);
+    count_launch();
+    k_gemm_dw_reduce<<<(O * (K + 1) + 255) / 256, 256, 0, h->stream>>>(s->dwpart, nparts, O, K, dW, db);
+    return FSD_OK;
+}
+
+static GemmIn cat3(const float* e, const float* hs, const float* hd, const int* src, const int* dst) {
+    GemmIn g{};
+    g.p[0] = e;
+    g.p[1] = hs;
+    g.p[2] = hd;
+    g.idx[0] = nullptr;
+    g.idx[1] = src;
+    g.idx[2] = dst;
+    g.width = W;
+    g.parts = 3;
+    return g;
+}
+static GemmIn cat2(const float* a, const float* b) {
+    GemmIn g{};
+    g.p[0] = a;
+    g.p[1] = b;
+    g.width = W;
+    g.parts = 2;
+    return g;
+}
+static GemmIn one(const float* a, int width) {
+    GemmIn g{};
+    g.p[0] = a;
+    g.width = width;
+    g.parts = 1;
+    return g;
+}
+
+// Graph, features and J for these positions (neighbour list and the pruned
+// matrix must be current).
+static int mp_graph(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist,
+                    const float* a_blocks) {
+    MP_TRY(mp_alloc_static(h));
+    MpState* s = mp(h);
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
+    const float rg2 = h->p.learned_rg * h->p.learned_rg;
+    count_launch();
+    k_g_count<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride, rg2, s->cnt);
+    exclusive_scan(s->cnt, s->cnt, N, s->scan, st);
+    unsigned E = 0;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(&E, s->cnt + N, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    MP_TRY(mp_alloc_edges(h, (int)E));
+    s->E = (int)E;
+    count_launch();
+    k_g_fill<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride, rg2, s->cnt,
+                                              s->src, s->dst, s->rhat);
+    if (E) {
+        count_launch();
+        k_g_rev<<<(E + 255) / 256, 256, 0, st>>>(s->cnt, s->src, s->dst, (int)E, s->rev);
+        count_launch();
+        k_g_feat<<<(E + 255) / 256, 256, 0, st>>>(s->rhat, (int)E, ResTable{h->d_res_dist, h->d_res_vals}, s->x);
+    }
+    count_launch();
+    k_g_jinv<<<(N + 127) / 128, 128, 0, st>>>(a_pn, a_plist, a_blocks, N, s->J);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+static int mp_forward(fsd_handle* h) {
+    MpState* s = mp(h);
+    const int N = s->N, E = s->E;
+    cudaStream_t st = h->stream;
+    const float* w = s->w;
+    mp_gemm(h, one(s->x, kMpFeat), E, w + MpLayout::W_in, W, w + MpLayout::b_in, 1, nullptr, s->e[0]);
+    count_launch();
+    k_seg_mean<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->e[0], N, s->h[0]);
+    for (int l = 0; l < kMpLayers; ++l) {
+        const float* L = w + MpLayout::layer(l);
+        mp_gemm(h, cat3(s->e[l], s->h[l], s->h[l], s->src, s->dst), E, L + MpLayout::W_m, W, L + MpLayout::b_m, 1,
+                nullptr, s->m[l]);
+        // e[l+1] = e[l] + m[l]
+        FSD_CHECK_CUDA(cudaMemcpyAsync(s->e[l + 1], s->e[l], sizeof(float) * (size_t)E * W, cudaMemcpyDeviceToDevice,
+                                       st));
+        count_launch();
+        k_add_slice<<<(unsigned)(((size_t)E * W + 255) / 256), 256, 0, st>>>(s->m[l], W, 0, E, s->e[l + 1]);
+        count_launch();
+        k_seg_mean<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->m[l], N, s->a[l]);
+        mp_gemm(h, cat2(s->h[l], s->a[l]), N, L + MpLayout::W_h, W, L + MpLayout::b_h, 1, nullptr, s->u[l]);
+        FSD_CHECK_CUDA(cudaMemcpyAsync(s->h[l + 1], s->h[l], sizeof(float) * (size_t)N * W, cudaMemcpyDeviceToDevice,
+                                       st));
+        count_launch();
+        k_add_slice<<<(unsigned)(((size_t)N * W + 255) / 256), 256, 0, st>>>(s->u[l], W, 0, N, s->h[l + 1]);
+    }
+    mp_gemm(h, cat3(s->e[kMpLayers], s->h[kMpLayers], s->h[kMpLayers], s->src, s->dst), E, w + MpLayout::W_o,
+            kMpHeadE, w + MpLayout::b_o, 0, nullptr, s->oe);
+    mp_gemm(h, one(s->h[kMpLayers], W), N, w + MpLayout::W_n, kMpHeadN, w + MpLayout::b_n, 0, nullptr, s->on);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// G blocks into the learned state's block CSR.
+static int mp_head(fsd_handle* h) {
+    MpState* s = mp(h);
+    LearnedState* ls = learned(h);
+    const int N = s->N;
+    MP_TRY(learned_reserve(h, s->E + N));
+    count_launch();
+    k_head_blocks<<<(N + 1 + 127) / 128, 128, 0, h->stream>>>(s->cnt, s->rhat, s->oe, s->on, s->J, N, ls->g_rowptr,
+                                                              ls->g_col, s->dst, ls->g_val);
+    ls->g_nnzb = s->E + N;
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// Backward from d(oe), d(on) to the weight gradient s->gw (accumulated).
+static int mp_backward(fsd_handle* h) {
+    MpState* s = mp(h);
+    const int N = s->N, E = s->E;
+    cudaStream_t st = h->stream;
+    const float* w = s->w;
+    float* gw = s->gw;
+    const size_t EW = (size_t)E * W, NW = (size_t)N * W;
+    const unsigned ge = (unsigned)((EW + 255) / 256), gn = (unsigned)((NW + 255) / 256);
+    // heads
+    MP_TRY(mp_gemm_dw(h, one(s->h[kMpLayers], W), N, s->don, kMpHeadN, gw + MpLayout::W_n, gw + MpLayout::b_n));
+    mp_gemm_dx(h, s->don, N, kMpHeadN, w + MpLayout::W_n, W, s->dh);  // dh = d h3 (node head)
+    MP_TRY(mp_gemm_dw(h, cat3(s->e[kMpLayers], s->h[kMpLayers], s->h[kMpLayers], s->src, s->dst), E, s->doe, kMpHeadE,
+                      gw + MpLayout::W_o, gw + MpLayout::b_o));
+    mp_gemm_dx(h, s->doe, E, kMpHeadE, w + MpLayout::W_o, 3 * W, s->dX);
+    // de = dX[:, 0:64]; dh += gathered parts
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->de, 0, sizeof(float) * EW, st));
+    count_launch();
+    k_add_slice<<<ge, 256, 0, st>>>(s->dX, 3 * W, 0, E, s->de);
+    count_launch();
+    k_node_from_edges<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->rev, s->dX, 3 * W, W, 2 * W, N, s->dh);
+    for (int l = kMpLayers - 1; l >= 0; --l) {
+        const float* L = w + MpLayout::layer(l);
+        float* GL = gw + MpLayout::layer(l);
+        // h[l+1] = h[l] + u[l], u = relu(W_h [h[l], a[l]] + b_h)
+        count_launch();
+        k_relu_bwd<<<gn, 256, 0, st>>>(s->dh, W, 0, s->u[l], N, s->du);
+        MP_TRY(mp_gemm_dw(h, cat2(s->h[l], s->a[l]), N, s->du, W, GL + MpLayout::W_h, GL + MpLayout::b_h));
+        mp_gemm_dx(h, s->du, N, W, L + MpLayout::W_h, 2 * W, s->dXn);
+        // d h[l] = dh (residual) + dXn[:, 0:64];  d a[l] = dXn[:, 64:128]
+        count_launch();
+        k_add_slice<<<gn, 256, 0, st>>>(s->dXn, 2 * W, 0, N, s->dh);
+        // a = seg_mean(m): dm = d a / deg scattered to edges;  e[l+1] = e[l] + m: dm += de
+        FSD_CHECK_CUDA(cudaMemcpy2DAsync(s->dA, sizeof(float) * W, s->dXn + W, sizeof(float) * 2 * W,
+                                         sizeof(float) * W, N, cudaMemcpyDeviceToDevice, st));
+        count_launch();
+        k_seg_mean_bwd<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->dA, N, s->dm, 0);
+        count_launch();
+        k_add_slice<<<ge, 256, 0, st>>>(s->de, W, 0, E, s->dm);
+        // m = relu(W_m [e[l], h[l]_src, h[l]_dst] + b_m)
+        count_launch();
+        k_relu_bwd<<<ge, 256, 0, st>>>(s->dm, W, 0, s->m[l], E, s->dm);
+        MP_TRY(mp_gemm_dw(h, cat3(s->e[l], s->h[l], s->h[l], s->src, s->dst), E, s->dm, W, GL + MpLayout::W_m,
+                          GL + MpLayout::b_m));
+        mp_gemm_dx(h, s->dm, E, W, L + MpLayout::W_m, 3 * W, s->dX);
+        // d e[l] = de (residual) + dX[:, 0:64];  d h[l] += gathered
+        count_launch();
+        k_add_slice<<<ge, 256, 0, st>>>(s->dX, 3 * W, 0, E, s->de);
+        count_launch();
+        k_node_from_edges<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->rev, s->dX, 3 * W, W, 2 * W, N, s->dh);
+    }
+    // h[0] = seg_mean(e[0]): de += scatter(dh / deg)
+    count_launch();
+    k_seg_mean_bwd<<<(N * 32 + 255) / 256, 256, 0, st>>>(s->cnt, s->dh, N, s->de, 1);
+    // e[0] = relu(W_in x + b_in)
+    count_launch();
+    k_relu_bwd<<<ge, 256, 0, st>>>(s->de, W, 0, s->e[0], E, s->dm);
+    MP_TRY(mp_gemm_dw(h, one(s->x, kMpFeat), E, s->dm, W, gw + MpLayout::W_in, gw + MpLayout::b_in));
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// Loss L = sum_p ||A G z_p - z_p||^2 / (P 6N) for the probes in s->Zp, and
+// (when grad) the gradient dL/dG into s->dG, then through the head.
+static int mp_loss(fsd_handle* h, int P, bool grad) {
+    MpState* s = mp(h);
+    LearnedState* ls = learned(h);
+    const int N = s->N;
+    cudaStream_t st = h->stream;
+    const size_t n = (size_t)P * 6 * N;
+    const int rows = (8 * N + 255) / 256;
+    count_launch();
+    k_bsr_multi<<<rows, 256, 0, st>>>(ls->g_rowptr, ls->g_col, ls->g_val, s->Zp, s->Up, N, P);
+    count_launch();
+    k_pruned_multi<<<rows, 256, 0, st>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Up, s->Vp, N, P);
+    const double inv = 1.0 / ((double)P * 6.0 * N);
+    count_launch();
+    k_resid<<<296, kThreads, 0, st>>>(s->Vp, s->Zp, n, (float)(2.0 * inv), s->part);
+    count_launch();
+    k_sum_part<<<1, 32, 0, st>>>(s->part, 296, inv, s->loss);
+    if (!grad) return FSD_OK;
+    // dU = A^T dR = A dR (A symmetric); dG_ie = sum_p dU_p[i] z_p[col]^T
+    count_launch();
+    k_pruned_multi<<<rows, 256, 0, st>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Vp, s->Up, N, P);
+    count_launch();
+    k_dG<<<(N + 127) / 128, 128, 0, st>>>(ls->g_rowptr, ls->g_col, s->Up, s->Zp, N, P, s->dG);
+    count_launch();
+    k_head_bwd<<<(N + 127) / 128, 128, 0, st>>>(s->cnt, s->rhat, s->J, s->dG, N, s->doe, s->don);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+static int mp_probes(fsd_handle* h, int P) {
+    MpState* s = mp(h);
+    if (P > s->P_cap) {
+        const size_t n = (size_t)P * 6 * s->N;
+        MP_TRY(grow(&s->Zp, n));
+        MP_TRY(grow(&s->Up, n));
+        MP_TRY(grow(&s->Vp, n));
+        s->P_cap = P;
+    }
+    return FSD_OK;
+}
+
+// ------------------------------------------------------------ entry points
+int mpnn_set_weights(fsd_handle* h, const float* host_w, int n) {
+    if (n != MpLayout::total) return FSD_ERR_BAD_PARAMS;
+    MP_TRY(mp_alloc_static(h));
+    MpState* s = mp(h);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->w, host_w, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->mw, 0, sizeof(float) * n, h->stream));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->vw, 0, sizeof(float) * n, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    s->adam_t = 0;
+    s->loaded = true;
+    return FSD_OK;
+}
+
+int mpnn_get_weights(fsd_handle* h, float* host_w, int n) {
+    MpState* s = mp(h);
+    if (n != MpLayout::total || !s->loaded) return FSD_ERR_BAD_PARAMS;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host_w, s->w, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return FSD_OK;
+}
+
+bool mpnn_loaded(fsd_handle* h) {
+    LearnedState* ls = (LearnedState*)h->learned;
+    return ls && ls->mp && ((MpState*)ls->mp)->loaded;
+}
+
+void mpnn_use_umma(fsd_handle* h, bool on) { mp(h)->use_umma = on; }
+
+// Inference: graph, forward, head -> G (precond_build of FSD_PRECOND_LEARNED).
+int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist,
+               const float* a_blocks) {
+    MP_TRY(mp_graph(h, pos, a_pn, a_plist, a_blocks));
+    MP_TRY(mp_forward(h));
+    return mp_head(h);
+}
+
+// Loss and gradient for given probes (host P x 6N, or NULL to draw standard
+// normals from (seed, step)); with lr > 0 also one Adam step.  The neighbour
+// list must be current for pos; the pruned matrix is assembled here.
+int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, int P, uint32_t step, float lr,
+                    float* loss_out, float* host_grad) {
+    LearnedState* ls = learned(h);
+    if (!mpnn_loaded(h) || P < 1) return FSD_ERR_BAD_PARAMS;
+    MpState* s = mp(h);
+    MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
+    MP_TRY(mpnn_infer(h, pos, ls->a_pn, ls->a_plist, ls->a_blocks));
+    MP_TRY(mp_alloc_backward(h));
+    MP_TRY(mp_probes(h, P));
+    const size_t n = (size_t)P * 6 * s->N;
+    if (host_probes)
+        FSD_CHECK_CUDA(cudaMemcpyAsync(s->Zp, host_probes, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+    else
+        gaussian(h, s->Zp, n, step, kStreamLearned, 1.0f);
+    MP_TRY(mp_loss(h, P, true));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->gw, 0, sizeof(float) * MpLayout::total, h->stream));
+    MP_TRY(mp_backward(h));
+    if (lr > 0.f) {
+        s->adam_t += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)s->adam_t), c2 = 1.f - powf(b2, (float)s->adam_t);
+        count_launch();
+        k_adam<<<(MpLayout::total + 255) / 256, 256, 0, h->stream>>>(s->w, s->gw, s->mw, s->vw, MpLayout::total, lr,
+                                                                     b1, b2, c1, c2, 1e-8f, 1.0f);
+    }
+    double loss = 0.0;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(&loss, s->loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (host_grad)
+        FSD_CHECK_CUDA(cudaMemcpyAsync(host_grad, s->gw, sizeof(float) * MpLayout::total, cudaMemcpyDeviceToHost,
+                                       h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (loss_out) *loss_out = (float)loss;
+    return FSD_OK;
+}
+
+}  // namespace fsd

@@ -1,0 +1,286 @@
+// Sparse approximate inverse of A = R_FU^pruned + D on the two-hop pattern of
+// the pruned contact graph (the base of FSD_PRECOND_LEARNED).
+//
+// For each particle c, S_c = {c} + pruned neighbours + their pruned
+// neighbours (first kSpaiCap, in that order).  The columns of A restricted to
+// S_c give the least-squares problem
+//     min || A[:, S_c] X_c - E_c ||_F,     E_c = the 6 columns of particle c,
+// whose normal equations (A^2)[S_c, S_c] X_c = A[S_c, c] are assembled and
+// solved by Cholesky in FP64, one CTA per particle with the packed normal
+// matrix in shared memory.  X_c is column c of a right approximate inverse,
+// A G ~ I (Grote and Huckle's SPAI with a fixed pattern), which suits the
+// right-preconditioned inner GMRES.
+// Launches are bucketed by |S_c| so small systems share an SM.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fsd_device.cuh"
+#include "fsd_kernels.cuh"
+#include "fsd_learned.h"
+#include "fsd_profile.h"
+#include "fsd_solver.h"
+
+namespace fsd {
+
+namespace {
+constexpr int kBuckets = 3;
+constexpr int kBucketMax[kBuckets] = {12, 20, kSpaiCap};
+__host__ __device__ constexpr int bucket_of(int n) { return n <= 12 ? 0 : (n <= 20 ? 1 : 2); }
+constexpr int kSpaiThreads = 128;
+
+inline size_t spai_smem(int m) {  // packed FP64 lower triangle + 6 right-hand sides + the set
+    const size_t n = 6 * (size_t)m;
+    return sizeof(double) * (n * (n + 1) / 2 + 6 * n) + sizeof(int) * kSpaiCap;
+}
+}  // namespace
+
+// Two-hop sets (c first, then the 1-hop list, then new 2-hop members in list
+// order), truncated at kSpaiCap; bucket lists for the solve launches.
+__global__ void k_spai_sets(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist, int N, int* sets,
+                            unsigned* ns, unsigned* bucket_cnt, int* bucket_list, int* truncated) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    int* S = sets + (size_t)c * kSpaiCap;
+    int n = 0;
+    bool over = false;
+    S[n++] = c;
+    const unsigned* row = plist + (size_t)c * kPrunedCap;
+    for (unsigned q = 0; q < pn[c]; ++q)
+        if ((int)row[q] != c) {
+            if (n < kSpaiCap) S[n++] = (int)row[q];
+            else over = true;
+        }
+    const int n1 = n;
+    for (int a = 1; a < n1; ++a) {
+        const int k = S[a];
+        const unsigned* rk = plist + (size_t)k * kPrunedCap;
+        for (unsigned q = 0; q < pn[k]; ++q) {
+            const int s = (int)rk[q];
+            bool seen = false;
+            for (int b = 0; b < n; ++b)
+                if (S[b] == s) {
+                    seen = true;
+                    break;
+                }
+            if (seen) continue;
+            if (n < kSpaiCap) S[n++] = s;
+            else over = true;
+        }
+    }
+    ns[c] = (unsigned)n;
+    if (over) atomicAdd(truncated, 1);
+    const int b = bucket_of(n);
+    const unsigned slot = atomicAdd(bucket_cnt + b, 1u);
+    bucket_list[(size_t)b * N + slot] = c;
+}
+
+__device__ __forceinline__ size_t tri(int i, int j) { return (size_t)i * (i + 1) / 2 + j; }  // i >= j
+
+// Block (s, k) of A from the pruned list of s (k must be on it), or null.
+__device__ __forceinline__ const float* a_block(const unsigned* pn, const unsigned* plist, const float* A, int s,
+                                                int k) {
+    const unsigned* row = plist + (size_t)s * kPrunedCap;
+    const unsigned n = pn[s];
+    for (unsigned q = 0; q < n; ++q)
+        if ((int)row[q] == k) return A + ((size_t)s * kPrunedCap + q) * 36;
+    return nullptr;
+}
+
+__global__ void __launch_bounds__(kSpaiThreads) k_spai_solve(const unsigned* __restrict__ pn,
+                                                             const unsigned* __restrict__ plist,
+                                                             const float* __restrict__ A,
+                                                             const int* __restrict__ sets,
+                                                             const unsigned* __restrict__ ns,
+                                                             const unsigned* __restrict__ bucket_cnt,
+                                                             const int* __restrict__ bucket_list, int bucket, int N,
+                                                             const int* __restrict__ rowptr, int* g_col, float* g_val,
+                                                             int* fail) {
+    if (blockIdx.x >= bucket_cnt[bucket]) return;
+    const int c = bucket_list[(size_t)bucket * N + blockIdx.x];
+    extern __shared__ double sm[];
+    const int m = (int)ns[c];
+    const int n = 6 * m;
+    double* H = sm;                               // packed lower triangle, n(n+1)/2
+    double* R = sm + (size_t)n * (n + 1) / 2;     // n x 6, row-major
+    int* S = (int*)(R + 6 * (size_t)n);
+    for (int a = threadIdx.x; a < m; a += blockDim.x) S[a] = sets[(size_t)c * kSpaiCap + a];
+    __syncthreads();
+    // Normal matrix: H[a][b] = sum_k A_{s_a k} A_{s_b k}^T over k in both pruned lists (b <= a).
+    const int npairs = m * (m + 1) / 2;
+    for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+        int a = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+        while ((a + 1) * (a + 2) / 2 <= t) ++a;
+        while (a * (a + 1) / 2 > t) --a;
+        const int b = t - a * (a + 1) / 2;
+        const int sa = S[a], sb = S[b];
+        double blk[36];
+        for (int q = 0; q < 36; ++q) blk[q] = 0.0;
+        const unsigned* ra = plist + (size_t)sa * kPrunedCap;
+        const unsigned* rb = plist + (size_t)sb * kPrunedCap;
+        unsigned ia = 0, ib = 0;
+        const unsigned na = pn[sa], nb = pn[sb];
+        while (ia < na && ib < nb) {
+            const unsigned ka = ra[ia], kb = rb[ib];
+            if (ka == kb) {
+                const float* Pa = A + ((size_t)sa * kPrunedCap + ia) * 36;
+                const float* Pb = A + ((size_t)sb * kPrunedCap + ib) * 36;
+                for (int r = 0; r < 6; ++r)
+                    for (int q = 0; q < 6; ++q) {
+                        double v = 0.0;
+                        for (int u = 0; u < 6; ++u) v += (double)Pa[r * 6 + u] * (double)Pb[q * 6 + u];
+                        blk[r * 6 + q] += v;
+                    }
+                ++ia;
+                ++ib;
+            } else if (ka < kb) {
+                ++ia;
+            } else {
+                ++ib;
+            }
+        }
+        for (int r = 0; r < 6; ++r)
+            for (int q = 0; q < 6; ++q) {
+                const int i = 6 * a + r, j = 6 * b + q;
+                if (i >= j) H[tri(i, j)] = blk[r * 6 + q];
+            }
+    }
+    // Right-hand sides: R[6a + r][q] = A_{s_a c}[r][q].
+    for (int a = threadIdx.x; a < m; a += blockDim.x) {
+        const float* blk = a_block(pn, plist, A, S[a], c);
+        for (int k = 0; k < 36; ++k) R[(size_t)(6 * a + k / 6) * 6 + k % 6] = blk ? (double)blk[k] : 0.0;
+    }
+    __syncthreads();
+    // Right-looking Cholesky in place.
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = H[tri(j, j)];
+            if (!(d > 0.0)) bad = 1;
+            H[tri(j, j)] = d > 0.0 ? sqrt(d) : 1.0;
+        }
+        __syncthreads();
+        const double piv = H[tri(j, j)];
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) H[tri(i, j)] /= piv;
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+            const double lij = H[tri(i, j)];
+            for (int k = j + 1; k <= i; ++k) H[tri(i, k)] -= lij * H[tri(k, j)];
+        }
+        __syncthreads();
+    }
+    // Forward and backward substitution, one warp per right-hand side.
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = warp; q < 6; q += blockDim.x >> 5) {
+        for (int i = 0; i < n; ++i) {
+            double s = 0.0;
+            for (int k = lane; k < i; k += 32) s += H[tri(i, k)] * R[(size_t)k * 6 + q];
+            s = group_sum_d<32>(s);
+            if (lane == 0) R[(size_t)i * 6 + q] = (R[(size_t)i * 6 + q] - s) / H[tri(i, i)];
+            __syncwarp();
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double s = 0.0;
+            for (int k = i + 1 + lane; k < n; k += 32) s += H[tri(k, i)] * R[(size_t)k * 6 + q];
+            s = group_sum_d<32>(s);
+            if (lane == 0) R[(size_t)i * 6 + q] = (R[(size_t)i * 6 + q] - s) / H[tri(i, i)];
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // Column c of G: block (s_a, c) = X block a, stored in row s_a at the
+    // position of c in that row's set (the sets are mutual unless one was
+    // truncated; a block without a slot is dropped).  A failed factorisation
+    // (never expected: the normal matrix of a full-rank A[:, S] is SPD) leaves
+    // the block-Jacobi inverse in column c.
+    if (!bad) {
+        for (int a = threadIdx.x; a < m; a += blockDim.x) {
+            const int sa = S[a];
+            const int* Ss = sets + (size_t)sa * kSpaiCap;
+            const int ms = (int)ns[sa];
+            int p = -1;
+            for (int q = 0; q < ms; ++q)
+                if (Ss[q] == c) {
+                    p = q;
+                    break;
+                }
+            if (p < 0) continue;
+            float* out = g_val + (size_t)(rowptr[sa] + p) * 36;
+            for (int k = 0; k < 36; ++k) out[k] = (float)R[(size_t)(6 * a + k / 6) * 6 + k % 6];
+        }
+    } else if (threadIdx.x == 0) {
+        atomicAdd(fail, 1);
+        const float* d = a_block(pn, plist, A, c, c);
+        double M[6][12];
+        for (int r = 0; r < 6; ++r)
+            for (int q = 0; q < 12; ++q) M[r][q] = q < 6 ? (double)d[r * 6 + q] : (q - 6 == r ? 1.0 : 0.0);
+        for (int k = 0; k < 6; ++k) {
+            const double pv = M[k][k] != 0.0 ? 1.0 / M[k][k] : 0.0;
+            for (int q = 0; q < 12; ++q) M[k][q] *= pv;
+            for (int r = 0; r < 6; ++r)
+                if (r != k) {
+                    const double f = M[r][k];
+                    for (int q = 0; q < 12; ++q) M[r][q] -= f * M[k][q];
+                }
+        }
+        for (int r = 0; r < 6; ++r)
+            for (int q = 0; q < 6; ++q) g_val[(size_t)rowptr[c] * 36 + r * 6 + q] = (float)M[r][6 + q];
+    }
+}
+
+// Column indices of G's rows: row s holds its own set.
+__global__ void k_spai_cols(const int* __restrict__ sets, const unsigned* __restrict__ ns,
+                            const int* __restrict__ rowptr, int N, int* g_col) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= N) return;
+    for (unsigned q = 0; q < ns[s]; ++q) g_col[rowptr[s] + q] = sets[(size_t)s * kSpaiCap + q];
+}
+
+int spai_build(fsd_handle* h) {
+    LearnedState* s = learned(h);
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
+    if (!s->sp_sets) {
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_sets, sizeof(int) * (size_t)N * kSpaiCap));
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_size, sizeof(unsigned) * N));
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_rowptr, sizeof(unsigned) * (N + 1)));
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_scan, sizeof(unsigned) * scan_scratch_elems(N)));
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_bucket, sizeof(int) * (size_t)kBuckets * N));
+        FSD_CHECK_CUDA(cudaMalloc(&s->sp_cnt, sizeof(unsigned) * (kBuckets + 2)));
+        FSD_CHECK_CUDA(cudaMallocHost(&s->sp_host, sizeof(unsigned) * 4));
+        FSD_CHECK_CUDA(cudaFuncSetAttribute(k_spai_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)spai_smem(kBucketMax[kBuckets - 1])));
+    }
+    // counters: buckets [0, kBuckets), then truncated sets, then failed rows
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->sp_cnt, 0, sizeof(unsigned) * (kBuckets + 2), st));
+    int* truncated = (int*)(s->sp_cnt + kBuckets);
+    int* fail = (int*)(s->sp_cnt + kBuckets + 1);
+    count_launch();
+    k_spai_sets<<<(N + 127) / 128, 128, 0, st>>>(s->a_pn, s->a_plist, N, s->sp_sets, s->sp_size, s->sp_cnt,
+                                                 s->sp_bucket, truncated);
+    exclusive_scan(s->sp_size, s->sp_rowptr, N, s->sp_scan, st);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->sp_host, s->sp_rowptr + N, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->sp_host + 1, truncated, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    const int nnzb = (int)s->sp_host[0];
+    s->sp_truncated = (int)s->sp_host[1];
+    int e = learned_reserve(h, nnzb);
+    if (e != FSD_OK) return e;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->g_rowptr, s->sp_rowptr, sizeof(int) * (N + 1), cudaMemcpyDeviceToDevice, st));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->g_val, 0, sizeof(float) * 36 * (size_t)nnzb, st));
+    count_launch();
+    k_spai_cols<<<(N + 127) / 128, 128, 0, st>>>(s->sp_sets, s->sp_size, s->g_rowptr, N, s->g_col);
+    for (int b = 0; b < kBuckets; ++b) {
+        count_launch();
+        k_spai_solve<<<N, kSpaiThreads, spai_smem(kBucketMax[b]), st>>>(
+            s->a_pn, s->a_plist, s->a_blocks, s->sp_sets, s->sp_size, s->sp_cnt, s->sp_bucket, b, N, s->g_rowptr,
+            s->g_col, s->g_val, fail);
+    }
+    FSD_CHECK_CUDA(cudaGetLastError());
+    s->g_nnzb = nnzb;
+    return FSD_OK;
+}
+
+}  // namespace fsd

@@ -244,6 +244,26 @@ int fsd_precond_build(fsd_handle* h, const float* d_pos);
  * d_blocks (nnzb x 36, row-major 6x6 fp32).  The structure is checked
  * (rowptr monotone, rowptr[N] = nnzb, 0 <= col < N) and the arrays copied. */
 int fsd_precond_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_blocks);
+/* Learned preconditioner network (FSD_PRECOND_LEARNED; the network has no
+ * counterpart in the reference).  A message-passing network on the graph of
+ * pairs closer than learned_rg predicts G ~ (R_FU^pruned + D)^-1 from
+ * rotation-invariant pair features through an axisymmetric 6x6 block basis,
+ * so G rotates with the configuration.  Weights are one flat fp32 vector of
+ * fsd_learned_num_weights() entries (layout in fsd_b200/csrc/fsd_mpnn.h);
+ * setting weights makes precond_build use the network (blocks set with
+ * fsd_precond_set_blocks take over again when set later).
+ * fsd_learned_train_step: loss E_z ||A G z - z||^2 / 6N over n_probes probe
+ * vectors z (host_probes, n_probes x 6N, or NULL for counter-based normals
+ * drawn from (seed, step)), its gradient (host_grad, optional) and, when
+ * lr > 0, one Adam step.  The neighbour list must be current for d_pos.
+ * fsd_learned_tensor_cores(h, 0) runs the dense layers in FP32 SIMT instead
+ * of BF16 on the tensor cores. */
+int fsd_learned_num_weights(void);
+int fsd_learned_set_weights(fsd_handle* h, const float* host_w, int n);
+int fsd_learned_get_weights(fsd_handle* h, float* host_w, int n);
+int fsd_learned_tensor_cores(fsd_handle* h, int on);
+int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,
+                           unsigned int step, float lr, float* loss, float* host_grad);
 /* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x);
 /* Preconditioned GMRES on the saddle system (Solvers_Saddle, Solvers.cu:55).

@@ -744,6 +744,49 @@ def pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=None, rp=2.1, relaxer=1.0):
     return sp.csr_matrix((vals.ravel(), (rows_.ravel(), cols_.ravel())), shape=(6 * N, 6 * N))
 
 
+def spai_sets(A_bsr, N, cap=32):
+    """Two-hop sets as the CUDA path builds them: the particle, its pruned
+    neighbours in index order, then new members of their lists in order,
+    truncated at cap."""
+    sets = []
+    rows = [A_bsr.indices[A_bsr.indptr[k]:A_bsr.indptr[k + 1]] for k in range(N)]
+    for c in range(N):
+        S = [c] + [int(k) for k in rows[c] if k != c][: cap - 1]
+        for k in S[1:len(S)]:
+            for q in rows[k]:
+                q = int(q)
+                if q not in S and len(S) < cap:
+                    S.append(q)
+        sets.append(S)
+    return sets
+
+
+def spai2(A, N, cap=32):
+    """Right sparse approximate inverse on the two-hop sets: column c of G is
+    X_c with (A^2)[S_c, S_c] X_c = A[S_c, c] (FP64 normal equations), block
+    (s, c) kept where c is in the set of s (as the CUDA path stores it in row
+    s).  Returns a SciPy CSR matrix."""
+    import scipy.sparse as sp
+    Ab = sp.bsr_matrix(A, blocksize=(6, 6))
+    Ab.sort_indices()
+    sets = spai_sets(Ab, N, cap)
+    member = [set(S) for S in sets]
+    Ac = A.tocsc()
+    rows, cols, vals = [], [], []
+    r, q = np.meshgrid(np.arange(6), np.arange(6), indexing="ij")
+    for c, S in enumerate(sets):
+        idx = np.concatenate([np.arange(6 * s, 6 * s + 6) for s in S])
+        As = Ac[:, idx].toarray()
+        X = np.linalg.solve(As.T @ As, As[6 * c:6 * c + 6].T)
+        for a, s in enumerate(S):
+            if c not in member[s]:
+                continue
+            rows.append((6 * s + r).ravel())
+            cols.append((6 * c + q).ravel())
+            vals.append(X[6 * a:6 * a + 6].ravel())
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=A.shape)
+
+
 def ichol0_dense(A, pattern):
     """Scalar IC(0) restricted to `pattern` (boolean), FP64.  Returns L or None on a non-positive pivot."""
     n = len(A)

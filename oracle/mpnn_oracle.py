@@ -1,0 +1,177 @@
+"""FP64 NumPy restatement of the learned preconditioner -- TEST INFRASTRUCTURE ONLY.
+
+Checker for fsd_b200/csrc/mpnn.cu: the pair graph, the invariant edge
+features, the message-passing network, the axisymmetric block head that turns
+its outputs into G ~ (R_FU^pruned + D)^-1, and the approximate-inverse loss
+    L = sum_p ||A G z_p - z_p||^2 / (P 6N).
+The network has no counterpart in the reference; A is the reference's pruned
+preconditioner matrix (Precondition.cu:530-836 plus the identity shift of
+Helper_Precondition.cu:535-580), restated in fsd_oracle.pruned_rfu_sparse.
+Gradients are checked against central differences of `loss` in FP64.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import fsd_oracle as O
+
+WIDTH, LAYERS, FEAT, HEAD_E, HEAD_N = 64, 3, 16, 16, 16
+
+
+def layout():
+    """Offsets of the flat weight vector (fsd_mpnn.h MpLayout)."""
+    o = {}
+    k = 0
+    def take(name, n):
+        nonlocal k
+        o[name] = (k, n)
+        k += n
+    take("W_in", WIDTH * FEAT)
+    take("b_in", WIDTH)
+    for l in range(LAYERS):
+        take(f"W_m{l}", WIDTH * 3 * WIDTH)
+        take(f"b_m{l}", WIDTH)
+        take(f"W_h{l}", WIDTH * 2 * WIDTH)
+        take(f"b_h{l}", WIDTH)
+    take("W_o", HEAD_E * 3 * WIDTH)
+    take("b_o", HEAD_E)
+    take("W_n", HEAD_N * WIDTH)
+    take("b_n", HEAD_N)
+    return o, k
+
+
+def unpack(w):
+    o, n = layout()
+    assert len(w) == n
+    shapes = {"W_in": (WIDTH, FEAT), "W_o": (HEAD_E, 3 * WIDTH), "W_n": (HEAD_N, WIDTH)}
+    for l in range(LAYERS):
+        shapes[f"W_m{l}"] = (WIDTH, 3 * WIDTH)
+        shapes[f"W_h{l}"] = (WIDTH, 2 * WIDTH)
+    out = {}
+    for name, (k, m) in o.items():
+        v = np.asarray(w[k:k + m], np.float64)
+        out[name] = v.reshape(shapes[name]) if name in shapes else v
+    return out
+
+
+def init_weights(seed=0, head_scale=1e-3):
+    """He-initialised hidden layers, near-zero heads (G starts at the block-Jacobi inverse)."""
+    rng = np.random.default_rng(seed)
+    o, n = layout()
+    w = np.zeros(n, np.float32)
+    for name, (k, m) in o.items():
+        if name.startswith("b"):
+            continue
+        fan_in = {"W_in": FEAT, "W_o": 3 * WIDTH, "W_n": WIDTH}.get(name, 3 * WIDTH if name.startswith("W_m") else 2 * WIDTH)
+        scale = head_scale if name in ("W_o", "W_n") else np.sqrt(2.0 / fan_in)
+        w[k:k + m] = rng.standard_normal(m) * scale
+    return w
+
+
+def graph(pos, L, xy, rg):
+    """Directed pairs i -> j closer than rg (single-precision separations, as
+    the kernels), with unit vectors and distances."""
+    p = np.asarray(pos, np.float32)[:, :3]
+    N = len(p)
+    i_all, j_all = np.nonzero(np.ones((N, N), bool) & ~np.eye(N, dtype=bool))
+    R = O.min_image32(p[j_all] - p[i_all], L, xy)
+    d2 = R[:, 0] * R[:, 0] + R[:, 1] * R[:, 1] + R[:, 2] * R[:, 2]
+    keep = d2 < np.float32(rg) * np.float32(rg)
+    i, j, R, d2 = i_all[keep], j_all[keep], R[keep].astype(np.float64), d2[keep]
+    d = np.sqrt(d2.astype(np.float32)).astype(np.float64)
+    return i, j, R / d[:, None], d
+
+
+def features(d, tdist, tvals):
+    h = d - 2.0
+    c = O.res_interp(d, 0, 10, tdist, tvals, mode="lub")
+    x = np.zeros((len(d), FEAT))
+    x[:, 0] = np.log(np.maximum(h, 1e-4)) * 0.2
+    x[:, 1] = h
+    x[:, 2] = np.exp(-10.0 * np.maximum(h, 0.0))
+    x[:, 3] = 2.0 / d
+    x[:, 4:14] = np.sign(c) * np.log1p(np.abs(c)) * 0.25
+    x[:, 14] = 1.0
+    return x
+
+
+def segmean(v, i, N):
+    out = np.zeros((N, v.shape[1]))
+    np.add.at(out, i, v)
+    deg = np.bincount(i, minlength=N).astype(np.float64)
+    return out / np.maximum(deg, 1)[:, None]
+
+
+def forward(wv, x, i, j, N):
+    P = unpack(wv)
+    relu = lambda z: np.maximum(z, 0.0)
+    e = relu(x @ P["W_in"].T + P["b_in"])
+    h = segmean(e, i, N)
+    for l in range(LAYERS):
+        m = relu(np.concatenate([e, h[i], h[j]], 1) @ P[f"W_m{l}"].T + P[f"b_m{l}"])
+        e = e + m
+        a = segmean(m, i, N)
+        h = h + relu(np.concatenate([h, a], 1) @ P[f"W_h{l}"].T + P[f"b_h{l}"])
+    oe = np.concatenate([e, h[i], h[j]], 1) @ P["W_o"].T + P["b_o"]
+    on = h @ P["W_n"].T + P["b_n"]
+    return oe, on
+
+
+def axis_block(o, r):
+    """B(o, r) = [o0 rr + o1 (I - rr), o2 [r]x ; o3 [r]x, o4 rr + o5 (I - rr)] per row."""
+    n = len(r)
+    rr = r[:, :, None] * r[:, None, :]
+    I = np.eye(3)[None]
+    cx = np.zeros((n, 3, 3))
+    cx[:, 0, 1], cx[:, 0, 2] = -r[:, 2], r[:, 1]
+    cx[:, 1, 0], cx[:, 1, 2] = r[:, 2], -r[:, 0]
+    cx[:, 2, 0], cx[:, 2, 1] = -r[:, 1], r[:, 0]
+    w = lambda k: o[:, k][:, None, None]
+    B = np.zeros((n, 6, 6))
+    B[:, :3, :3] = w(0) * rr + w(1) * (I - rr)
+    B[:, :3, 3:] = w(2) * cx
+    B[:, 3:, :3] = w(3) * cx
+    B[:, 3:, 3:] = w(4) * rr + w(5) * (I - rr)
+    return B
+
+
+def g_blocks(oe, on, J, i, rhat, N):
+    """Edge blocks G_ij = J_i B(o_ij) and self blocks G_ii = J_i (I + iso + sum_j B(s_ij))."""
+    Ge = np.einsum("nab,nbc->nac", J[i], axis_block(oe[:, :6], rhat))
+    S = np.zeros((N, 6, 6))
+    np.add.at(S, i, axis_block(oe[:, 6:12], rhat))
+    d = np.concatenate([np.repeat(1.0 + on[:, :1], 3, 1), np.repeat(1.0 + on[:, 1:2], 3, 1)], 1)
+    S[:, np.arange(6), np.arange(6)] += d
+    Gs = np.einsum("nab,nbc->nac", J, S)
+    return Ge, Gs
+
+
+def problem(pos, L, xy, rg=3.0):
+    """Everything the loss needs that does not depend on the weights."""
+    tdist, tvals = O.resistance_table()
+    N = len(pos)
+    A = O.pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=O.neighbor_list(pos, L, xy, rg + 2.5)).tocsr()
+    J = np.stack([np.linalg.inv(A[6 * k:6 * k + 6, 6 * k:6 * k + 6].toarray()) for k in range(N)])
+    i, j, rhat, d = graph(pos, L, xy, rg)
+    x = features(d, tdist, tvals)
+    return dict(N=N, A=A, J=J, i=i, j=j, rhat=rhat, x=x)
+
+
+def g_matrix(wv, pr):
+    import scipy.sparse as sp
+    N, i, j = pr["N"], pr["i"], pr["j"]
+    oe, on = forward(wv, pr["x"], i, j, N)
+    Ge, Gs = g_blocks(oe, on, pr["J"], i, pr["rhat"], N)
+    rows = np.concatenate([i, np.arange(N)])
+    cols = np.concatenate([j, np.arange(N)])
+    blocks = np.concatenate([Ge, Gs])
+    ri = (6 * rows[:, None, None] + np.arange(6)[None, :, None]) * np.ones((1, 1, 6), np.int64)
+    ci = (6 * cols[:, None, None] + np.arange(6)[None, None, :]) * np.ones((1, 6, 1), np.int64)
+    return sp.csr_matrix((blocks.ravel(), (ri.ravel(), ci.ravel())), shape=(6 * N, 6 * N))
+
+
+def loss(wv, pr, Z):
+    """Z: probes (P, 6N)."""
+    G = g_matrix(wv, pr)
+    R = (pr["A"] @ (G @ Z.T)).T - Z
+    return float(np.sum(R * R) / (Z.shape[0] * 6 * pr["N"]))

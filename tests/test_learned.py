@@ -1,0 +1,91 @@
+"""Learned block-sparse preconditioner: network loss and gradient against the
+FP64 oracle, tensor-core layers against the FP32 ones, and what the trained
+network gains in the saddle solve.
+
+Tolerances: the FP32 SIMT path must reproduce the oracle loss to 1e-4 relative
+and its gradient along random directions to 2e-3 relative (central differences
+of the FP64 oracle loss).  The tensor-core path rounds activations and weights
+to BF16, so it is held to 3e-2 on the loss and 6e-2 on directional gradients.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from fsd_b200 import _lib
+from fsd_b200.configs import suspension
+from fsd_b200.core import FSD
+from oracle import mpnn_oracle as M
+
+
+def test_weight_layout_matches_library():
+    assert _lib.lib().fsd_learned_num_weights() == M.layout()[1]
+
+
+def _setup(N=200, phi=0.35, seed=4):
+    pos, Lc = suspension(N, phi, seed)
+    L = (Lc, Lc, Lc)
+    s = FSD(N, (Lc, Lc, Lc, 0.0), precond="learned")
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    s.build_neighbor_list(p)
+    return s, p, M.problem(pos, L, 0.0)
+
+
+def _directional(w, pr, Z, d, eps=1e-4):
+    return (M.loss(w + eps * d, pr, Z) - M.loss(w - eps * d, pr, Z)) / (2 * eps)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tensor_cores,tol_l,tol_g", [(False, 1e-4, 2e-3), (True, 3e-2, 6e-2)])
+def test_loss_and_gradient_match_oracle(cuda, tensor_cores, tol_l, tol_g):
+    s, p, pr = _setup()
+    s.learned_tensor_cores(tensor_cores)
+    w = M.init_weights(0, head_scale=0.01)
+    s.learned_set_weights(w)
+    rng = np.random.default_rng(1)
+    Z = rng.standard_normal((3, 6 * pr["N"]))
+    loss, g = s.learned_train_step(p, probes=Z.astype(np.float32), want_grad=True)
+    wd = w.astype(np.float64)
+    ref = M.loss(wd, pr, Z.astype(np.float32).astype(np.float64))
+    assert abs(loss - ref) <= tol_l * abs(ref)
+    for k in range(3):
+        d = rng.standard_normal(len(w))
+        fd = _directional(wd, pr, Z.astype(np.float32).astype(np.float64), d)
+        assert abs(float(g.astype(np.float64) @ d) - fd) <= tol_g * abs(fd)
+    s.close()
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss_and_is_reproducible(cuda):
+    runs = []
+    for rep in range(2):
+        s, p, pr = _setup(N=400, phi=0.4, seed=6)
+        s.learned_set_weights(M.init_weights(0))
+        losses = [s.learned_train_step(p, n_probes=4, step=t, lr=2e-3) for t in range(40)]
+        runs.append((losses, s.learned_get_weights()))
+        s.close()
+    assert np.mean(runs[0][0][-5:]) < 0.8 * np.mean(runs[0][0][:5])
+    assert runs[0][0] == runs[1][0] and np.array_equal(runs[0][1], runs[1][1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,phi,seed", [(300, 0.4, 3), (500, 0.5, 5)])
+def test_two_hop_spai_matches_oracle(cuda, N, phi, seed):
+    """The base of the learned preconditioner: the right sparse approximate
+    inverse on two-hop sets, FP64 normal equations on the GPU against the FP64
+    oracle.  FP32 storage of the blocks gives ~1e-7; the bar is 1e-5."""
+    from oracle import fsd_oracle as O
+    pos, Lc = suspension(N, phi, seed)
+    s = FSD(N, (Lc, Lc, Lc, 0.0), precond="learned", learned_inner=0)
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    s.build_neighbor_list(p)
+    s.precond_build(p)
+    td, tv = O.resistance_table()
+    A = O.pruned_rfu_sparse(pos, (Lc, Lc, Lc), 0.0, td, tv).tocsr()
+    G = O.spai2(A, N)
+    b = np.random.default_rng(seed).standard_normal(17 * N)
+    got = s.precond_apply(torch.as_tensor(b, dtype=torch.float32).cuda()).cpu().numpy()
+    ref = O.saddle_precond(b, G, N)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+    s.close()
