@@ -1,14 +1,21 @@
 """Benchmark: full FSD time steps per second at N=32768, phi=0.4.
 
-Workload (one "step"): neighbour list, IC(0) preconditioner build, pair
-forces, far-field Brownian slip (wave-space noise + Lanczos on the real-space
+Workload (one "step"): neighbour list, preconditioner build, pair forces,
+far-field Brownian slip (wave-space noise + Lanczos on the real-space
 mobility), near-field Brownian force (Lanczos on R_FU), random finite
 difference drift (two saddle solves), main saddle solve to relative residual
-1e-4 (GMRES, warm-started), Euler update with simple shear 1.0.  kT = 1,
-dt = 1e-4, Ewald accuracy 1e-3 (xi 0.5, 72^3 grid, P = 6).  Positions from
-seeded random sequential addition followed by overlap relaxation.
+1e-4 (warm-started), Euler update with simple shear 1.0.  kT = 1, dt = 1e-4,
+Ewald accuracy 1e-3 (xi 0.5, 72^3 grid, P = 6).  Positions from seeded random
+sequential addition followed by overlap relaxation.
+
+The timed preconditioner is the learned one by default (two-hop sparse
+approximate inverse of the lubrication block, inner GMRES steps, flexible outer
+GMRES, and the trained network's correction when fsd_b200/data holds
+weights); the same steps with the plain IChol preconditioner are timed after
+it for the metric's comparison ("ichol" in the JSON line).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fsd|reference]
+                  [--precond learned|ichol|none] [--inner k] [--no-ichol] [--no-net]
 
 Under torchrun each rank steps its own independent suspension (the path does
 not shard within one suspension; replicas only).  Prints one JSON line.
@@ -44,7 +51,11 @@ def parse():
     ap.add_argument("--impl", default="fsd", choices=["fsd", "reference"])
     ap.add_argument("--N", type=int, default=32768)
     ap.add_argument("--phi", type=float, default=0.4)
-    ap.add_argument("--precond", default="ichol", choices=["ichol", "none", "learned"])
+    ap.add_argument("--precond", default="learned", choices=["ichol", "none", "learned"])
+    ap.add_argument("--inner", type=int, default=6, help="inner GMRES steps of the learned preconditioner")
+    ap.add_argument("--no-ichol", action="store_true", help="skip the IChol comparison run")
+    ap.add_argument("--no-net", action="store_true", help="learned preconditioner without the network correction")
+    ap.add_argument("--ichol-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -110,12 +121,9 @@ def peak_hbm():
         return FALLBACK_HBM, "fallback"
 
 
-def region_bytes(name, N, G, nnzb, pairs_real, pairs_lub, launches_per_call):
-    """Algorithmic DRAM bytes of one launch of the region's kernel."""
-    if name == "precond_apply":
-        # forward or backward block solve: factor blocks (6x6 fp32) + column ids once,
-        # the 6N right-hand side and result
-        return nnzb * (36 * 4 + 4) / 1 + 6 * N * 4 * 3
+def region_bytes(name, N, G, pairs_real, pairs_lub):
+    """Algorithmic DRAM bytes of one launch of a single-kernel region (DESIGN.md
+    lists the per-unit figures): each array the kernel must read or write once."""
     if name == "fft":
         return 2 * 6 * G * 8  # one axis pass over the 6 packed complex grids, read + write
     if name == "spread":
@@ -131,12 +139,97 @@ def region_bytes(name, N, G, nnzb, pairs_real, pairs_lub, launches_per_call):
     return None
 
 
-def run_fsd(args, ws, rank, local):
+SINGLE_KERNEL_REGIONS = {"fft": 3, "spread": 1, "contract": 1, "green": 1, "real_space": 1, "rfu": 1}
+WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_precond.f32"
+
+
+def make_solver(args, precond, N, L, dev, seed):
+    from fsd_b200.core import FSD
+
+    s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=seed, error=1e-3, solver_tol=1e-4,
+            lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=precond, period=0, gmres_max_iter=3000,
+            gmres_restart=200 if precond == "ichol" else 100, learned_inner=args.inner if precond == "learned" else 0)
+    net = False
+    if precond == "learned" and WEIGHTS.exists() and not args.no_net:
+        s.learned_set_weights(np.fromfile(WEIGHTS, "<f4"))
+        net = True
+    return s, net
+
+
+def timed_steps(args, s, state, steps, warmup, dev, ws, clocks=False, profile=False):
+    """Warm-up, then `steps` steps each bracketed by CUDA events on the launching
+    stream with a 256 MiB L2 flush before it (outside the events)."""
     import torch
 
     from fsd_b200 import _lib
+
+    p, ori, img, F, V, step_no = state
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def one_step():
+        st = s.step(step_no[0], 1.0, p, ori, img, F, V, raise_on_error=False)
+        step_no[0] += 1
+        if st not in (0, 4):  # Lanczos not converged (4) is reported, not fatal, as in the reference
+            raise RuntimeError(f"fsd_step status {st}")
+
+    for _ in range(warmup):
+        one_step()
+    lib = _lib.lib()
+    nreg = len(_lib.REGIONS)
+    ms_regions = np.zeros(nreg)
+    cnt_regions = np.zeros(nreg, np.int64)
+    if profile:
+        lib.fsd_profile_enable(s._h, 1)
+        lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
+                             nreg, 1)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    iters = []
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    launch0 = lib.fsd_launch_count()
+    clk = ClockSampler(dev.index) if clocks else None
+    if clk:
+        clk.__enter__()
+    for k in range(steps):
+        flush.fill_(float(k))
+        evs[k][0].record(stream)
+        one_step()
+        evs[k][1].record(stream)
+        si = s.solve_info()
+        iters.append(si["gmres_iters"] + [si["lanczos_ff_iters"], si["lanczos_nf_iters"]])
+    torch.cuda.synchronize(dev)
+    if clk:
+        clk.__exit__()
+    launches = lib.fsd_launch_count() - launch0
+    if ws > 1:
+        torch.distributed.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(sum(step_ms))
+    if ws > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    regions = None
+    if profile:
+        lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
+                             nreg, 1)
+        lib.fsd_profile_enable(s._h, 0)
+        regions = {n: {"ms": float(ms_regions[i]), "calls": int(cnt_regions[i])} for i, n in enumerate(_lib.REGIONS)}
+    it = np.array(iters, np.float64)
+    iters_out = {"gmres_rfd_plus": float(it[:, 0].mean()), "gmres_rfd_minus": float(it[:, 1].mean()),
+                 "gmres_main": float(it[:, 2].mean()), "lanczos_ff": float(it[:, 3].mean()),
+                 "lanczos_nf": float(it[:, 4].mean())}
+    return {"total_ms": total_ms, "step_ms": step_ms, "iters": iters_out, "launches": int(launches),
+            "regions": regions, "clocks": clk.summary() if clk else None}
+
+
+def run_fsd(args, ws, rank, local):
+    import torch
+
     from fsd_b200.configs import suspension
-    from fsd_b200.core import FSD
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -146,66 +239,25 @@ def run_fsd(args, ws, rank, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
     N, phi = args.N, args.phi
     pos, L = suspension(N, phi, seed=1 + rank)
-    s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=1 + rank, error=1e-3, solver_tol=1e-4,
-            lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=args.precond, period=0, gmres_max_iter=3000, gmres_restart=200)
+
+    def fresh_state():
+        p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
+        ori = torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev).contiguous()
+        img = torch.zeros(3 * N, dtype=torch.int32, device=dev)
+        F = torch.zeros(6 * N, device=dev)
+        V = torch.zeros(11 * N, device=dev)
+        return [p, ori, img, F, V, [0]]
+
+    s, net = make_solver(args, args.precond, N, L, dev, 1 + rank)
     info = s.pse_info()
-    shear_rate = 1.0
-    p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
-    ori = torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev).contiguous()
-    img = torch.zeros(3 * N, dtype=torch.int32, device=dev)
-    F = torch.zeros(6 * N, device=dev)
-    V = torch.zeros(11 * N, device=dev)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
-    stream = torch.cuda.current_stream(dev)
-    step_no = [0]
-
-    def one_step():
-        st = s.step(step_no[0], shear_rate, p, ori, img, F, V, raise_on_error=False)
-        step_no[0] += 1
-        if st not in (0, 4):  # Lanczos not converged (4) is reported, not fatal, as in the reference
-            raise RuntimeError(f"fsd_step status {st}")
-
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize(dev)
-    lib = _lib.lib()
-    # --- device-timed region: K steps, L2 flushed before each step (outside its events)
-    iters = []
-    launch0 = lib.fsd_launch_count()
-    check_prof = lib.fsd_profile_enable(s._h, 1)
-    ms_regions = np.zeros(len(_lib.REGIONS))
-    cnt_regions = np.zeros(len(_lib.REGIONS), np.int64)
-    lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
-                         len(_lib.REGIONS), 1)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            evs[k][0].record(stream)
-            one_step()
-            evs[k][1].record(stream)
-            si = s.solve_info()
-            iters.append(si["gmres_iters"] + [si["lanczos_ff_iters"], si["lanczos_nf_iters"]])
-        torch.cuda.synchronize(dev)
-    if ws > 1:
-        torch.distributed.barrier()
-    launches = lib.fsd_launch_count() - launch0
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = float(sum(step_ms))
-    lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
-                         len(_lib.REGIONS), 1)
-    lib.fsd_profile_enable(s._h, 0)
-    if ws > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = ws * args.steps / (total_ms / 1e3)
+    state = fresh_state()
+    main = timed_steps(args, s, state, args.steps, args.warmup, dev, ws, clocks=True, profile=True)
+    value = ws * args.steps / (main["total_ms"] / 1e3)
     # --- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
+        p, ori, img, F, V, step_no = state
+        stream = torch.cuda.current_stream(dev)
         pin = lambda t: t.detach().cpu().pin_memory()
         h_pos, h_ori, h_img = pin(p), pin(ori), pin(img)
         h_V, h_P = torch.empty(11 * N).pin_memory(), torch.empty(4 * N).pin_memory()
@@ -216,7 +268,10 @@ def run_fsd(args, ws, rank, local):
             p.copy_(h_pos, non_blocking=True)
             ori.copy_(h_ori, non_blocking=True)
             img.copy_(h_img, non_blocking=True)
-            one_step()
+            st = s.step(step_no[0], 1.0, p, ori, img, F, V, raise_on_error=False)
+            step_no[0] += 1
+            if st not in (0, 4):
+                raise RuntimeError(f"fsd_step status {st}")
             h_V.copy_(V, non_blocking=True)
             h_P.copy_(p, non_blocking=True)
         e1.record(stream)
@@ -229,49 +284,52 @@ def run_fsd(args, ws, rank, local):
         e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": "steps/s",
                "h2d_bytes_per_step": int(h_pos.numel() * 4 + h_ori.numel() * 4 + h_img.numel() * 4),
                "d2h_bytes_per_step": int(h_V.numel() * 4 + h_P.numel() * 4)}
-    # --- roofline of the dominant kernel (largest device time among the timed kernels)
-    regions = {n: {"ms": float(ms_regions[i]), "calls": int(cnt_regions[i])} for i, n in enumerate(_lib.REGIONS)}
+    s.close()
+    # --- the same step with the plain IChol preconditioner (the metric's comparison)
+    ichol = None
+    if not args.no_ichol and args.precond != "ichol":
+        si, _ = make_solver(args, "ichol", N, L, dev, 1 + rank)
+        r = timed_steps(args, si, fresh_state(), args.ichol_steps, 1, dev, ws)
+        si.close()
+        ichol = {"value": ws * args.ichol_steps / (r["total_ms"] / 1e3), "unit": "steps/s",
+                 "ms_per_step": r["total_ms"] / args.ichol_steps, "steps": args.ichol_steps, "warmup": 1,
+                 "iterations_per_step": r["iters"]}
+    # --- roofline of the dominant single-kernel region
+    regions = main["regions"]
     G = info.Nx * info.Ny * info.Nz
-    nlist_rows = None
-    candidates = {n: r for n, r in regions.items() if n in ("precond_apply", "fft", "spread", "contract", "green",
-                                                             "real_space", "rfu") and r["calls"] > 0}
-    dom = max(candidates, key=lambda n: candidates[n]["ms"])
-    launches_per_call = {"precond_apply": 2, "fft": 3}.get(dom, 1)
-    avg_launch_ms = candidates[dom]["ms"] / candidates[dom]["calls"] / launches_per_call
-    nnzb = int(N * 4.1)  # pruned blocks incl. diagonal (mean pruned degree ~3.1 at phi=0.4)
-    pairs_real = int(N * 60)
-    pairs_lub = int(N * 75)
-    nb = region_bytes(dom, N, G, nnzb, pairs_real, pairs_lub, launches_per_call)
+    cands = {n: r for n, r in regions.items() if n in SINGLE_KERNEL_REGIONS and r["calls"] > 0}
+    dom = max(cands, key=lambda n: cands[n]["ms"])
+    avg_launch_ms = cands[dom]["ms"] / cands[dom]["calls"] / SINGLE_KERNEL_REGIONS[dom]
+    nb = region_bytes(dom, N, G, pairs_real=int(N * 60), pairs_lub=int(N * 75))
     peak, peak_kind = peak_hbm()
-    achieved = nb / (avg_launch_ms * 1e-3) / 1e9 if nb else None
+    achieved = nb / (avg_launch_ms * 1e-3) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "dram_traffic.json"
     if tf.exists():
         traffic = json.loads(tf.read_text()).get(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "avg_launch_us": avg_launch_ms * 1e3, "algorithmic_bytes_per_launch": nb}
-    it = np.array(iters)
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "avg_launch_us": avg_launch_ms * 1e3,
+                "algorithmic_bytes_per_launch": nb}
     out = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (FP64 Krylov/Lanczos scalars and IC pivots)",
+        "warmup": args.warmup, "ms_per_step": main["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 Krylov/Lanczos scalars, IC pivots, SPAI solves)",
         "data": "synthetic: seeded random sequential addition + overlap relaxation, min gap 1e-3",
         "config": {"workload": f"full FSD step, N={N}, phi={phi}, shear 1.0, kT 1, dt 1e-4, Ewald 1e-3, "
-                               f"GMRES(200) 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
+                               f"GMRES 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
                    "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
+                   "learned_inner": args.inner if args.precond == "learned" else None, "learned_network": net,
                    "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
                    "parallelism": f"replicas x{ws}"},
-        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
-        "iterations_per_step": {"gmres_rfd_plus": float(it[:, 0].mean()), "gmres_rfd_minus": float(it[:, 1].mean()),
-                                "gmres_main": float(it[:, 2].mean()), "lanczos_ff": float(it[:, 3].mean()),
-                                "lanczos_nf": float(it[:, 4].mean())},
+        "e2e": e2e, "gpu_launches": main["launches"], "roofline": roofline,
+        "iterations_per_step": main["iters"],
         "regions_ms_per_step": {n: r["ms"] / args.steps for n, r in regions.items()},
-        "clocks": clk.summary(),
+        "ichol": ichol,
+        "speedup_vs_ichol": (value / ichol["value"]) if ichol else None,
+        "clocks": main["clocks"],
     }
     if rank == 0:
         out["cpu_baseline"] = cpu_baseline(args, pos, L, out)
-    s.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
     return out if rank == 0 else None
@@ -297,7 +355,7 @@ def cpu_baseline(args, pos, L, gpu_out=None):
             break
     t_op = (time.time() - t) / n
     if gpu_out is not None:
-        it = gpu_out["iterations_per_step"]
+        it = (gpu_out.get("ichol") or gpu_out)["iterations_per_step"]
         ops = it["gmres_rfd_plus"] + it["gmres_rfd_minus"] + it["gmres_main"] + 9
     else:
         ops = 600.0

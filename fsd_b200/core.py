@@ -212,6 +212,20 @@ class FSD:
               "fsd_learned_get_weights")
         return w
 
+    def learned_get_state(self):
+        n = 3 * lib().fsd_learned_num_weights()
+        buf = np.zeros(n, np.float32)
+        t = C.c_int(0)
+        check(lib().fsd_learned_get_state(self._h, buf.ctypes.data_as(C.c_void_p), n, C.byref(t)),
+              "fsd_learned_get_state")
+        return buf, t.value
+
+    def learned_set_state(self, state):
+        buf, t = state
+        buf = np.ascontiguousarray(buf, np.float32)
+        check(lib().fsd_learned_set_state(self._h, buf.ctypes.data_as(C.c_void_p), int(buf.size), int(t)),
+              "fsd_learned_set_state")
+
     def learned_tensor_cores(self, on: bool):
         check(lib().fsd_learned_tensor_cores(self._h, int(bool(on))), "fsd_learned_tensor_cores")
 

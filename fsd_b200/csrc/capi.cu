@@ -173,7 +173,6 @@ void fsd_default_params(fsd_params* p) {
     p->ichol_local_shift = 1;
     p->ichol_gain_limit = 100.0f;
     p->learned_inner = 4;
-    p->learned_rg = 3.0f;
 }
 
 const char* fsd_status_string(int status) {
@@ -238,7 +237,7 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
     if (p->N < 1 || !(p->Lx > 0 && p->Ly > 0 && p->Lz > 0) || !(p->xi > 0) || !(p->error > 0 && p->error < 1))
         return FSD_ERR_BAD_PARAMS;
     if (p->gmres_restart < 1 || p->gmres_restart > kMaxRestart || p->lanczos_max < 4) return FSD_ERR_BAD_PARAMS;
-    if (p->learned_inner < 0 || p->learned_inner > kMaxInner || !(p->learned_rg > 2.0f)) return FSD_ERR_BAD_PARAMS;
+    if (p->learned_inner < 0 || p->learned_inner > kMaxInner) return FSD_ERR_BAD_PARAMS;
     fsd_handle* h = new fsd_handle();
     h->p = *p;
     h->stream = (cudaStream_t)stream;
@@ -441,6 +440,18 @@ int fsd_learned_set_weights(fsd_handle* h, const float* host_w, int n) {
 int fsd_learned_get_weights(fsd_handle* h, float* host_w, int n) {
     if (!h || !host_w) return FSD_ERR_BAD_PARAMS;
     return mpnn_get_weights(h, host_w, n);
+}
+
+int fsd_learned_get_state(fsd_handle* h, float* host, int n, int* adam_step) {
+    if (!h || !host || !adam_step) return FSD_ERR_BAD_PARAMS;
+    return mpnn_get_state(h, host, n, adam_step);
+}
+
+int fsd_learned_set_state(fsd_handle* h, const float* host, int n, int adam_step) {
+    if (!h || !host) return FSD_ERR_BAD_PARAMS;
+    const int e = mpnn_set_state(h, host, n, adam_step);
+    if (e == FSD_OK) learned(h)->g_user = false;
+    return e;
 }
 
 int fsd_learned_tensor_cores(fsd_handle* h, int on) {

@@ -52,6 +52,8 @@ void mpnn_free(fsd_handle* h);
 int mpnn_set_weights(fsd_handle* h, const float* host_w, int n);
 int mpnn_get_weights(fsd_handle* h, float* host_w, int n);
 bool mpnn_loaded(fsd_handle* h);
+int mpnn_get_state(fsd_handle* h, float* host, int n, int* t);
+int mpnn_set_state(fsd_handle* h, const float* host, int n, int t);
 void mpnn_use_umma(fsd_handle* h, bool on);
 int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist, const float* a_blocks);
 int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, int P, uint32_t step, float lr,

@@ -1,17 +1,19 @@
-// Message-passing network that predicts the block-sparse approximate inverse
-// G ~ (R_FU^pruned + D)^-1 used by FSD_PRECOND_LEARNED (mpnn.cu).
+// Message-passing network that predicts a correction to the two-hop sparse
+// approximate inverse G ~ (R_FU^pruned + D)^-1 used by FSD_PRECOND_LEARNED
+// (mpnn.cu).
 //
-// Graph: particles, and a directed edge i -> j for every pair closer than
-// learned_rg (both directions).  Inputs are rotation invariants of each pair
-// (gap, inverse distance and the tabulated resistance scalars); outputs are
-// scalar coefficients of an axisymmetric tensor basis built from the pair's
-// unit vector, so G rotates with the configuration by construction:
-//   G_ij = J_i B(o_ij, r_ij)                  (j != i)
-//   G_ii = J_i (I + diag(c_t I3, c_r I3) + sum_j B(s_ij, r_ij))
-// with J_i = (A_ii)^-1 the inverse diagonal block of A = R_FU^pruned + D and
+// Graph: particles, and a directed edge c -> s for every member s != c of
+// c's two-hop set (the pattern of G).  Inputs are rotation invariants of each
+// pair (gap, inverse distance, the tabulated resistance scalars and whether
+// the pair is in direct contact range); outputs are scalar coefficients of an
+// axisymmetric tensor basis built from the pair's unit vector, so the
+// correction rotates with the configuration by construction:
+//   dG_cs = J_c B(o_cs, r_cs)                       (s != c)
+//   dG_cc = J_c (diag(c_t I3, c_r I3) + sum_s B(q_cs, r_cs))
+// with J_c = (A_cc)^-1 the inverse diagonal block of A = R_FU^pruned + D and
 //   B(o, r) = [ o0 rr + o1 (I - rr)   o2 [r]x          ]
 //             [ o3 [r]x               o4 rr + o5 (I - rr) ]
-// ([r]x the cross-product matrix).  o = out[0:6], s = out[6:12] of the edge
+// ([r]x the cross-product matrix).  o = out[0:6], q = out[6:12] of the edge
 // head; (c_t, c_r) from the node head.
 //
 // Network (width 64, three message-passing layers, ReLU):

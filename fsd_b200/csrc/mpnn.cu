@@ -32,40 +32,48 @@ inline int nblk(size_t n, int t = kThreads) { return (int)std::min<size_t>((n + 
 }  // namespace
 
 // ------------------------------------------------------------------ graph
-__global__ void k_g_count(const float4* __restrict__ pos, int N, Box b, const unsigned* __restrict__ nneigh,
-                          const unsigned* __restrict__ nlist, int stride, float rg2, unsigned* cnt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const float4 pi = pos[i];
-    unsigned c = 0;
-    for (unsigned q = 0; q < nneigh[i]; ++q) {
-        const float4 pj = pos[nlist[(size_t)i * stride + q]];
-        const float3 r = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
-        if (dist2_rn(r) < rg2) ++c;
-    }
-    cnt[i] = c;
+// Edges c -> s for the members s != c of c's two-hop set, in set order, so
+// edge e of row c sits at G position sp_rowptr[c] + 1 + (e - rowptr[c]).
+// rhat = (unit vector c -> s, distance); features are rotation invariants.
+__device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x) * 0.25f; }
+
+__global__ void k_g_rows(const unsigned* __restrict__ sp_rowptr, int N, unsigned* rowptr) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c <= N) rowptr[c] = sp_rowptr[c] - (unsigned)c;
 }
 
-// Edges of row i in neighbour-list order; rhat = (unit vector i -> j, distance).
-__global__ void k_g_fill(const float4* __restrict__ pos, int N, Box b, const unsigned* __restrict__ nneigh,
-                         const unsigned* __restrict__ nlist, int stride, float rg2,
-                         const unsigned* __restrict__ rowptr, int* src, int* dst, float4* rhat) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const float4 pi = pos[i];
-    unsigned e = rowptr[i];
-    for (unsigned q = 0; q < nneigh[i]; ++q) {
-        const unsigned j = nlist[(size_t)i * stride + q];
+__global__ void k_g_from_sets(const float4* __restrict__ pos, int N, Box b, const int* __restrict__ sets,
+                              const unsigned* __restrict__ ns, const unsigned* __restrict__ rowptr,
+                              const unsigned* __restrict__ pn, const unsigned* __restrict__ plist, ResTable tab,
+                              int* src, int* dst, float4* rhat, float* x) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    const float4 pc = pos[c];
+    const int* S = sets + (size_t)c * kSpaiCap;
+    for (unsigned a = 1; a < ns[c]; ++a) {
+        const size_t e = rowptr[c] + a - 1;
+        const int j = S[a];
         const float4 pj = pos[j];
-        const float3 r = min_image_rn(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
-        const float d2 = dist2_rn(r);
-        if (d2 < rg2) {
-            const float d = sqrtf(d2);
-            src[e] = i;
-            dst[e] = (int)j;
-            rhat[e] = make_float4(r.x / d, r.y / d, r.z / d, d);
-            ++e;
-        }
+        const float3 r = min_image_rn(make_float3(pj.x - pc.x, pj.y - pc.y, pj.z - pc.z), b);
+        const float d = sqrtf(dist2_rn(r));
+        src[e] = c;
+        dst[e] = j;
+        rhat[e] = make_float4(r.x / d, r.y / d, r.z / d, d);
+        bool direct = false;
+        for (unsigned q = 0; q < pn[c]; ++q)
+            if ((int)plist[(size_t)c * kPrunedCap + q] == j) direct = true;
+        const float h = d - 2.0f;
+        float cf[10];
+        res_interp<10>(tab, d, 0, cf);
+        float* o = x + e * kMpFeat;
+        o[0] = logf(fmaxf(h, 1e-4f)) * 0.2f;
+        o[1] = h;
+        o[2] = expf(-10.0f * fmaxf(h, 0.0f));
+        o[3] = 2.0f / d;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) o[4 + k] = slog(cf[k]);
+        o[14] = direct ? 1.0f : 0.0f;
+        o[15] = 1.0f;
     }
 }
 
@@ -82,27 +90,6 @@ __global__ void k_g_rev(const unsigned* __restrict__ rowptr, const int* __restri
             break;
         }
     rev[e] = r;
-}
-
-__device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x) * 0.25f; }
-
-// Rotation-invariant edge features.
-__global__ void k_g_feat(const float4* __restrict__ rhat, int E, ResTable tab, float* x) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= E) return;
-    const float r = rhat[e].w;
-    const float h = r - 2.0f;
-    float c[10];
-    res_interp<10>(tab, r, 0, c);
-    float* o = x + (size_t)e * kMpFeat;
-    o[0] = logf(fmaxf(h, 1e-4f)) * 0.2f;
-    o[1] = h;
-    o[2] = expf(-10.0f * fmaxf(h, 0.0f));
-    o[3] = 2.0f / r;
-#pragma unroll
-    for (int k = 0; k < 10; ++k) o[4 + k] = slog(c[k]);
-    o[14] = 1.0f;
-    o[15] = 0.0f;
 }
 
 // J_i = (A_ii)^-1 for the self block of the pruned matrix (FP64 Gauss-Jordan
@@ -403,25 +390,21 @@ __device__ __forceinline__ void axis_block_grad(const float* dB, float3 r, float
     for (int k = 0; k < 6; ++k) go[k] = g[k];
 }
 
-// G in block CSR: row i = [self, edges of i].  One thread per row.
+// Correction added to G (block CSR of the two-hop sets; row i = [self,
+// edges of i]).  One thread per row.
 __global__ void k_head_blocks(const unsigned* __restrict__ rowptr, const float4* __restrict__ rhat,
                               const float* __restrict__ oe, const float* __restrict__ on, const float* __restrict__ J,
-                              int N, int* g_rowptr, int* g_col, const int* __restrict__ dst, float* G) {
+                              int N, float* G) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > N) return;
-    if (i == N) {
-        g_rowptr[N] = (int)rowptr[N] + N;
-        return;
-    }
+    if (i >= N) return;
     const unsigned b = rowptr[i], e = rowptr[i + 1];
-    const int base = (int)b + i;
-    g_rowptr[i] = base;
+    const size_t base = (size_t)b + i;
     float Ji[36];
     for (int k = 0; k < 36; ++k) Ji[k] = J[(size_t)i * 36 + k];
     float S[36];
     for (int k = 0; k < 36; ++k) S[k] = 0.f;
     const float ct = on[(size_t)i * kMpHeadN + 0], cr = on[(size_t)i * kMpHeadN + 1];
-    for (int d = 0; d < 6; ++d) S[d * 7] = 1.0f + (d < 3 ? ct : cr);
+    for (int d = 0; d < 6; ++d) S[d * 7] = (d < 3 ? ct : cr);
     float B[36];
     for (unsigned f = b; f < e; ++f) {
         const float4 rh = rhat[f];
@@ -429,23 +412,21 @@ __global__ void k_head_blocks(const unsigned* __restrict__ rowptr, const float4*
         axis_block(oe + (size_t)f * kMpHeadE + 6, r, B);
         for (int k = 0; k < 36; ++k) S[k] += B[k];
         axis_block(oe + (size_t)f * kMpHeadE, r, B);
-        float* out = G + (size_t)(base + 1 + (f - b)) * 36;
+        float* out = G + (base + 1 + (f - b)) * 36;
         for (int a = 0; a < 6; ++a)
             for (int c = 0; c < 6; ++c) {
                 float s = 0.f;
                 for (int q = 0; q < 6; ++q) s += Ji[a * 6 + q] * B[q * 6 + c];
-                out[a * 6 + c] = s;
+                out[a * 6 + c] += s;
             }
-        g_col[base + 1 + (f - b)] = dst[f];
     }
-    float* out = G + (size_t)base * 36;
+    float* out = G + base * 36;
     for (int a = 0; a < 6; ++a)
         for (int c = 0; c < 6; ++c) {
             float s = 0.f;
             for (int q = 0; q < 6; ++q) s += Ji[a * 6 + q] * S[q * 6 + c];
-            out[a * 6 + c] = s;
+            out[a * 6 + c] += s;
         }
-    g_col[base] = i;
 }
 
 // From dG (block CSR like G) to head gradients: dB = J_i^T dG.
@@ -830,31 +811,27 @@ static GemmIn one(const float* a, int width) {
     return g;
 }
 
-// Graph, features and J for these positions (neighbour list and the pruned
-// matrix must be current).
+// Graph (the two-hop sets of the approximate inverse), features and J for
+// these positions; spai_build must have run for them.
 static int mp_graph(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist,
                     const float* a_blocks) {
     MP_TRY(mp_alloc_static(h));
     MpState* s = mp(h);
+    LearnedState* ls = learned(h);
     const int N = h->p.N;
     cudaStream_t st = h->stream;
-    const float rg2 = h->p.learned_rg * h->p.learned_rg;
+    const int E = ls->g_nnzb - N;
+    MP_TRY(mp_alloc_edges(h, E));
+    s->E = E;
     count_launch();
-    k_g_count<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride, rg2, s->cnt);
-    exclusive_scan(s->cnt, s->cnt, N, s->scan, st);
-    unsigned E = 0;
-    FSD_CHECK_CUDA(cudaMemcpyAsync(&E, s->cnt + N, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-    MP_TRY(mp_alloc_edges(h, (int)E));
-    s->E = (int)E;
+    k_g_rows<<<(N + 1 + 127) / 128, 128, 0, st>>>(ls->sp_rowptr, N, s->cnt);
     count_launch();
-    k_g_fill<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, h->w.nneigh, h->w.nlist, h->w.nl_stride, rg2, s->cnt,
-                                              s->src, s->dst, s->rhat);
+    k_g_from_sets<<<(N + 127) / 128, 128, 0, st>>>(pos, N, h->box, ls->sp_sets, ls->sp_size, s->cnt, a_pn, a_plist,
+                                                   ResTable{h->d_res_dist, h->d_res_vals}, s->src, s->dst, s->rhat,
+                                                   s->x);
     if (E) {
         count_launch();
-        k_g_rev<<<(E + 255) / 256, 256, 0, st>>>(s->cnt, s->src, s->dst, (int)E, s->rev);
-        count_launch();
-        k_g_feat<<<(E + 255) / 256, 256, 0, st>>>(s->rhat, (int)E, ResTable{h->d_res_dist, h->d_res_vals}, s->x);
+        k_g_rev<<<(E + 255) / 256, 256, 0, st>>>(s->cnt, s->src, s->dst, E, s->rev);
     }
     count_launch();
     k_g_jinv<<<(N + 127) / 128, 128, 0, st>>>(a_pn, a_plist, a_blocks, N, s->J);
@@ -894,16 +871,13 @@ static int mp_forward(fsd_handle* h) {
     return FSD_OK;
 }
 
-// G blocks into the learned state's block CSR.
+// Add the network's correction to the approximate inverse in place.
 static int mp_head(fsd_handle* h) {
     MpState* s = mp(h);
     LearnedState* ls = learned(h);
     const int N = s->N;
-    MP_TRY(learned_reserve(h, s->E + N));
     count_launch();
-    k_head_blocks<<<(N + 1 + 127) / 128, 128, 0, h->stream>>>(s->cnt, s->rhat, s->oe, s->on, s->J, N, ls->g_rowptr,
-                                                              ls->g_col, s->dst, ls->g_val);
-    ls->g_nnzb = s->E + N;
+    k_head_blocks<<<(N + 127) / 128, 128, 0, h->stream>>>(s->cnt, s->rhat, s->oe, s->on, s->J, N, ls->g_val);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
 }
@@ -970,8 +944,9 @@ static int mp_backward(fsd_handle* h) {
     return FSD_OK;
 }
 
-// Loss L = sum_p ||A G z_p - z_p||^2 / (P 6N) for the probes in s->Zp, and
-// (when grad) the gradient dL/dG into s->dG, then through the head.
+// Loss L = sum_p ||A G z_p - z_p||^2 / (P 6N) for the probes z in s->Zp and,
+// when grad, the gradient dL/dG_ij = sum_p (A dR_p)[i] z_p[j]^T (A symmetric),
+// then through the head.
 static int mp_loss(fsd_handle* h, int P, bool grad) {
     MpState* s = mp(h);
     LearnedState* ls = learned(h);
@@ -989,7 +964,6 @@ static int mp_loss(fsd_handle* h, int P, bool grad) {
     count_launch();
     k_sum_part<<<1, 32, 0, st>>>(s->part, 296, inv, s->loss);
     if (!grad) return FSD_OK;
-    // dU = A^T dR = A dR (A symmetric); dG_ie = sum_p dU_p[i] z_p[col]^T
     count_launch();
     k_pruned_multi<<<rows, 256, 0, st>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Vp, s->Up, N, P);
     count_launch();
@@ -998,6 +972,14 @@ static int mp_loss(fsd_handle* h, int P, bool grad) {
     k_head_bwd<<<(N + 127) / 128, 128, 0, st>>>(s->cnt, s->rhat, s->J, s->dG, N, s->doe, s->don);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
+}
+
+// z = w - A G0 w: the residual one application of the approximate inverse
+// leaves, probes for the correction's loss (the approximate inverse itself
+// is optimal for white-noise probes on its pattern).
+__global__ void k_sub(const float* __restrict__ a, float* __restrict__ b, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        b[k] = a[k] - b[k];
 }
 
 static int mp_probes(fsd_handle* h, int P) {
@@ -1034,6 +1016,32 @@ int mpnn_get_weights(fsd_handle* h, float* host_w, int n) {
     return FSD_OK;
 }
 
+// Weights with the Adam moments and step count, so that training can move
+// between handles (one per box size) without restarting the optimiser.
+int mpnn_get_state(fsd_handle* h, float* host, int n, int* t) {
+    MpState* s = mp(h);
+    if (n != 3 * MpLayout::total || !s->loaded) return FSD_ERR_BAD_PARAMS;
+    const size_t m = MpLayout::total;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host, s->w, sizeof(float) * m, cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host + m, s->mw, sizeof(float) * m, cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(host + 2 * m, s->vw, sizeof(float) * m, cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    *t = s->adam_t;
+    return FSD_OK;
+}
+
+int mpnn_set_state(fsd_handle* h, const float* host, int n, int t) {
+    if (n != 3 * MpLayout::total || t < 0) return FSD_ERR_BAD_PARAMS;
+    MP_TRY(mpnn_set_weights(h, host, MpLayout::total));
+    MpState* s = mp(h);
+    const size_t m = MpLayout::total;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->mw, host + m, sizeof(float) * m, cudaMemcpyHostToDevice, h->stream));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->vw, host + 2 * m, sizeof(float) * m, cudaMemcpyHostToDevice, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    s->adam_t = t;
+    return FSD_OK;
+}
+
 bool mpnn_loaded(fsd_handle* h) {
     LearnedState* ls = (LearnedState*)h->learned;
     return ls && ls->mp && ((MpState*)ls->mp)->loaded;
@@ -1041,7 +1049,8 @@ bool mpnn_loaded(fsd_handle* h) {
 
 void mpnn_use_umma(fsd_handle* h, bool on) { mp(h)->use_umma = on; }
 
-// Inference: graph, forward, head -> G (precond_build of FSD_PRECOND_LEARNED).
+// Inference: graph, forward, head -> correction added to the approximate
+// inverse (precond_build of FSD_PRECOND_LEARNED, after spai_build).
 int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist,
                const float* a_blocks) {
     MP_TRY(mp_graph(h, pos, a_pn, a_plist, a_blocks));
@@ -1049,8 +1058,9 @@ int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const uns
     return mp_head(h);
 }
 
-// Loss and gradient for given probes (host P x 6N, or NULL to draw standard
-// normals from (seed, step)); with lr > 0 also one Adam step.  The neighbour
+// Loss and gradient for given probes z (host P x 6N), or for z = w - A G0 w
+// with w standard normals drawn from (seed, step); with lr > 0 also one Adam
+// step.  The neighbour
 // list must be current for pos; the pruned matrix is assembled here.
 int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, int P, uint32_t step, float lr,
                     float* loss_out, float* host_grad) {
@@ -1058,14 +1068,23 @@ int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, 
     if (!mpnn_loaded(h) || P < 1) return FSD_ERR_BAD_PARAMS;
     MpState* s = mp(h);
     MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
-    MP_TRY(mpnn_infer(h, pos, ls->a_pn, ls->a_plist, ls->a_blocks));
-    MP_TRY(mp_alloc_backward(h));
+    MP_TRY(spai_build(h));
     MP_TRY(mp_probes(h, P));
     const size_t n = (size_t)P * 6 * s->N;
-    if (host_probes)
+    if (host_probes) {
         FSD_CHECK_CUDA(cudaMemcpyAsync(s->Zp, host_probes, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
-    else
-        gaussian(h, s->Zp, n, step, kStreamLearned, 1.0f);
+    } else {
+        const int rows = (8 * s->N + 255) / 256;
+        gaussian(h, s->Vp, n, step, kStreamLearned, 1.0f);
+        count_launch();
+        k_bsr_multi<<<rows, 256, 0, h->stream>>>(ls->g_rowptr, ls->g_col, ls->g_val, s->Vp, s->Up, s->N, P);
+        count_launch();
+        k_pruned_multi<<<rows, 256, 0, h->stream>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Up, s->Zp, s->N, P);
+        count_launch();
+        k_sub<<<296, kThreads, 0, h->stream>>>(s->Vp, s->Zp, n);
+    }
+    MP_TRY(mpnn_infer(h, pos, ls->a_pn, ls->a_plist, ls->a_blocks));
+    MP_TRY(mp_alloc_backward(h));
     MP_TRY(mp_loss(h, P, true));
     FSD_CHECK_CUDA(cudaMemsetAsync(s->gw, 0, sizeof(float) * MpLayout::total, h->stream));
     MP_TRY(mp_backward(h));

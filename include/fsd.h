@@ -96,7 +96,6 @@ typedef struct fsd_params {
     int learned_inner;           /* FSD_PRECOND_LEARNED: inner GMRES steps on R_FU^pruned + D per application,
                                     right-preconditioned by the learned block-sparse G (4; 0 = apply G once).
                                     With inner steps the outer solve is flexible GMRES. */
-    float learned_rg;            /* FSD_PRECOND_LEARNED: pair distance below which G has a block (3.0) */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
@@ -244,24 +243,31 @@ int fsd_precond_build(fsd_handle* h, const float* d_pos);
  * d_blocks (nnzb x 36, row-major 6x6 fp32).  The structure is checked
  * (rowptr monotone, rowptr[N] = nnzb, 0 <= col < N) and the arrays copied. */
 int fsd_precond_set_blocks(fsd_handle* h, int nnzb, const int* d_rowptr, const int* d_col, const float* d_blocks);
-/* Learned preconditioner network (FSD_PRECOND_LEARNED; the network has no
- * counterpart in the reference).  A message-passing network on the graph of
- * pairs closer than learned_rg predicts G ~ (R_FU^pruned + D)^-1 from
- * rotation-invariant pair features through an axisymmetric 6x6 block basis,
- * so G rotates with the configuration.  Weights are one flat fp32 vector of
- * fsd_learned_num_weights() entries (layout in fsd_b200/csrc/fsd_mpnn.h);
- * setting weights makes precond_build use the network (blocks set with
- * fsd_precond_set_blocks take over again when set later).
+/* Learned preconditioner (FSD_PRECOND_LEARNED; no counterpart in the
+ * reference, which factors the same block by IC(0)).  G ~ (R_FU^pruned + D)^-1
+ * is the sparse approximate inverse of that matrix on the two-hop sets of the
+ * pruned contact graph (FP64 least squares per particle), plus, once weights
+ * are set, a correction predicted by a message-passing network on the same
+ * pairs from rotation-invariant pair features through an axisymmetric 6x6
+ * block basis (so G rotates with the configuration).  Weights are one flat
+ * fp32 vector of fsd_learned_num_weights() entries (layout in
+ * fsd_b200/csrc/fsd_mpnn.h); blocks set with fsd_precond_set_blocks replace
+ * both until weights are set again.
  * fsd_learned_train_step: loss E_z ||A G z - z||^2 / 6N over n_probes probe
- * vectors z (host_probes, n_probes x 6N, or NULL for counter-based normals
- * drawn from (seed, step)), its gradient (host_grad, optional) and, when
- * lr > 0, one Adam step.  The neighbour list must be current for d_pos.
+ * vectors z (host_probes, n_probes x 6N; or NULL for z = w - A G0 w, the
+ * residuals the uncorrected approximate inverse G0 leaves for counter-based
+ * normals w drawn from (seed, step)), its gradient (host_grad, optional)
+ * and, when lr > 0, one Adam step.  The neighbour list must be current for d_pos.
  * fsd_learned_tensor_cores(h, 0) runs the dense layers in FP32 SIMT instead
  * of BF16 on the tensor cores. */
 int fsd_learned_num_weights(void);
 int fsd_learned_set_weights(fsd_handle* h, const float* host_w, int n);
 int fsd_learned_get_weights(fsd_handle* h, float* host_w, int n);
 int fsd_learned_tensor_cores(fsd_handle* h, int on);
+/* Training state: weights, Adam first and second moments (3 x num_weights
+ * floats) and the Adam step count, to continue training on another handle. */
+int fsd_learned_get_state(fsd_handle* h, float* host, int n, int* adam_step);
+int fsd_learned_set_state(fsd_handle* h, const float* host, int n, int adam_step);
 int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,
                            unsigned int step, float lr, float* loss, float* host_grad);
 /* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */

@@ -1,9 +1,11 @@
 """FP64 NumPy restatement of the learned preconditioner -- TEST INFRASTRUCTURE ONLY.
 
-Checker for fsd_b200/csrc/mpnn.cu: the pair graph, the invariant edge
-features, the message-passing network, the axisymmetric block head that turns
-its outputs into G ~ (R_FU^pruned + D)^-1, and the approximate-inverse loss
-    L = sum_p ||A G z_p - z_p||^2 / (P 6N).
+Checker for fsd_b200/csrc/mpnn.cu: the pair graph (the two-hop sets of the
+sparse approximate inverse), the invariant edge features, the message-passing
+network, the axisymmetric block head whose output corrects the approximate
+inverse G ~ (R_FU^pruned + D)^-1, and the loss
+    L = sum_p ||A G z_p - z_p||^2 / (P 6N)
+(training draws z = w - A G0 w from the residuals of the uncorrected G0).
 The network has no counterpart in the reference; A is the reference's pruned
 preconditioner matrix (Precondition.cu:530-836 plus the identity shift of
 Helper_Precondition.cu:535-580), restated in fsd_oracle.pruned_rfu_sparse.
@@ -68,21 +70,20 @@ def init_weights(seed=0, head_scale=1e-3):
     return w
 
 
-def graph(pos, L, xy, rg):
-    """Directed pairs i -> j closer than rg (single-precision separations, as
-    the kernels), with unit vectors and distances."""
+def graph(pos, L, xy, sets, prow):
+    """Directed pairs c -> s for s != c in c's two-hop set, single-precision
+    separations as the kernels; `direct` marks pairs in each other's pruned list."""
     p = np.asarray(pos, np.float32)[:, :3]
-    N = len(p)
-    i_all, j_all = np.nonzero(np.ones((N, N), bool) & ~np.eye(N, dtype=bool))
-    R = O.min_image32(p[j_all] - p[i_all], L, xy)
+    i = np.array([c for c, S in enumerate(sets) for s in S[1:]], np.int64)
+    j = np.array([s for c, S in enumerate(sets) for s in S[1:]], np.int64)
+    R = O.min_image32(p[j] - p[i], L, xy)
     d2 = R[:, 0] * R[:, 0] + R[:, 1] * R[:, 1] + R[:, 2] * R[:, 2]
-    keep = d2 < np.float32(rg) * np.float32(rg)
-    i, j, R, d2 = i_all[keep], j_all[keep], R[keep].astype(np.float64), d2[keep]
     d = np.sqrt(d2.astype(np.float32)).astype(np.float64)
-    return i, j, R / d[:, None], d
+    direct = np.array([s in prow[c] for c, s in zip(i, j)], bool)
+    return i, j, R.astype(np.float64) / d[:, None], d, direct
 
 
-def features(d, tdist, tvals):
+def features(d, direct, tdist, tvals):
     h = d - 2.0
     c = O.res_interp(d, 0, 10, tdist, tvals, mode="lub")
     x = np.zeros((len(d), FEAT))
@@ -91,7 +92,8 @@ def features(d, tdist, tvals):
     x[:, 2] = np.exp(-10.0 * np.maximum(h, 0.0))
     x[:, 3] = 2.0 / d
     x[:, 4:14] = np.sign(c) * np.log1p(np.abs(c)) * 0.25
-    x[:, 14] = 1.0
+    x[:, 14] = direct
+    x[:, 15] = 1.0
     return x
 
 
@@ -136,25 +138,30 @@ def axis_block(o, r):
 
 
 def g_blocks(oe, on, J, i, rhat, N):
-    """Edge blocks G_ij = J_i B(o_ij) and self blocks G_ii = J_i (I + iso + sum_j B(s_ij))."""
+    """Correction blocks dG_ij = J_i B(o_ij) and dG_ii = J_i (iso + sum_j B(q_ij))."""
     Ge = np.einsum("nab,nbc->nac", J[i], axis_block(oe[:, :6], rhat))
     S = np.zeros((N, 6, 6))
     np.add.at(S, i, axis_block(oe[:, 6:12], rhat))
-    d = np.concatenate([np.repeat(1.0 + on[:, :1], 3, 1), np.repeat(1.0 + on[:, 1:2], 3, 1)], 1)
+    d = np.concatenate([np.repeat(on[:, :1], 3, 1), np.repeat(on[:, 1:2], 3, 1)], 1)
     S[:, np.arange(6), np.arange(6)] += d
     Gs = np.einsum("nab,nbc->nac", J, S)
     return Ge, Gs
 
 
-def problem(pos, L, xy, rg=3.0):
+def problem(pos, L, xy):
     """Everything the loss needs that does not depend on the weights."""
+    import scipy.sparse as sp
     tdist, tvals = O.resistance_table()
     N = len(pos)
-    A = O.pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=O.neighbor_list(pos, L, xy, rg + 2.5)).tocsr()
+    A = O.pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=O.neighbor_list(pos, L, xy, 6.0)).tocsr()
+    Ab = sp.bsr_matrix(A, blocksize=(6, 6))
+    Ab.sort_indices()
+    sets = O.spai_sets(Ab, N)
+    prow = [set(int(k) for k in Ab.indices[Ab.indptr[c]:Ab.indptr[c + 1]]) for c in range(N)]
     J = np.stack([np.linalg.inv(A[6 * k:6 * k + 6, 6 * k:6 * k + 6].toarray()) for k in range(N)])
-    i, j, rhat, d = graph(pos, L, xy, rg)
-    x = features(d, tdist, tvals)
-    return dict(N=N, A=A, J=J, i=i, j=j, rhat=rhat, x=x)
+    i, j, rhat, d, direct = graph(pos, L, xy, sets, prow)
+    x = features(d, direct, tdist, tvals)
+    return dict(N=N, A=A, G0=O.spai2(A, N), J=J, i=i, j=j, rhat=rhat, x=x)
 
 
 def g_matrix(wv, pr):
@@ -167,7 +174,8 @@ def g_matrix(wv, pr):
     blocks = np.concatenate([Ge, Gs])
     ri = (6 * rows[:, None, None] + np.arange(6)[None, :, None]) * np.ones((1, 1, 6), np.int64)
     ci = (6 * cols[:, None, None] + np.arange(6)[None, None, :]) * np.ones((1, 6, 1), np.int64)
-    return sp.csr_matrix((blocks.ravel(), (ri.ravel(), ci.ravel())), shape=(6 * N, 6 * N))
+    dG = sp.csr_matrix((blocks.ravel(), (ri.ravel(), ci.ravel())), shape=(6 * N, 6 * N))
+    return pr["G0"] + dG
 
 
 def loss(wv, pr, Z):

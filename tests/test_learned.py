@@ -4,7 +4,8 @@ network gains in the saddle solve.
 
 Tolerances: the FP32 SIMT path must reproduce the oracle loss to 1e-4 relative
 and its gradient along random directions to 2e-3 relative (central differences
-of the FP64 oracle loss).  The tensor-core path rounds activations and weights
+of the FP64 oracle loss).  The loss includes the two-hop approximate inverse
+the network corrects.  The tensor-core path rounds activations and weights
 to BF16, so it is held to 3e-2 on the loss and 6e-2 on directional gradients.
 """
 from __future__ import annotations
@@ -30,6 +31,7 @@ def _setup(N=200, phi=0.35, seed=4):
     p = torch.as_tensor(pos).cuda().view(-1).contiguous()
     s.build_neighbor_list(p)
     return s, p, M.problem(pos, L, 0.0)
+
 
 
 def _directional(w, pr, Z, d, eps=1e-4):
@@ -58,15 +60,20 @@ def test_loss_and_gradient_match_oracle(cuda, tensor_cores, tol_l, tol_g):
 
 @pytest.mark.gpu
 def test_training_reduces_loss_and_is_reproducible(cuda):
+    """From zero heads (G = the two-hop approximate inverse), Adam steps on
+    fresh probes lower the loss on a held-fixed probe draw, bit for bit the
+    same in two runs."""
     runs = []
     for rep in range(2):
         s, p, pr = _setup(N=400, phi=0.4, seed=6)
-        s.learned_set_weights(M.init_weights(0))
-        losses = [s.learned_train_step(p, n_probes=4, step=t, lr=2e-3) for t in range(40)]
-        runs.append((losses, s.learned_get_weights()))
+        s.learned_set_weights(M.init_weights(0, head_scale=0.0))
+        before = s.learned_train_step(p, n_probes=4, step=0, lr=0.0)
+        losses = [s.learned_train_step(p, n_probes=4, step=t, lr=1e-4) for t in range(1, 41)]
+        after = s.learned_train_step(p, n_probes=4, step=0, lr=0.0)
+        runs.append((before, after, losses, s.learned_get_weights()))
         s.close()
-    assert np.mean(runs[0][0][-5:]) < 0.8 * np.mean(runs[0][0][:5])
-    assert runs[0][0] == runs[1][0] and np.array_equal(runs[0][1], runs[1][1])
+    assert runs[0][1] < runs[0][0]
+    assert runs[0][2] == runs[1][2] and np.array_equal(runs[0][3], runs[1][3])
 
 
 @pytest.mark.gpu
