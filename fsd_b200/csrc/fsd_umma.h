@@ -15,5 +15,7 @@ void umma_gemm(const float* const* p, const int* const* idx, int width, int part
 // dX[r][k] = sum_o dY[r][o] W[o][k]
 bool umma_gemm_dx_supported(int O, int K);
 void umma_gemm_dx(const float* dY, int rows, int O, const float* Wt, int K, float* dX, cudaStream_t st);
+// 1 if an mbarrier wait of these kernels ran out since the last call (then cleared); synchronises the device.
+int umma_error();
 
 }  // namespace fsd

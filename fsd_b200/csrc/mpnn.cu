@@ -1102,6 +1102,7 @@ int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, 
         FSD_CHECK_CUDA(cudaMemcpyAsync(host_grad, s->gw, sizeof(float) * MpLayout::total, cudaMemcpyDeviceToHost,
                                        h->stream));
     FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (s->use_umma && umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
     if (loss_out) *loss_out = (float)loss;
     return FSD_OK;
 }
