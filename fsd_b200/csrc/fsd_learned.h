@@ -35,6 +35,14 @@ struct LearnedState {
     unsigned* sp_cnt = nullptr;      // bucket counts, truncated sets, failed rows
     unsigned* sp_host = nullptr;
     int sp_truncated = 0;
+    // inner solve replayed as a CUDA graph on fixed 17N input/output buffers
+    float* tb = nullptr;
+    float* tx = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey[8] = {};
+    int gkey_k = -1;
+    int captures = 0;
 };
 
 LearnedState* learned(fsd_handle* h);

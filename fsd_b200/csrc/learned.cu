@@ -7,6 +7,8 @@
 // message-passing network at each preconditioner build, or set directly through
 // fsd_precond_set_blocks.  The saddle pre/post steps (Saddle.cu:171-264) are
 // fused into the SpMV kernel, exactly as in the IC(0) solve kernels.
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -32,6 +34,10 @@ void learned_free(fsd_handle* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->sp_host) cudaFreeHost(s->sp_host);
+    if (s->tb) cudaFree(s->tb);
+    if (s->tx) cudaFree(s->tx);
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
     delete s;
     h->learned = nullptr;
 }
@@ -47,9 +53,11 @@ int learned_reserve(fsd_handle* h, int nnzb) {
         s->g_col = nullptr;
         s->g_val = nullptr;
         s->g_cap = 0;
-        FSD_CHECK_CUDA(cudaMalloc(&s->g_col, sizeof(int) * (size_t)nnzb));
-        FSD_CHECK_CUDA(cudaMalloc(&s->g_val, sizeof(float) * 36 * (size_t)nnzb));
-        s->g_cap = nnzb;
+        // headroom, so that pattern growth from step to step rarely reallocates
+        const int cap = nnzb + nnzb / 8 + 1024;
+        FSD_CHECK_CUDA(cudaMalloc(&s->g_col, sizeof(int) * (size_t)cap));
+        FSD_CHECK_CUDA(cudaMalloc(&s->g_val, sizeof(float) * 36 * (size_t)cap));
+        s->g_cap = cap;
     }
     return FSD_OK;
 }
@@ -352,6 +360,8 @@ static int inner_alloc(fsd_handle* h) {
     FSD_CHECK_CUDA(cudaMalloc(&s->Zi, sizeof(float) * n6 * kMaxInner));
     FSD_CHECK_CUDA(cudaMalloc(&s->part, sizeof(double) * (kMaxInner + 2) * kInnerBlocks));
     FSD_CHECK_CUDA(cudaMalloc(&s->H, sizeof(double) * ((kMaxInner + 1) * kMaxInner + 1 + kMaxInner)));
+    FSD_CHECK_CUDA(cudaMalloc(&s->tb, sizeof(float) * 17 * (size_t)h->p.N));
+    FSD_CHECK_CUDA(cudaMalloc(&s->tx, sizeof(float) * 17 * (size_t)h->p.N));
     s->inner_cap = kMaxInner;
     return FSD_OK;
 }
@@ -360,11 +370,70 @@ bool precond_is_flexible(const fsd_handle* h) {
     return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0;
 }
 
+// Kernels of one inner solve, enqueued on st (also used for graph capture).
+static int inner_enqueue(fsd_handle* h, const float* b, float* x, cudaStream_t st) {
+    LearnedState* s = learned(h);
+    const int N = h->p.N;
+    const int k = h->p.learned_inner;
+    const size_t n6 = 6 * (size_t)N;
+    const int rows = (8 * N + 255) / 256;
+    const int nb = kInnerBlocks;
+    k_inner_rhs<<<nb, kInnerThreads, 0, st>>>(b, s->t, N, s->part);
+    k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->t, s->Vi, n6, s->part, nb, s->H, -1);
+    for (int j = 0; j < k; ++j) {
+        float* vj = s->Vi + (size_t)j * n6;
+        float* zj = s->Zi + (size_t)j * n6;
+        k_bsr_spmv<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, vj, zj, N);
+        k_pruned_spmv<<<rows, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, zj, s->w, N);
+        k_inner_dots<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->w, n6, s->part);
+        k_inner_finish<<<1, 32 * (j + 1), 0, st>>>(s->part, nb, j + 1, s->H, j);
+        k_inner_orth<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->H, j, s->w, n6, s->part);
+        k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->w, s->Vi + (size_t)(j + 1) * n6, n6, s->part, nb, s->H, j);
+    }
+    k_inner_lsq<<<1, 32, 0, st>>>(s->H, k);
+    k_inner_post<<<(11 * N + 255) / 256, 256, 0, st>>>(s->Zi, n6, k, s->H + (size_t)(kMaxInner + 1) * kMaxInner + 1,
+                                                       b, x, N);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+static int inner_kernels(int k) { return 4 + 6 * k; }
+
+// (Re)capture the inner solve when the arrays it reads were reallocated or k changed.
+static int inner_graph(fsd_handle* h) {
+    LearnedState* s = learned(h);
+    const void* key[8] = {s->g_rowptr, s->g_col, s->g_val, s->a_pn, s->a_plist, s->a_blocks, s->Vi, s->Zi};
+    bool same = s->gexec && s->gkey_k == h->p.learned_inner;
+    for (int i = 0; i < 8 && same; ++i) same = key[i] == s->gkey[i];
+    if (same) return FSD_OK;
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+    if (!s->cap_stream) FSD_CHECK_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    FSD_CHECK_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+    const int e = inner_enqueue(h, s->tb, s->tx, s->cap_stream);
+    const cudaError_t ce = cudaStreamEndCapture(s->cap_stream, &g);
+    if (e != FSD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return e;
+    }
+    FSD_CHECK_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
+    cudaGraphDestroy(g);
+    FSD_CHECK_CUDA(ie);
+    for (int i = 0; i < 8; ++i) s->gkey[i] = key[i];
+    s->gkey_k = h->p.learned_inner;
+    s->captures += 1;
+    if (getenv("FSD_DEBUG_GRAPH")) fprintf(stderr, "inner graph captured (%d)\n", s->captures);
+    return FSD_OK;
+}
+
 // x = P^-1 b.  Without inner steps G is applied once (fused with the saddle
 // pre/post steps).  With k inner steps, y ~ (R_FU^pruned + D)^-1 t comes from
 // k steps of GMRES on that matrix from a zero guess, right-preconditioned by
 // G; the map b -> x then depends on b nonlinearly, which the flexible outer
-// GMRES allows.  No host synchronisation.
+// GMRES allows.  The inner solve is one CUDA graph launch between a copy of b
+// in and a copy of x out; no host synchronisation.
 int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
@@ -376,35 +445,13 @@ int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
         FSD_CHECK_CUDA(cudaGetLastError());
         return FSD_OK;
     }
-    const size_t n6 = 6 * (size_t)N;
-    const int rows = (8 * N + 255) / 256;
-    const int nb = kInnerBlocks;
-    count_launch();
-    k_inner_rhs<<<nb, kInnerThreads, 0, st>>>(b, s->t, N, s->part);
-    count_launch();
-    k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->t, s->Vi, n6, s->part, nb, s->H, -1);
-    for (int j = 0; j < k; ++j) {
-        float* vj = s->Vi + (size_t)j * n6;
-        float* zj = s->Zi + (size_t)j * n6;
-        count_launch();
-        k_bsr_spmv<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, vj, zj, N);
-        count_launch();
-        k_pruned_spmv<<<rows, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, zj, s->w, N);
-        count_launch();
-        k_inner_dots<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->w, n6, s->part);
-        count_launch();
-        k_inner_finish<<<1, 32 * (j + 1), 0, st>>>(s->part, nb, j + 1, s->H, j);
-        count_launch();
-        k_inner_orth<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->H, j, s->w, n6, s->part);
-        count_launch();
-        k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->w, s->Vi + (size_t)(j + 1) * n6, n6, s->part, nb, s->H, j);
-    }
-    count_launch();
-    k_inner_lsq<<<1, 32, 0, st>>>(s->H, k);
-    count_launch();
-    k_inner_post<<<(11 * N + 255) / 256, 256, 0, st>>>(s->Zi, n6, k,
-                                                       s->H + (size_t)(kMaxInner + 1) * kMaxInner + 1, b, x, N);
-    FSD_CHECK_CUDA(cudaGetLastError());
+    const int e = inner_graph(h);
+    if (e != FSD_OK) return e;
+    const size_t n17 = 17 * (size_t)N;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->tb, b, sizeof(float) * n17, cudaMemcpyDeviceToDevice, st));
+    FSD_CHECK_CUDA(cudaGraphLaunch(s->gexec, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(x, s->tx, sizeof(float) * n17, cudaMemcpyDeviceToDevice, st));
+    for (int i = 0; i < inner_kernels(k); ++i) count_launch();
     return FSD_OK;
 }
 
