@@ -122,9 +122,11 @@ class FSD:
 
     def set_box(self, Lx, Ly, Lz, xy):
         check(lib().fsd_set_box(self._h, Lx, Ly, Lz, xy), "fsd_set_box")
+        self.params.xy = float(xy)
 
     def set_temperature(self, T):
         check(lib().fsd_set_temperature(self._h, T), "fsd_set_temperature")
+        self.params.T = float(T)
 
     # -- neighbour list --------------------------------------------------------
     def build_neighbor_list(self, pos: torch.Tensor):
