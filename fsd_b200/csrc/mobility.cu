@@ -77,19 +77,41 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
-// Radix-p DFT of y[0..p) in place, w_p^1 = wp (forward convention handled by caller).
+// Radix-P DFT of y[0..P) in place with the roots w_P^m = exp(-2 pi i m / P)
+// as constants (conjugated for the inverse).
+// cos and sin of -2 pi m / P for the radices used (m < P); folded to
+// constants once the DFT loops are unrolled.
+__host__ __device__ constexpr float root_c(int P, int m) {
+    return P == 2 ? (m == 0 ? 1.0f : -1.0f)
+         : P == 3 ? (m == 0 ? 1.0f : -0.5f)
+         : P == 4 ? (m == 0 ? 1.0f : (m == 2 ? -1.0f : 0.0f))
+         : P == 5 ? (m == 0 ? 1.0f : (m == 1 || m == 4) ? 0.30901699437494742f : -0.80901699437494742f)
+         : /* 8 */ (m == 0 ? 1.0f : m == 4 ? -1.0f : (m == 2 || m == 6) ? 0.0f
+                    : (m == 1 || m == 7) ? 0.70710678118654752f : -0.70710678118654752f);
+}
+__host__ __device__ constexpr float root_s(int P, int m) {
+    return P == 2 ? 0.0f
+         : P == 3 ? (m == 0 ? 0.0f : m == 1 ? -0.86602540378443865f : 0.86602540378443865f)
+         : P == 4 ? (m == 1 ? -1.0f : m == 3 ? 1.0f : 0.0f)
+         : P == 5 ? (m == 0 ? 0.0f : m == 1 ? -0.95105651629515357f : m == 2 ? -0.58778525229247313f
+                    : m == 3 ? 0.58778525229247313f : 0.95105651629515357f)
+         : /* 8 */ (m == 0 || m == 4 ? 0.0f : m == 2 ? -1.0f : m == 6 ? 1.0f
+                    : (m == 1 || m == 3) ? -0.70710678118654752f : 0.70710678118654752f);
+}
+
 template <int P>
-__device__ __forceinline__ void small_dft(float2* y, const float2* tw, int n, bool inv) {
+__device__ __forceinline__ void small_dft(float2* y, bool inv) {
+    const float sg = inv ? -1.0f : 1.0f;
     float2 z[P];
 #pragma unroll
     for (int j = 0; j < P; ++j) {
         float2 acc = y[0];
 #pragma unroll
         for (int s = 1; s < P; ++s) {
-            float2 w = tw[((j * s) % P) * (n / P)];
-            if (inv) w.y = -w.y;
-            acc.x += y[s].x * w.x - y[s].y * w.y;
-            acc.y += y[s].x * w.y + y[s].y * w.x;
+            const int m = (j * s) % P;
+            const float wc = root_c(P, m), ws = sg * root_s(P, m);
+            acc.x += y[s].x * wc - y[s].y * ws;
+            acc.y += y[s].x * ws + y[s].y * wc;
         }
         z[j] = acc;
     }
@@ -97,13 +119,26 @@ __device__ __forceinline__ void small_dft(float2* y, const float2* tw, int n, bo
     for (int j = 0; j < P; ++j) y[j] = z[j];
 }
 
+// floor(a / d) for a < 2^20 and 1 <= d <= 2^12 from a float reciprocal: the
+// true quotient plus 0.5/d stays at least 0.5/d away from an integer, more
+// than the rounding error of the product (a/d * 2^-22 < 0.25/d).
+__device__ __forceinline__ int qdiv(int a, float inv_d, float half_inv) {
+    return (int)__fmaf_rn((float)a, inv_d, half_inv);
+}
+
+// One Stockham stage of radix P over nlines lines of length n; Ls = product of
+// the radices before it.  The twiddle index j1 * s * r is below n (j1 < Ls,
+// r = n / (Ls P), s < P), so no reduction is needed.
 template <int P>
 __device__ __forceinline__ void stockham_stage(const float2* in, float2* out, int nlines, int n, int Ls,
                                                const float2* tw, bool inv) {
     const int L = Ls * P, r = n / L, nb = n / P;
-    for (int w = threadIdx.x; w < nlines * nb; w += blockDim.x) {
-        const int line = w / nb, bf = w - line * nb;
-        const int k = bf % r, j1 = bf / r;
+    const float inv_nb = 1.0f / (float)nb, h_nb = 0.5f / (float)nb;
+    const float inv_r = 1.0f / (float)r, h_r = 0.5f / (float)r;
+    const int total = nlines * nb;
+    for (int w = threadIdx.x; w < total; w += blockDim.x) {
+        const int line = qdiv(w, inv_nb, h_nb), bf = w - line * nb;
+        const int j1 = qdiv(bf, inv_r, h_r), k = bf - j1 * r;
         const float2* X = in + line * n;
         float2* Y = out + line * n;
         float2 y[P];
@@ -111,13 +146,13 @@ __device__ __forceinline__ void stockham_stage(const float2* in, float2* out, in
         for (int s = 0; s < P; ++s) {
             float2 v = X[k + s * r + r * P * j1];
             if (s > 0 && j1 > 0) {
-                float2 w = tw[(j1 * s * r) % n];
-                if (inv) w.y = -w.y;
-                v = cmul(v, w);
+                float2 t = tw[j1 * s * r];
+                if (inv) t.y = -t.y;
+                v = cmul(v, t);
             }
             y[s] = v;
         }
-        small_dft<P>(y, tw, n, inv);
+        small_dft<P>(y, inv);
 #pragma unroll
         for (int j2 = 0; j2 < P; ++j2) Y[k + r * (j1 + Ls * j2)] = y[j2];
     }
@@ -223,7 +258,14 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids) {
     const float2* twx = h->w.twiddle;
     const float2* twy = twx + Nx;
     const float2* twz = twy + Ny;
-    const int Bxy = 16;
+    // x and y passes: lines of consecutive z, B of them per block; a divisor
+    // of Nz avoids a partial last chunk.
+    int Bxy = 16;
+    for (int d = 32; d >= 8; --d)
+        if (Nz % d == 0) {
+            Bxy = d;
+            break;
+        }
     const int Bz = fft_batch_z(Nx, Ny, Nz);
     auto launch = [&](int axis) {
         const FFTPlan& pl = axis == 0 ? px : (axis == 1 ? py : pz);
