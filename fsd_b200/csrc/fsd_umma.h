@@ -15,6 +15,12 @@ void umma_gemm(const float* const* p, const int* const* idx, int width, int part
 // dX[r][k] = sum_o dY[r][o] W[o][k]
 bool umma_gemm_dx_supported(int O, int K);
 void umma_gemm_dx(const float* dY, int rows, int O, const float* Wt, int K, float* dX, cudaStream_t st);
+// dW[o][k] += sum_r dY[r][o] X(r, k) and db[o] += sum_r dY[r][o]; `part`
+// holds umma_dw_part_floats(rows, K, O) floats of per-CTA partial sums.
+bool umma_gemm_dw_supported(int K, int O);
+size_t umma_dw_part_floats(int rows, int K, int O);
+void umma_gemm_dw(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* dY,
+                  int O, float* dW, float* db, float* part, cudaStream_t st);
 // 1 if an mbarrier wait of these kernels ran out since the last call (then cleared); synchronises the device.
 int umma_error();
 

@@ -770,6 +770,16 @@ static int mp_gemm_dw(fsd_handle* h, const GemmIn& in, int rows, const float* dY
     MpState* s = mp(h);
     if (rows <= 0) return FSD_OK;
     const int K = in.width * in.parts;
+    if (s->use_umma && umma_gemm_dw_supported(K, O)) {
+        const size_t need = umma_dw_part_floats(rows, K, O);
+        if (need > s->dwpart_cap) {
+            MP_TRY(grow(&s->dwpart, need));
+            s->dwpart_cap = need;
+        }
+        for (int i = 0; i < 4; ++i) count_launch();
+        umma_gemm_dw(in.p, in.idx, in.width, in.parts, rows, dY, O, dW, db, s->dwpart, h->stream);
+        return FSD_OK;
+    }
     const int nparts = (rows + kRowsPerPart - 1) / kRowsPerPart;
     const size_t need = (size_t)nparts * O * (K + 1);
     if (need > s->dwpart_cap) {

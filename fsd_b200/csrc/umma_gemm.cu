@@ -260,10 +260,132 @@ __global__ void __launch_bounds__(kThreads) k_umma_dx(const float* __restrict__ 
     if (warp == 0) tmem_dealloc(tmem, tmem_cols(K));
 }
 
+// Weight gradient dW^T[K x O] = X^T dY over one chunk of kDwRows rows per
+// CTA: M = the K features in tiles of 128 (zero-padded), N = O, the MMA's
+// K dimension = rows, staged kDwSub rows at a time (smem reused after each
+// commit completes).  Each CTA writes its partial (Kpad x O, FP32); a second
+// kernel sums the partials in CTA order into dW and db.
+constexpr int kDwRows = 512;
+constexpr int kDwSub = 64;
+
+__global__ void __launch_bounds__(kThreads) k_umma_dw(Parts in, int width, int parts, int rows,
+                                                      const float* __restrict__ dY, int O, float* __restrict__ part) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    const int K = width * parts;
+    const int mt = (K + kRows - 1) / kRows;  // 128-feature M tiles
+    const int Kp = mt * kRows;
+    unsigned char* sa = smem;                            // X^T: Kp features x kDwSub rows
+    unsigned char* sb = smem + (size_t)Kp * kDwSub * 2;  // dY^T: O x kDwSub rows
+    const int r0 = blockIdx.x * kDwRows;
+    const int warp = threadIdx.x >> 5;
+    if (warp == 0) tmem_alloc(&tmem_base, tmem_cols(mt * O));
+    if (threadIdx.x == 0) mbar_init(&bar);
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base;
+    bool ok = true;
+    int phase = 0;
+    for (int c0 = 0; c0 < kDwRows && r0 + c0 < rows; c0 += kDwSub) {
+        for (int t = threadIdx.x; t < Kp * kDwSub; t += blockDim.x) {
+            const int rr = t / Kp, f = t - rr * Kp;  // consecutive threads: consecutive features of one row
+            const int r = r0 + c0 + rr;
+            float v = 0.f;
+            if (f < K && r < rows) {
+                const int p = f / width, col = f - p * width;
+                const int src = in.idx[p] ? in.idx[p][r] : r;
+                v = in.p[p][(size_t)src * width + col];
+            }
+            st_bf16(sa, kmajor_off(f, rr, Kp), v);
+        }
+        for (int t = threadIdx.x; t < O * kDwSub; t += blockDim.x) {
+            const int rr = t / O, o = t - rr * O;
+            const int r = r0 + c0 + rr;
+            st_bf16(sb, kmajor_off(o, rr, O), r < rows ? dY[(size_t)r * O + o] : 0.f);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        fence_after();
+        if (threadIdx.x == 0) {
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+            const uint32_t lbo_a = (uint32_t)(Kp / 8) * 128, lbo_b = (uint32_t)(O / 8) * 128;
+            const uint32_t idesc = make_idesc(kRows, O);
+            for (int m = 0; m < mt; ++m)
+                for (int ks = 0; ks < kDwSub / 16; ++ks) {
+                    // A rows [m*128, m*128+128): 16 core-matrix groups further along M (SBO = 128 B each)
+                    const uint64_t da = make_desc(a0 + (uint32_t)ks * 2 * lbo_a + (uint32_t)m * 16 * 128, lbo_a, 128);
+                    const uint64_t db = make_desc(b0 + (uint32_t)ks * 2 * lbo_b, lbo_b, 128);
+                    mma_bf16(tmem + (uint32_t)(m * O), da, db, idesc, (c0 > 0 || ks > 0));
+                }
+            mma_commit(&bar);
+        }
+        bool w = mbar_wait(&bar, (uint32_t)phase);
+        if (!w) {
+            atomicExch(&g_umma_error, 1);
+            mbar_wait(&bar, (uint32_t)phase);
+        }
+        ok = (__syncthreads_and(w) != 0) && ok;
+        fence_after();
+        phase ^= 1;
+        if (!ok) break;
+    }
+    if (ok) {
+        const int row = warp * 32 + (threadIdx.x & 31);  // feature within an M tile
+        float* out = part + (size_t)blockIdx.x * Kp * O;
+        for (int m = 0; m < mt; ++m)
+            for (int c0 = 0; c0 < O; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * O + c0), v);
+#pragma unroll
+                for (int c = 0; c < 16; ++c) out[(size_t)(m * kRows + row) * O + c0 + c] = v[c];
+            }
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols(mt * O));
+}
+
+// dW[o][k] += sum_b part[b][k][o];  db[o] += sum_r dY[r][o] (column sums in row order).
+__global__ void k_dw_reduce(const float* __restrict__ part, int nparts, int Kp, int K, int O, float* dW) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= K * O) return;
+    const int k = t / O, o = t - k * O;
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += part[((size_t)b * Kp + k) * O + o];
+    dW[(size_t)o * K + k] += (float)s;
+}
+
+// Bias gradient in two fixed-order stages: column sums per kDwRows chunk, then over chunks.
+__global__ void k_db_part(const float* __restrict__ dY, int rows, int O, float* __restrict__ dpart) {
+    const int o = threadIdx.x;
+    if (o >= O) return;
+    const int r0 = blockIdx.x * kDwRows, r1 = min(rows, r0 + kDwRows);
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += dY[(size_t)r * O + o];
+    dpart[(size_t)blockIdx.x * O + o] = s;
+}
+
+__global__ void k_db_reduce(const float* __restrict__ dpart, int nparts, int O, float* db) {
+    const int o = threadIdx.x;
+    if (o >= O) return;
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += dpart[(size_t)b * O + o];
+    db[o] += (float)s;
+}
+
 // Shapes the kernels take: M = 128 needs N a multiple of 16 in [16, 256];
 // the K (or K-dim O) extent is a whole number of 16-wide MMA slices.
 bool umma_gemm_supported(int K, int O) { return K % 16 == 0 && K <= 192 && O % 16 == 0 && O >= 16 && O <= 64; }
 bool umma_gemm_dx_supported(int O, int K) { return O % 16 == 0 && O <= 64 && K % 16 == 0 && K >= 16 && K <= 256; }
+bool umma_gemm_dw_supported(int K, int O) { return K % 16 == 0 && K <= 256 && O % 16 == 0 && O >= 16 && O <= 64; }
+static size_t dw_smem(int K, int O) { return ((size_t)((K + kRows - 1) / kRows) * kRows + O) * kDwSub * 2; }
+size_t umma_dw_part_floats(int rows, int K, int O) {
+    const size_t nparts = (size_t)((rows + kDwRows - 1) / kDwRows);
+    return nparts * ((K + kRows - 1) / kRows) * kRows * O + nparts * O;
+}
 
 static size_t fwd_smem(int K, int O) { return (size_t)(kRows + O) * K * 2; }
 static size_t dx_smem(int O, int K) { return (size_t)(kRows + K) * O * 2; }
@@ -294,6 +416,28 @@ void umma_gemm_dx(const float* dY, int rows, int O, const float* Wt, int K, floa
         attr = true;
     }
     k_umma_dx<<<(rows + kRows - 1) / kRows, kThreads, dx_smem(O, K), st>>>(dY, rows, O, Wt, K, dX);
+}
+
+void umma_gemm_dw(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* dY,
+                  int O, float* dW, float* db, float* part, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_umma_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dw_smem(256, 64));
+        attr = true;
+    }
+    Parts in{};
+    for (int i = 0; i < parts; ++i) {
+        in.p[i] = p[i];
+        in.idx[i] = idx[i];
+    }
+    const int K = width * parts;
+    const int nparts = (rows + kDwRows - 1) / kDwRows;
+    const int Kp = ((K + kRows - 1) / kRows) * kRows;
+    k_umma_dw<<<nparts, kThreads, dw_smem(K, O), st>>>(in, width, parts, rows, dY, O, part);
+    k_dw_reduce<<<(K * O + 255) / 256, 256, 0, st>>>(part, nparts, Kp, K, O, dW);
+    float* dpart = part + (size_t)nparts * Kp * O;
+    k_db_part<<<nparts, 64, 0, st>>>(dY, rows, O, dpart);
+    k_db_reduce<<<1, 64, 0, st>>>(dpart, nparts, O, db);
 }
 
 int umma_error() {
