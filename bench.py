@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--inner", type=int, default=6, help="inner GMRES steps of the learned preconditioner")
     ap.add_argument("--no-ichol", action="store_true", help="skip the IChol comparison run")
     ap.add_argument("--no-net", action="store_true", help="learned preconditioner without the network correction")
+    ap.add_argument("--replicas", type=int, default=0,
+                    help="batched-replica mode: this many independent suspensions, N log-uniform in [500, 8000], "
+                         "phi uniform in [0.1, 0.5], shear rate uniform in [0, 2], stepped concurrently and then "
+                         "one by one (prints its own JSON line)")
     ap.add_argument("--ichol-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=20.0)
@@ -335,6 +339,81 @@ def run_fsd(args, ws, rank, local):
     return out if rank == 0 else None
 
 
+def run_replicas(args, rank, local):
+    """Independent suspensions of uneven size on their own streams, stepped
+    concurrently by fsd_step_batch, then the same replicas one by one through
+    the same kernels.  Device time: the span from the earliest start event to
+    the latest end event over all replica streams."""
+    import torch
+
+    from fsd_b200.configs import suspension
+    from fsd_b200.core import FSD, step_batch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(1234 + rank)
+    R = args.replicas
+    spec = [(int(np.exp(rng.uniform(np.log(500), np.log(8000)))), float(rng.uniform(0.1, 0.5)),
+             float(rng.uniform(0.0, 2.0))) for _ in range(R)]
+    confs = [suspension(N, phi, 100 + k) for k, (N, phi, _) in enumerate(spec)]
+
+    def make():
+        reps = []
+        for k, ((N, phi, rate), (pos, L)) in enumerate(zip(spec, confs)):
+            stream = torch.cuda.Stream(dev)
+            with torch.cuda.stream(stream):
+                s, _ = make_solver(args, args.precond, N, L, dev, 100 + k)
+                st = [torch.as_tensor(pos, device=dev).view(-1).contiguous(),
+                      torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev),
+                      torch.zeros(3 * N, dtype=torch.int32, device=dev), torch.zeros(6 * N, device=dev),
+                      torch.zeros(11 * N, device=dev)]
+            reps.append((s, st, rate, stream))
+        torch.cuda.synchronize(dev)
+        return reps
+
+    def run(reps, t0, steps, threads):
+        starts = [torch.cuda.Event(enable_timing=True) for _ in reps]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in reps]
+        origin = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        origin.record(torch.cuda.current_stream(dev))
+        torch.cuda.synchronize(dev)
+        for e, r in zip(starts, reps):
+            e.record(r[3])
+        for t in range(t0, t0 + steps):
+            args_ = [s.step_args(t, rate, *st) for s, st, rate, _ in reps]
+            status = step_batch([r[0] for r in reps], args_, nthreads=threads, raise_on_error=False)
+            bad = [x for x in status if x not in (0, 4)]
+            if bad:
+                raise RuntimeError(f"fsd_step_batch status {bad[0]}")
+        for e, r in zip(ends, reps):
+            e.record(r[3])
+        torch.cuda.synchronize(dev)
+        return max(origin.elapsed_time(e) for e in ends) - min(origin.elapsed_time(e) for e in starts)
+
+    reps = make()
+    run(reps, 0, args.warmup, 0)
+    batched_ms = run(reps, args.warmup, args.steps, 0)
+    for s, *_ in reps:
+        s.close()
+    reps = make()
+    run(reps, 0, args.warmup, 1)
+    seq_ms = run(reps, args.warmup, args.steps, 1)
+    for s, *_ in reps:
+        s.close()
+    value = R * args.steps / (batched_ms / 1e3)
+    return {"metric": f"aggregate replica steps/s, {R} independent suspensions (N log-uniform in [500, 8000], "
+                      f"phi uniform in [0.1, 0.5], shear rate uniform in [0, 2])",
+            "value": value, "unit": "replica-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": batched_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: seeded random sequential addition + overlap relaxation",
+            "config": {"workload": "batched replicas", "replicas": R, "precond": args.precond,
+                       "N": [n for n, _, _ in spec], "phi": [round(p, 3) for _, p, _ in spec]},
+            "sequential": {"value": R * args.steps / (seq_ms / 1e3), "unit": "replica-steps/s",
+                           "ms_per_step": seq_ms / args.steps},
+            "speedup_vs_sequential": seq_ms / batched_ms}
+
+
 def cpu_baseline(args, pos, L, gpu_out=None):
     """FP64 NumPy oracle of the same method on host cores: the saddle operator
     (mobility + lubrication, the work of every GMRES iteration) timed at the
@@ -392,6 +471,8 @@ def main():
     ws, rank, local = dist_env()
     if args.impl == "reference":
         out = run_reference(args, ws, rank)
+    elif args.replicas > 0:
+        out = run_replicas(args, rank, local)
     else:
         out = run_fsd(args, ws, rank, local)
     if out is not None:

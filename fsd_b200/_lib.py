@@ -117,6 +117,7 @@ _SIGS = {
     "fsd_rfd_drift": (C.c_int, [H, P, P, C.c_uint, P]),
     "fsd_compute_velocity": (C.c_int, [H, C.POINTER(fsd_step_args)]),
     "fsd_step": (C.c_int, [H, C.POINTER(fsd_step_args)]),
+    "fsd_step_batch": (C.c_int, [P, P, C.c_int, C.c_int, P]),
 }
 EXPORTED = tuple(_SIGS)
 

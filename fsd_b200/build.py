@@ -74,7 +74,7 @@ def build(verbose: bool = False) -> Path:
     if LIB.exists() and all(LIB.stat().st_mtime >= o.stat().st_mtime for o in objs):
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lquadmath"]
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs), "-lquadmath", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed\n{r.stdout}\n{r.stderr}")

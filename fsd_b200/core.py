@@ -281,6 +281,10 @@ class FSD:
         check(lib().fsd_rfd_drift(self._h, _ptr(pos), _ptr(image), timestep, _ptr(out)), "fsd_rfd_drift")
         return out
 
+    def step_args(self, timestep, shear_rate, pos, ori, image, force, velocity, pos_gb=None, noise_ang=None,
+                  b1_mask=None, b2_mask=None):
+        return self._args(timestep, shear_rate, pos, ori, pos_gb, image, force, velocity, noise_ang, b1_mask, b2_mask)
+
     def _args(self, timestep, shear_rate, pos, ori, pos_gb, image, force, velocity, noise_ang, b1_mask, b2_mask):
         a = _lib.fsd_step_args()
         a.timestep = int(timestep)
@@ -304,3 +308,17 @@ class FSD:
         if raise_on_error:
             check(st, "fsd_step")
         return st
+
+
+def step_batch(solvers, args, nthreads: int = 0, raise_on_error: bool = True):
+    """One step of each solver concurrently (fsd_step_batch); args from FSD.step_args.
+    Solvers should live on distinct CUDA streams for their kernels to overlap."""
+    n = len(solvers)
+    hs = (C.c_void_p * n)(*[s._h.value for s in solvers])
+    arr = (_lib.fsd_step_args * n)(*args)
+    st = (C.c_int * n)()
+    first = lib().fsd_step_batch(C.cast(hs, C.c_void_p), C.cast(arr, C.c_void_p), n, int(nthreads),
+                                 C.cast(st, C.c_void_p))
+    if raise_on_error:
+        check(first, "fsd_step_batch")
+    return list(st)

@@ -241,6 +241,7 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
     fsd_handle* h = new fsd_handle();
     h->p = *p;
     h->stream = (cudaStream_t)stream;
+    cudaGetDevice(&h->device);
     h->box = Box{p->Lx, p->Ly, p->Lz, p->xy};
     int st = compute_grid_params(p->xi, p->error, p->max_strain, p->Lx, p->Ly, p->Lz, &h->g);
     if (st != FSD_OK) {

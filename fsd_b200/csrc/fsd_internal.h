@@ -127,6 +127,7 @@ struct fsd_handle {
     fsd_params p;
     fsd::Box box;
     cudaStream_t stream = nullptr;
+    int device = 0;                // CUDA device current at fsd_create
     fsd::GridParams g;
     float self_x = 0, self_y = 0, ewald_cut = 0, ewald_dr = 0;
     int ewald_n = 0;

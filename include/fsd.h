@@ -288,6 +288,14 @@ int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigne
 int fsd_compute_velocity(fsd_handle* h, const fsd_step_args* a);
 /* One full time step (Stokes_StepOne, Stokes.cu:119). */
 int fsd_step(fsd_handle* h, const fsd_step_args* a);
+/* One step of each of n independent suspensions (no counterpart in the
+ * reference, which steps one system per process).  Handle i takes args[i];
+ * the steps run concurrently on nthreads host threads (0: one per handle),
+ * so handles created on distinct streams overlap their kernels on the GPU.
+ * status (optional, n entries) receives each step's fsd_status; the return
+ * value is the first error other than FSD_ERR_LANCZOS_MAXIT, or FSD_OK.
+ * A handle must not appear twice in one batch. */
+int fsd_step_batch(fsd_handle* const* hs, const fsd_step_args* args, int n, int nthreads, int* status);
 
 #ifdef __cplusplus
 }
