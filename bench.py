@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--inner", type=int, default=6, help="inner GMRES steps of the learned preconditioner")
     ap.add_argument("--no-ichol", action="store_true", help="skip the IChol comparison run")
     ap.add_argument("--no-net", action="store_true", help="learned preconditioner without the network correction")
+    ap.add_argument("--no-autotune", action="store_true", help="fixed spreading tiles and FFT batches")
     ap.add_argument("--replicas", type=int, default=0,
                     help="batched-replica mode: this many independent suspensions, N log-uniform in [500, 8000], "
                          "phi uniform in [0.1, 0.5], shear rate uniform in [0, 2], stepped concurrently and then "
@@ -152,7 +153,8 @@ def make_solver(args, precond, N, L, dev, seed):
 
     s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=seed, error=1e-3, solver_tol=1e-4,
             lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=precond, period=0, gmres_max_iter=3000,
-            gmres_restart=200 if precond == "ichol" else 100, learned_inner=args.inner if precond == "learned" else 0)
+            gmres_restart=200 if precond == "ichol" else 100, learned_inner=args.inner if precond == "learned" else 0,
+            autotune=0 if args.no_autotune else 1)
     net = False
     if precond == "learned" and WEIGHTS.exists() and not args.no_net:
         s.learned_set_weights(np.fromfile(WEIGHTS, "<f4"))
@@ -323,6 +325,7 @@ def run_fsd(args, ws, rank, local):
                                f"GMRES 1e-4, {args.precond} preconditioner", "N": N, "phi": phi,
                    "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
                    "learned_inner": args.inner if args.precond == "learned" else None, "learned_network": net,
+                   "autotune": not args.no_autotune,
                    "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
                    "parallelism": f"replicas x{ws}"},
         "e2e": e2e, "gpu_launches": main["launches"], "roofline": roofline,

@@ -39,7 +39,7 @@ class fsd_params(C.Structure):
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
         ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
-        ("learned_inner", C.c_int),
+        ("learned_inner", C.c_int), ("autotune", C.c_int),
     ]
 
 

@@ -123,6 +123,13 @@ struct Workspace {
 };
 }  // namespace fsd
 
+// Launch shapes chosen by the autotuner (0 = built-in defaults).
+struct TuneChoice {
+    int TX = 0, TY = 0, TZ = 0;  // spreading tile
+    int Bxy = 0, Bz = 0;         // FFT lines per block (x/y passes, z pass)
+    bool set = false;
+};
+
 struct fsd_handle {
     fsd_params p;
     fsd::Box box;
@@ -144,5 +151,6 @@ struct fsd_handle {
     int m_lanczos_ff = 2, m_lanczos_nf = 2;
     void* ichol = nullptr;     // preconditioner state (precond.cu)
     void* learned = nullptr;   // block-sparse preconditioner state (learned.cu)
+    TuneChoice tune;
     void* profiler = nullptr;  // region timers (profile.cpp)
 };

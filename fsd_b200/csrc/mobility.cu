@@ -21,6 +21,11 @@
 #include <algorithm>
 #include <cmath>
 
+#include <array>
+#include <functional>
+#include <map>
+#include <mutex>
+
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
 #include "fsd_profile.h"
@@ -266,7 +271,11 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids) {
             Bxy = d;
             break;
         }
-    const int Bz = fft_batch_z(Nx, Ny, Nz);
+    int Bz = fft_batch_z(Nx, Ny, Nz);
+    if (h->tune.set && h->tune.Bxy > 0) {
+        Bxy = h->tune.Bxy;
+        Bz = h->tune.Bz;
+    }
     auto launch = [&](int axis) {
         const FFTPlan& pl = axis == 0 ? px : (axis == 1 ? py : pz);
         const float2* tw = axis == 0 ? twx : (axis == 1 ? twy : twz);
@@ -880,9 +889,15 @@ static void spread(fsd_handle* h, const float4* pos) {
     a.Ny = g.Ny;
     a.Nz = g.Nz;
     a.P = g.P;
-    a.TZ = std::min(8, g.Nz - g.P + 1);
-    a.TY = std::min(8, g.Ny - g.P + 1);
-    a.TX = std::min(4, g.Nx - g.P + 1);
+    if (h->tune.set && h->tune.TX > 0) {
+        a.TX = h->tune.TX;
+        a.TY = h->tune.TY;
+        a.TZ = h->tune.TZ;
+    } else {
+        a.TZ = std::min(8, g.Nz - g.P + 1);
+        a.TY = std::min(8, g.Ny - g.P + 1);
+        a.TX = std::min(4, g.Nx - g.P + 1);
+    }
     a.hx = g.hx;
     a.hy = g.hy;
     a.hz = g.hz;
@@ -942,6 +957,96 @@ void mobility_combine(fsd_handle* h, const float4* pos, const float* genF, float
     k_real_combine<<<(N * kRealGroup + 127) / 128, 128, 0, h->stream>>>(r);
 }
 
+// ---------------------------------------------------------------- autotuner
+// On the first wave-space application with autotune set: time each candidate
+// spreading tile and FFT line batch with CUDA events on the live grid (one
+// warm-up, then the best of three) and keep the fastest.  Choices are cached
+// per process for the grid shape and particle count, so all handles of a
+// process agree.  The grid contents are overwritten; the caller spreads anew.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::array<int, 5>, TuneChoice> g_tune_cache;
+
+float time_ms(fsd_handle* h, const std::function<void()>& f) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    f();
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(a, h->stream);
+        f();
+        cudaEventRecord(b, h->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return best;
+}
+}  // namespace
+
+static int autotune(fsd_handle* h, const float4* pos) {
+    const GridParams& g = h->g;
+    const std::array<int, 5> key{g.Nx, g.Ny, g.Nz, g.P, h->p.N};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            h->tune = it->second;
+            return FSD_OK;
+        }
+    }
+    TuneChoice best;
+    best.set = true;
+    float best_ms = 1e30f;
+    const int tx_c[] = {1, 2, 4, 8}, ty_c[] = {2, 4, 8}, tz_c[] = {4, 8, 16, 32};
+    for (int TX : tx_c)
+        for (int TY : ty_c)
+            for (int TZ : tz_c) {
+                const int T = TX * TY * TZ;
+                if (T < 64 || T > 256 || TX > g.Nx - g.P + 1 || TY > g.Ny - g.P + 1 || TZ > g.Nz - g.P + 1) continue;
+                h->tune = TuneChoice{TX, TY, TZ, 0, 0, true};
+                const float ms = time_ms(h, [&] { spread(h, pos); });
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.TX = TX;
+                    best.TY = TY;
+                    best.TZ = TZ;
+                }
+            }
+    std::vector<int> bxy, bz;
+    for (int d = 8; d <= 32; ++d)
+        if (g.Nz % d == 0) bxy.push_back(d);
+    if (bxy.empty()) bxy.push_back(16);
+    for (int d = 1; d * g.Nz <= 4096; ++d)
+        if ((g.Nx * g.Ny) % d == 0 && sizeof(float2) * ((size_t)g.Nz + 2 * (size_t)d * g.Nz) <= 200 * 1024 &&
+            d * g.Nz >= 256)
+            bz.push_back(d);
+    if (bz.empty()) bz.push_back(fft_batch_z(g.Nx, g.Ny, g.Nz));
+    best_ms = 1e30f;
+    for (int a : bxy)
+        for (int b : bz) {
+            h->tune = TuneChoice{best.TX, best.TY, best.TZ, a, b, true};
+            const float ms = time_ms(h, [&] {
+                fft3d(h, false, 6);
+                fft3d(h, true, 6);
+            });
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.Bxy = a;
+                best.Bz = b;
+            }
+        }
+    h->tune = best;
+    FSD_CHECK_CUDA(cudaGetLastError());
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache.emplace(key, best);
+    return FSD_OK;
+}
+
 int mobility_apply(fsd_handle* h, const float4* pos, const float* genF, float* genU, int parts, const float* saddle_x,
                    bool rebin) {
     const int N = h->p.N;
@@ -953,6 +1058,10 @@ int mobility_apply(fsd_handle* h, const float4* pos, const float* genF, float* g
             ProfRegion pr(h, R_SPREAD);
             if (rebin) {
                 int st = mobility_bin_particles(h, pos);
+                if (st != FSD_OK) return st;
+            }
+            if (h->p.autotune && !h->tune.set) {
+                const int st = autotune(h, pos);
                 if (st != FSD_OK) return st;
             }
             spread(h, pos);

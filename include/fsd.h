@@ -96,6 +96,10 @@ typedef struct fsd_params {
     int learned_inner;           /* FSD_PRECOND_LEARNED: inner GMRES steps on R_FU^pruned + D per application,
                                     right-preconditioned by the learned block-sparse G (4; 0 = apply G once).
                                     With inner steps the outer solve is flexible GMRES. */
+    int autotune;                /* 1: time candidate spreading tiles and FFT line batches on the first mobility
+                                    call and keep the fastest (cached per process and grid shape).  Results then
+                                    depend on the choice through the summation order, so runs in different
+                                    processes may differ in the last bits.  0 (default): fixed shapes. */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */

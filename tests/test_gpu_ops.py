@@ -194,3 +194,17 @@ def test_step_deterministic_and_finite(cuda):
     moved = np.abs(outs[0][0] - pos.ravel()).max()
     assert 0 < moved < 1.0
     s.close()
+
+
+def test_autotuned_shapes_give_the_same_mobility(cuda):
+    """The autotuner only changes launch shapes (spreading tile, FFT batches),
+    so the mobility agrees with the fixed shapes to rounding."""
+    pos, Lc = suspension(2000, 0.3, 8)
+    L = (Lc, Lc, Lc)
+    F = dev(np.random.default_rng(8).standard_normal(11 * 2000))
+    out = []
+    for tune in (0, 1):
+        s, p = solver_for(pos, L, 0.1, autotune=tune)
+        out.append(s.mobility(p, F).cpu().numpy())
+        s.close()
+    assert rel(out[1], out[0]) < 1e-6
