@@ -127,6 +127,7 @@ struct Workspace {
 struct TuneChoice {
     int TX = 0, TY = 0, TZ = 0;  // spreading tile
     int Bxy = 0, Bz = 0;         // FFT lines per block (x/y passes, z pass)
+    int Bg = 0;                  // z-run length of the fused x-pass + Green kernel
     bool set = false;
 };
 

@@ -257,7 +257,7 @@ static int fft_batch_z(int Nx, int Ny, int Nz) {
     return B;
 }
 
-static void fft3d(fsd_handle* h, bool inv, int ngrids) {
+static void fft3d(fsd_handle* h, bool inv, int ngrids, bool skip_x = false) {
     const int Nx = h->g.Nx, Ny = h->g.Ny, Nz = h->g.Nz;
     const FFTPlan px = make_fft_plan(Nx), py = make_fft_plan(Ny), pz = make_fft_plan(Nz);
     const float2* twx = h->w.twiddle;
@@ -297,9 +297,9 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids) {
     if (!inv) {
         launch(2);
         launch(1);
-        launch(0);
+        if (!skip_x) launch(0);
     } else {
-        launch(0);
+        if (!skip_x) launch(0);
         launch(1);
         launch(2);
     }
@@ -401,9 +401,10 @@ __device__ __forceinline__ void green_apply(const float4 tk, const float2* f, fl
     }
 }
 
-// Packed pair p holds spectra (pa[p], pb[p]).
-__constant__ int kPackA[6] = {0, 3, 5, 7, 9, 2};
-__constant__ int kPackB[6] = {1, 4, 6, 8, 10, -1};
+// Packed pair p holds spectra (packA(p), packB(p)); compile-time so that the
+// unrolled loops keep the spectra in registers.
+__host__ __device__ constexpr int packA(int p) { return p == 0 ? 0 : p == 1 ? 3 : p == 2 ? 5 : p == 3 ? 7 : p == 4 ? 9 : 2; }
+__host__ __device__ constexpr int packB(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 6 : p == 3 ? 8 : p == 4 ? 10 : -1; }
 
 // One thread per mirror pair {k, -k}: unpack the 11 spectra of the real grids,
 // apply the Green's function (averaged with the mirror operator where the
@@ -429,8 +430,8 @@ __global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gr
         // A = (C(k) + conj C(m)) / 2 ; B = -i (C(k) - conj C(m)) / 2
         const float2 A = make_float2(0.5f * (ck[p].x + cm[p].x), 0.5f * (ck[p].y - cm[p].y));
         const float2 Bv = make_float2(0.5f * (ck[p].y + cm[p].y), -0.5f * (ck[p].x - cm[p].x));
-        f[kPackA[p]] = A;
-        if (kPackB[p] >= 0) f[kPackB[p]] = Bv;
+        f[packA(p)] = A;
+        if (packB(p) >= 0) f[packB(p)] = Bv;
     }
     if (idx == 0) {
 #pragma unroll
@@ -447,12 +448,168 @@ __global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gr
     }
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-        const float2 A = o[kPackA[p]];
-        const float2 Bv = (kPackB[p] >= 0) ? o[kPackB[p]] : make_float2(0.f, 0.f);
+        const float2 A = o[packA(p)];
+        const float2 Bv = (packB(p) >= 0) ? o[packB(p)] : make_float2(0.f, 0.f);
         // C_out(k) = A + i B ; C_out(m) = conj A + i conj B
         grid[(size_t)p * G + idx] = make_float2(A.x - Bv.y, A.y + Bv.x);
         if (m != idx) grid[(size_t)p * G + m] = make_float2(A.x + Bv.y, -A.y + Bv.x);
     }
+}
+
+// Forward x-pass, Green's function and inverse x-pass in one kernel.  A block
+// holds, for all 6 packed grids, a set of x-lines closed under the mirror map
+// (y, z) -> (-y, -z), so both points of every mirror pair {k, -k} are in
+// shared memory.  Blocks [0, Ny * nzc): line y with the z-run
+// {1 + c B, ..} inside [1, ceil(Nz / 2)) and the mirrored lines (-y, -z);
+// then the planes z = 0 (and z = Nz / 2 for even Nz), pairing y with -y.
+// Every line lies in exactly one block.  The Green step itself is that of
+// k_green (same unpacking, Nyquist averaging and choice of representative).
+__global__ void __launch_bounds__(256) k_fft_x_green(float2* __restrict__ grid, const float4* __restrict__ gridk,
+                                                    int Nx, int Ny, int Nz, int B, int nzc, FFTPlan pl,
+                                                    const float2* __restrict__ tw_global) {
+    extern __shared__ float2 smem[];
+    __shared__ int ly[64], lz[64], lmir[64];
+    __shared__ int s_nl, s_np;  // lines, primary lines (whose points start the pairs)
+    const int n = Nx;
+    float2* tw = smem;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_global[i];
+    const size_t G = (size_t)Nx * Ny * Nz;
+    if (threadIdx.x == 0) {
+        int nl = 0, np = 0;
+        const int bid = blockIdx.x;
+        if (bid < Ny * nzc) {
+            const int y = bid / nzc, c = bid % nzc;
+            const int h = (Nz + 1) / 2;
+            const int z0 = 1 + c * B, z1 = min(h, z0 + B);
+            const int ym = (Ny - y) % Ny;
+            const int cnt = z1 - z0;
+            for (int k = 0; k < cnt; ++k) {
+                ly[k] = y;
+                lz[k] = z0 + k;
+                lmir[k] = cnt + k;
+                ly[cnt + k] = ym;
+                lz[cnt + k] = Nz - (z0 + k);
+                lmir[cnt + k] = k;
+            }
+            nl = 2 * cnt;
+            np = cnt;
+        } else {
+            const int pb = bid - Ny * nzc;
+            const int ny_half = Ny / 2 + 1;  // y in [0, Ny/2]
+            const int zplane = (pb < ny_half) ? 0 : Nz / 2;
+            const int y = (pb < ny_half) ? pb : pb - ny_half;
+            const int ym = (Ny - y) % Ny;
+            ly[0] = y;
+            lz[0] = zplane;
+            if (ym != y) {
+                ly[1] = ym;
+                lz[1] = zplane;
+                lmir[0] = 1;
+                lmir[1] = 0;
+                nl = 2;
+            } else {
+                lmir[0] = 0;
+                nl = 1;
+            }
+            np = 1;
+        }
+        s_nl = nl;
+        s_np = np;
+    }
+    __syncthreads();
+    const int nl = s_nl, np = s_np;
+    const int L6 = 6 * nl;  // lines in shared memory: grid-major
+    float2* a = smem + n;
+    float2* b = a + (size_t)L6 * n;
+    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
+        const int x = i / L6, q = i - x * L6;  // consecutive threads: consecutive lines (z runs)
+        const int g = q / nl, l = q - g * nl;
+        a[(size_t)q * n + x] = grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]];
+    }
+    __syncthreads();
+    float2* res = fft_lines(a, b, L6, pl, tw, false);
+    // Green's function on the mirror pairs.
+    for (int t = threadIdx.x; t < np * n; t += blockDim.x) {
+        const int l = t / n, x = t - l * n;
+        const int lm = lmir[l];
+        const int xm = (Nx - x) % Nx;
+        if (lm == l && xm < x) continue;  // self-mirror line: each pair once
+        size_t idx = ((size_t)x * Ny + ly[l]) * Nz + lz[l];
+        size_t m = ((size_t)xm * Ny + ly[lm]) * Nz + lz[lm];
+        int sl = l, sx = x, ml = lm, mx = xm;
+        if (m < idx) {  // the smaller global index represents the pair, as in k_green
+            const size_t tmp = idx;
+            idx = m;
+            m = tmp;
+            sl = lm;
+            sx = xm;
+            ml = l;
+            mx = x;
+        }
+        float2 ck[6], cm[6], f[11], o[11];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            ck[p] = res[(size_t)(p * nl + sl) * n + sx];
+            cm[p] = res[(size_t)(p * nl + ml) * n + mx];
+        }
+        if (idx == 0) {
+#pragma unroll
+            for (int p = 0; p < 6; ++p) res[(size_t)(p * nl + sl) * n + sx] = make_float2(0.f, 0.f);
+            continue;
+        }
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            const float2 A = make_float2(0.5f * (ck[p].x + cm[p].x), 0.5f * (ck[p].y - cm[p].y));
+            const float2 Bv = make_float2(0.5f * (ck[p].y + cm[p].y), -0.5f * (ck[p].x - cm[p].x));
+            f[packA(p)] = A;
+            if (packB(p) >= 0) f[packB(p)] = Bv;
+        }
+        const int i = (int)(idx / ((size_t)Ny * Nz)), j = (int)((idx / Nz) % Ny), k = (int)(idx % Nz);
+        green_apply(gridk[idx], f, o, 1.0f);
+        if ((2 * i == Nx) || (2 * j == Ny) || (2 * k == Nz)) {
+            float2 o2[11];
+            green_apply(gridk[m], f, o2, -1.0f);
+#pragma unroll
+            for (int c = 0; c < 11; ++c) o[c] = make_float2(0.5f * (o[c].x + o2[c].x), 0.5f * (o[c].y + o2[c].y));
+        }
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            const float2 A = o[packA(p)];
+            const float2 Bv = (packB(p) >= 0) ? o[packB(p)] : make_float2(0.f, 0.f);
+            res[(size_t)(p * nl + sl) * n + sx] = make_float2(A.x - Bv.y, A.y + Bv.x);
+            if (m != idx) res[(size_t)(p * nl + ml) * n + mx] = make_float2(A.x + Bv.y, -A.y + Bv.x);
+        }
+    }
+    __syncthreads();
+    float2* other = (res == a) ? b : a;
+    float2* out = fft_lines(res, other, L6, pl, tw, true);
+    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
+        const int x = i / L6, q = i - x * L6;
+        const int g = q / nl, l = q - g * nl;
+        grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]] = out[(size_t)q * n + x];
+    }
+}
+
+// Launch of the fused x-pass: z-runs of B (4 unless tuned), fewer when the
+// lines would not fit in shared memory.
+static void fft_x_green(fsd_handle* h) {
+    const int Nx = h->g.Nx, Ny = h->g.Ny, Nz = h->g.Nz;
+    const FFTPlan px = make_fft_plan(Nx);
+    const size_t cap = 200 * 1024;
+    int B = (h->tune.set && h->tune.Bg > 0) ? h->tune.Bg : 4;
+    while (B > 1 && sizeof(float2) * ((size_t)Nx + 2 * 12 * (size_t)B * Nx) > cap) --B;
+    const int h2 = (Nz + 1) / 2;
+    const int nzc = (h2 - 1 + B - 1) / B;
+    const int nplanes = (Nz % 2 == 0) ? 2 : 1;
+    const int nblocks = Ny * nzc + nplanes * (Ny / 2 + 1);
+    const size_t shm = sizeof(float2) * ((size_t)Nx + 2 * 12 * (size_t)B * Nx);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_fft_x_green, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+        attr_set = true;
+    }
+    count_launch();
+    k_fft_x_green<<<nblocks, 256, shm, h->stream>>>(h->w.grid, h->w.gridk, Nx, Ny, Nz, B, nzc, px, h->w.twiddle);
 }
 
 // ------------------------------------------------------ particle preparation
@@ -1008,7 +1165,7 @@ static int autotune(fsd_handle* h, const float4* pos) {
             for (int TZ : tz_c) {
                 const int T = TX * TY * TZ;
                 if (T < 64 || T > 256 || TX > g.Nx - g.P + 1 || TY > g.Ny - g.P + 1 || TZ > g.Nz - g.P + 1) continue;
-                h->tune = TuneChoice{TX, TY, TZ, 0, 0, true};
+                h->tune = TuneChoice{TX, TY, TZ, 0, 0, 0, true};
                 const float ms = time_ms(h, [&] { spread(h, pos); });
                 if (ms < best_ms) {
                     best_ms = ms;
@@ -1029,7 +1186,7 @@ static int autotune(fsd_handle* h, const float4* pos) {
     best_ms = 1e30f;
     for (int a : bxy)
         for (int b : bz) {
-            h->tune = TuneChoice{best.TX, best.TY, best.TZ, a, b, true};
+            h->tune = TuneChoice{best.TX, best.TY, best.TZ, a, b, 0, true};
             const float ms = time_ms(h, [&] {
                 fft3d(h, false, 6);
                 fft3d(h, true, 6);
@@ -1040,6 +1197,16 @@ static int autotune(fsd_handle* h, const float4* pos) {
                 best.Bz = b;
             }
         }
+    best_ms = 1e30f;
+    for (int bg : {1, 2, 4, 8}) {
+        h->tune = best;
+        h->tune.Bg = bg;
+        const float ms = time_ms(h, [&] { fft_x_green(h); });
+        if (ms < best_ms) {
+            best_ms = ms;
+            best.Bg = bg;
+        }
+    }
     h->tune = best;
     FSD_CHECK_CUDA(cudaGetLastError());
     std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -1068,17 +1235,15 @@ int mobility_apply(fsd_handle* h, const float4* pos, const float* genF, float* g
         }
         {
             ProfRegion pr(h, R_FFT);
-            fft3d(h, false, 6);
+            fft3d(h, false, 6, true);  // z and y passes
         }
         {
-            ProfRegion pr(h, R_GREEN);
-            const int G = h->g.Nx * h->g.Ny * h->g.Nz;
-            count_launch();
-            k_green<<<(G + 255) / 256, 256, 0, h->stream>>>(h->w.grid, h->w.gridk, h->g.Nx, h->g.Ny, h->g.Nz);
+            ProfRegion pr(h, R_GREEN);  // x pass, Green's function, inverse x pass
+            fft_x_green(h);
         }
         {
             ProfRegion pr(h, R_FFT);
-            fft3d(h, true, 6);
+            fft3d(h, true, 6, true);  // y and z passes
         }
         {
             ProfRegion pr(h, R_CONTRACT);
