@@ -464,7 +464,7 @@ __global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gr
 // then the planes z = 0 (and z = Nz / 2 for even Nz), pairing y with -y.
 // Every line lies in exactly one block.  The Green step itself is that of
 // k_green (same unpacking, Nyquist averaging and choice of representative).
-__global__ void __launch_bounds__(256) k_fft_x_green(float2* __restrict__ grid, const float4* __restrict__ gridk,
+__global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ grid, const float4* __restrict__ gridk,
                                                     int Nx, int Ny, int Nz, int B, int nzc, FFTPlan pl,
                                                     const float2* __restrict__ tw_global) {
     extern __shared__ float2 smem[];
