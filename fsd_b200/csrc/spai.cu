@@ -87,7 +87,7 @@ __device__ __forceinline__ const float* a_block(const unsigned* pn, const unsign
     return nullptr;
 }
 
-__global__ void __launch_bounds__(kSpaiThreads) k_spai_solve(const unsigned* __restrict__ pn,
+__global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* __restrict__ pn,
                                                              const unsigned* __restrict__ plist,
                                                              const float* __restrict__ A,
                                                              const int* __restrict__ sets,
@@ -114,36 +114,43 @@ __global__ void __launch_bounds__(kSpaiThreads) k_spai_solve(const unsigned* __r
         while (a * (a + 1) / 2 > t) --a;
         const int b = t - a * (a + 1) / 2;
         const int sa = S[a], sb = S[b];
-        double blk[36];
-        for (int q = 0; q < 36; ++q) blk[q] = 0.0;
         const unsigned* ra = plist + (size_t)sa * kPrunedCap;
         const unsigned* rb = plist + (size_t)sb * kPrunedCap;
-        unsigned ia = 0, ib = 0;
         const unsigned na = pn[sa], nb = pn[sb];
-        while (ia < na && ib < nb) {
-            const unsigned ka = ra[ia], kb = rb[ib];
-            if (ka == kb) {
-                const float* Pa = A + ((size_t)sa * kPrunedCap + ia) * 36;
-                const float* Pb = A + ((size_t)sb * kPrunedCap + ib) * 36;
-                for (int r = 0; r < 6; ++r)
+        // one row of the 6x6 block at a time keeps the FP64 accumulators in registers
+        for (int r = 0; r < 6; ++r) {
+            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            unsigned ia = 0, ib = 0;
+            while (ia < na && ib < nb) {
+                const unsigned ka = ra[ia], kb = rb[ib];
+                if (ka == kb) {
+                    const float* Pa = A + ((size_t)sa * kPrunedCap + ia) * 36 + r * 6;
+                    const float* Pb = A + ((size_t)sb * kPrunedCap + ib) * 36;
+                    double pa[6];
+#pragma unroll
+                    for (int u = 0; u < 6; ++u) pa[u] = (double)Pa[u];
+#pragma unroll
                     for (int q = 0; q < 6; ++q) {
                         double v = 0.0;
-                        for (int u = 0; u < 6; ++u) v += (double)Pa[r * 6 + u] * (double)Pb[q * 6 + u];
-                        blk[r * 6 + q] += v;
+#pragma unroll
+                        for (int u = 0; u < 6; ++u) v += pa[u] * (double)Pb[q * 6 + u];
+                        acc[q] += v;
                     }
-                ++ia;
-                ++ib;
-            } else if (ka < kb) {
-                ++ia;
-            } else {
-                ++ib;
+                    ++ia;
+                    ++ib;
+                } else if (ka < kb) {
+                    ++ia;
+                } else {
+                    ++ib;
+                }
+            }
+            const int i = 6 * a + r;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const int j = 6 * b + q;
+                if (i >= j) H[tri(i, j)] = acc[q];
             }
         }
-        for (int r = 0; r < 6; ++r)
-            for (int q = 0; q < 6; ++q) {
-                const int i = 6 * a + r, j = 6 * b + q;
-                if (i >= j) H[tri(i, j)] = blk[r * 6 + q];
-            }
     }
     // Right-hand sides: R[6a + r][q] = A_{s_a c}[r][q].
     for (int a = threadIdx.x; a < m; a += blockDim.x) {
@@ -151,7 +158,9 @@ __global__ void __launch_bounds__(kSpaiThreads) k_spai_solve(const unsigned* __r
         for (int k = 0; k < 36; ++k) R[(size_t)(6 * a + k / 6) * 6 + k % 6] = blk ? (double)blk[k] : 0.0;
     }
     __syncthreads();
-    // Right-looking Cholesky in place.
+    // Right-looking Cholesky in place, with the forward substitution L y = R
+    // carried along: row j of R is scaled by the pivot and eliminated from the
+    // rows below in the same parallel update as the trailing matrix.
     __shared__ int bad;
     if (threadIdx.x == 0) bad = 0;
     __syncthreads();
@@ -164,23 +173,19 @@ __global__ void __launch_bounds__(kSpaiThreads) k_spai_solve(const unsigned* __r
         __syncthreads();
         const double piv = H[tri(j, j)];
         for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) H[tri(i, j)] /= piv;
+        if (threadIdx.x < 6) R[(size_t)j * 6 + threadIdx.x] /= piv;
         __syncthreads();
         for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
             const double lij = H[tri(i, j)];
             for (int k = j + 1; k <= i; ++k) H[tri(i, k)] -= lij * H[tri(k, j)];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) R[(size_t)i * 6 + q] -= lij * R[(size_t)j * 6 + q];
         }
         __syncthreads();
     }
-    // Forward and backward substitution, one warp per right-hand side.
+    // Backward substitution L^T x = y, one warp per right-hand side.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int q = warp; q < 6; q += blockDim.x >> 5) {
-        for (int i = 0; i < n; ++i) {
-            double s = 0.0;
-            for (int k = lane; k < i; k += 32) s += H[tri(i, k)] * R[(size_t)k * 6 + q];
-            s = group_sum_d<32>(s);
-            if (lane == 0) R[(size_t)i * 6 + q] = (R[(size_t)i * 6 + q] - s) / H[tri(i, i)];
-            __syncwarp();
-        }
         for (int i = n - 1; i >= 0; --i) {
             double s = 0.0;
             for (int k = i + 1 + lane; k < n; k += 32) s += H[tri(k, i)] * R[(size_t)k * 6 + q];
