@@ -37,7 +37,8 @@ enum fsd_status {
     FSD_OK = 0,
     FSD_ERR_BAD_PARAMS = 1,     /* parameters the reference rejects with exit() (Stokes.cc:140-261) */
     FSD_ERR_CUDA = 2,           /* a CUDA runtime call failed */
-    FSD_ERR_GMRES_MAXIT = 3,    /* GMRES hit its iteration limit (Solvers.cu:121) */
+    FSD_ERR_GMRES_MAXIT = 3,    /* GMRES hit its iteration limit (Solvers.cu:121) or stayed above its
+                                   tolerance after restarting from the true residual */
     FSD_ERR_LANCZOS_MAXIT = 4,  /* Lanczos did not reach its tolerance (Brownian_FarField.cu:787) */
     FSD_ERR_ICHOL = 5,          /* incomplete Cholesky failed even after relaxation (Precondition.cu:1246) */
     FSD_ERR_NLIST_OVERFLOW = 6, /* more neighbours than the list capacity even after growing it */

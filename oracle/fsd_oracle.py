@@ -559,15 +559,54 @@ class Problem:
         return A
 
     def solve(self, rhs, tol=1e-12):
-        """Converged saddle solution (dense LU for small N, else FP64 GMRES)."""
+        """Converged saddle solution: dense LU for small N, else FP64 GMRES with the
+        block preconditioner of Saddle.cu:171-264 built on the exact (R_FU^pruned + D)^-1
+        (sparse LU), iterated until the true residual is below tol."""
         if self.N <= 150:
             return np.linalg.solve(self.dense_saddle(), rhs)
-        from scipy.sparse.linalg import LinearOperator, gmres
-        n = 17 * self.N
-        A = LinearOperator((n, n), matvec=self.saddle_multiply, dtype=np.float64)
-        x, info = gmres(A, rhs, rtol=tol, restart=200, maxiter=2000)
-        assert info == 0
+        import scipy.sparse.linalg as sla
+        N = self.N
+        n = 17 * N
+        lu = sla.splu(pruned_rfu_sparse(self.pos, self.L, self.xy, self.tdist, self.tvals, rows=self.rows,
+                                        rp=self.rp).tocsc())
+
+        def pc(b):
+            y = lu.solve(b[: 6 * N] - b[11 * N:])
+            x = b.copy()
+            x[: 6 * N] = b[: 6 * N] - y
+            x[11 * N:] = y
+            return x
+
+        A = sla.LinearOperator((n, n), matvec=self.saddle_multiply, dtype=np.float64)
+        M = sla.LinearOperator((n, n), matvec=pc, dtype=np.float64)
+        x = np.zeros(n)
+        bn = np.linalg.norm(rhs)
+        for _ in range(5):
+            r = rhs - self.saddle_multiply(x)
+            if np.linalg.norm(r) <= tol * bn:
+                break
+            dx, info = sla.gmres(A, r, M=M, rtol=tol * bn / max(np.linalg.norm(r), 1e-300), restart=200,
+                                 maxiter=10)
+            x = x + dx
+        assert np.linalg.norm(rhs - self.saddle_multiply(x)) <= 10 * tol * bn
         return x
+
+    def velocity(self, shear_rate, ndsr=0.1, k_n=1e4, kappa=20.0, beta=0.0, epsq=1e-5, tol=1e-10):
+        """Integrator_ComputeVelocity (Integrator.cu:744-938) at kT = 0 without active
+        terms: right-hand side from the interparticle force (Helper_Stokes.cu:65-172),
+        the imposed strain (Helper_Integrator.cu:114-158) and R_FE:E
+        (Lubrication.cu:350-608); the saddle solution; then U (6N) and the stresslet
+        S = S^ff - R_SU U + R_SE:E (Integrator.cu:881-932, 5N).  Returns U, S, F."""
+        N = self.N
+        F = pair_force(self.pos, self.L, self.xy, self.rows, ndsr=ndsr, k_n=k_n, kappa=kappa, beta=beta, epsq=epsq)
+        rhs = strain_rhs(shear_rate, N)
+        rhs[11 * N:] -= F
+        rhs[11 * N:] += rfe(self.pos, shear_rate, self.L, self.xy, self.rows, self.tdist, self.tvals, rlub=self.rlub)
+        x = self.solve(rhs, tol)
+        U = x[11 * N:]
+        S = x[6 * N:11 * N] + rsu(self.pos, U, self.L, self.xy, self.rows, self.tdist, self.tvals, rlub=self.rlub) \
+            + rse(self.pos, shear_rate, self.L, self.xy, self.rows, self.tdist, self.tvals)
+        return U, S, F
 
 
 def rcm(rows):
@@ -819,15 +858,22 @@ def saddle_precond(b, G, N):
 def pair_force(pos, L, xy, rows, ndsr=0.1, k_n=1e4, kappa=20.0, beta=0.0, epsq=1e-5, T_ext=0.0):
     """Repulsion + van der Waals + collision force and z torque (Stokes_SetForce_manually_kernel,
     Helper_Stokes.cu:65-172)."""
-    pos = xyz(pos)
-    N = len(pos)
+    p32 = np.asarray(pos, F32)[:, :3]
+    N = len(p32)
     i, j = pair_arrays(rows)
-    R = min_image(pos[j] - pos[i], L, xy)
-    dist = np.sqrt(np.einsum("ij,ij->i", R, R))
-    rcol = 2.0 + np.sqrt(epsq)
+    # single-precision separation and distance, as the kernel: near contact the
+    # collision term k_n |gap| resolves the gap only to float32
+    R32 = min_image32(p32[j] - p32[i], L, xy)
+    d2 = R32[:, 0] * R32[:, 0] + R32[:, 1] * R32[:, 1] + R32[:, 2] * R32[:, 2]
+    R = R32.astype(np.float64)
+    d32 = np.sqrt(d2)
+    dist = d32.astype(np.float64)
+    # contact radius and gap in single precision as the kernel (2 + sqrt(epsq),
+    # dist - rcol): at k_n = 1e4 the rounding of rcol is visible in the force
+    rcol32 = F32(2.0) + F32(np.sqrt(F32(epsq)))
     F0 = 1.0 / ndsr
     H = F0 * beta
-    gap = dist - rcol
+    gap = (d32 - rcol32).astype(np.float64)
     mag = np.zeros_like(dist)
     m1 = (gap >= 0) & (dist <= 2.0 + 10.0 / kappa)
     mag[m1] = H / (12.0 * (gap[m1] ** 2 + epsq)) - F0 * np.exp(-kappa * gap[m1])
