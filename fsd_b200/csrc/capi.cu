@@ -90,11 +90,13 @@ static int allocate(fsd_handle* h) {
     FSD_TRY(dalloc(&w.sy, n17));
     FSD_TRY(dalloc(&w.sz, n17));
     const int m = std::min(h->p.gmres_restart, kMaxRestart);
-    FSD_TRY(dalloc(&w.V, (size_t)(m + 1) * n17));
+    FSD_TRY(dalloc(&w.V, (size_t)(m + 1) * krylov_ld(N)));
     if (h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0)  // flexible GMRES keeps M^-1 v_j
-        FSD_TRY(dalloc(&w.Z, (size_t)m * n17));
-    FSD_TRY(dalloc(&w.dred, (size_t)(kMaxRestart + 2) * 512));
-    FSD_TRY(dalloc(&w.hcol, kMaxRestart + 2));
+        FSD_TRY(dalloc(&w.Z, (size_t)m * krylov_ld(N)));
+    FSD_TRY(dalloc(&w.dred, (size_t)2 * (kMaxRestart + 2) * 512));
+    FSD_TRY(dalloc(&w.hcol, 2 * (kMaxRestart + 2)));
+    FSD_TRY(dalloc(&w.ticket, 1));
+    FSD_CHECK_CUDA(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned), h->stream));
     FSD_TRY(dalloc(&w.hcol2, kMaxRestart + 2));
     FSD_TRY(gmres_alloc(h));
     FSD_TRY(dalloc(&w.pc_t, 6 * (size_t)N));
@@ -123,7 +125,7 @@ static void release(fsd_handle* h) {
     void* dev[] = {w.nneigh, w.nlist, w.nl_overflow, w.scan_scratch, w.part_cell, w.cell_count, w.cell_start,
                    w.cell_fill, w.cell_parts, w.part_origin_key, w.part_origin, w.bin_count, w.bin_start, w.bin_fill,
                    w.bin_parts, w.grid, w.gridk, w.twiddle, w.f4, w.c4, w.uwave, w.sx, w.sy, w.sz, w.V, w.Z, w.dred,
-                   w.hcol, w.hcol2, w.gmres_state, w.pc_t, w.pc_y, w.rhs, w.sol, w.rfd_rhs, w.rfd_sol, w.psi,
+                   w.hcol, w.hcol2, w.ticket, w.gmres_state, w.pc_t, w.pc_y, w.rhs, w.sol, w.rfd_rhs, w.rfd_sol, w.psi,
                    w.pos_prime, w.vel, w.force, w.lanczos_V, w.lz_a, w.lz_b, w.lz_c, w.lz_dot, h->d_ewald,
                    h->d_res_dist, h->d_res_vals};
     for (void* p : dev)

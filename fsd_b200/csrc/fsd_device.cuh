@@ -103,4 +103,36 @@ __device__ __forceinline__ double group_sum_d(double v) {
     return v;
 }
 
+// Last-block reduction: every block has written its partials, fenced; the
+// block that takes the last ticket sees all of them and resets the ticket.
+__device__ __forceinline__ bool last_block(unsigned* ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Sum of part[0:n] in a fixed order by one warp (same result every run).
+__device__ __forceinline__ double warp_sum_parts(const double* part, int n) {
+    double s = 0.0;
+    for (int b = threadIdx.x & 31; b < n; b += 32) s += __ldcg(part + b);
+    return group_sum_d<32>(s);
+}
+
+// Block sum of v written to part[blockIdx.x].
+__device__ __forceinline__ void block_partial(double v, double* part) {
+    __shared__ double sh[32];
+    v = group_sum_d<32>(v);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        t = group_sum_d<32>(t);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+
 }  // namespace fsd

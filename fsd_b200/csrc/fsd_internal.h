@@ -97,7 +97,8 @@ struct Workspace {
     float* V = nullptr;            // (restart + 1) x 17N basis
     float* Z = nullptr;            // restart x 17N preconditioned basis (flexible GMRES only)
     double* dred = nullptr;        // per-block partial sums
-    double* hcol = nullptr;        // Hessenberg column
+    double* hcol = nullptr;        // Hessenberg column, or the 2(j+1) dots of a delayed Gram-Schmidt pass
+    unsigned* ticket = nullptr;    // last-block counter of the Gram-Schmidt update, zero between launches
     double* hcol2 = nullptr;       // re-orthogonalisation column
     void* gmres_state = nullptr;   // device GMRES state
     void* gmres_host = nullptr;    // pinned host mirror

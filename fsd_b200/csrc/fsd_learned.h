@@ -18,13 +18,12 @@ struct LearnedState {
     const float* a_blocks = nullptr;
     // inner GMRES work space
     int inner_cap = -1;
-    float* t = nullptr;      // 6N right-hand side of the inner solve
-    float* w = nullptr;      // 6N
-    float* y = nullptr;      // 6N inner solution
-    float* Vi = nullptr;     // (kMaxInner + 1) x 6N
-    float* Zi = nullptr;     // kMaxInner x 6N
-    double* part = nullptr;  // (kMaxInner + 2) x kInnerBlocks partial sums
-    double* H = nullptr;     // (kMaxInner + 1) x kMaxInner Hessenberg, column-major by step, plus beta
+    float* Vi = nullptr;      // (kMaxInner + 1) x 6N basis, unnormalised
+    float* Zi = nullptr;      // kMaxInner x 6N, Z_j = G V_j / |V_j|
+    double* part = nullptr;   // (kMaxInner + 1) x blocks partial sums
+    double* H = nullptr;      // (kMaxInner + 1) x kMaxInner Hessenberg, column-major by step, beta, y
+    double* nrm = nullptr;    // kMaxInner + 1 basis norms
+    unsigned* ticket = nullptr;  // last-block counter, zero between kernels
     void* mp = nullptr;      // message-passing network state (mpnn.cu)
     // two-hop sparse approximate inverse (spai.cu)
     int* sp_sets = nullptr;          // N x kSpaiCap members, particle itself first
@@ -35,11 +34,12 @@ struct LearnedState {
     unsigned* sp_cnt = nullptr;      // bucket counts, truncated sets, failed rows
     unsigned* sp_host = nullptr;
     int sp_truncated = 0;
-    // inner solve replayed as a CUDA graph on fixed 17N input/output buffers
-    float* tb = nullptr;
-    float* tx = nullptr;
+    // inner solve replayed as a CUDA graph; its first and last kernel nodes
+    // are re-pointed at each application's vectors
     cudaStream_t cap_stream = nullptr;
+    cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    cudaGraphNode_t node_rhs = nullptr, node_post = nullptr;
     const void* gkey[8] = {};
     int gkey_k = -1;
     int captures = 0;

@@ -7,8 +7,12 @@ namespace fsd {
 
 constexpr int kMaxRestart = 400;
 constexpr int kMaxInner = 16;    // inner GMRES steps of the learned preconditioner
-constexpr int kPrunedCap = 32;
-constexpr int kSpaiCap = 32;     // members of a two-hop approximate-inverse set  // pruned (r < rp) neighbours per particle, self included
+constexpr int kPrunedCap = 32;   // pruned (r < rp) neighbours per particle, self included
+constexpr int kSpaiCap = 32;     // members of a two-hop approximate-inverse set
+
+// Leading dimension of the Krylov bases V and Z: 17N rounded up to 32 floats,
+// so that every basis vector starts on a 128-byte boundary.
+inline size_t krylov_ld(int N) { return (17 * (size_t)N + 31) & ~(size_t)31; }
 
 int saddle_multiply(fsd_handle* h, const float4* pos, const float* x, float* b, bool rebin);
 int precond_apply(fsd_handle* h, const float* b, float* x);

@@ -9,6 +9,7 @@
 // fused into the SpMV kernel, exactly as in the IC(0) solve kernels.
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -29,14 +30,14 @@ void learned_free(fsd_handle* h) {
     LearnedState* s = (LearnedState*)h->learned;
     if (!s) return;
     mpnn_free(h);
-    void* ptrs[] = {s->g_rowptr, s->g_col, s->g_val, s->t, s->w, s->y, s->Vi, s->Zi, s->part, s->H,
-                    s->sp_sets, s->sp_size, s->sp_rowptr, s->sp_scan, s->sp_bucket, s->sp_cnt};
+    void* ptrs[] = {s->g_rowptr, s->g_col,   s->g_val,     s->Vi,        s->Zi,        s->part,   s->H,
+                    s->nrm,      s->ticket,  s->sp_sets,   s->sp_size,   s->sp_rowptr, s->sp_scan, s->sp_bucket,
+                    s->sp_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->sp_host) cudaFreeHost(s->sp_host);
-    if (s->tb) cudaFree(s->tb);
-    if (s->tx) cudaFree(s->tx);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
     delete s;
     h->learned = nullptr;
@@ -124,178 +125,121 @@ __global__ void __launch_bounds__(256) k_pc_bsr(const int* __restrict__ rowptr, 
 }
 
 // ----------------------------------------------------------- inner solve
-// y = sum_s A_is x_s over the pruned list (self included), 8 lanes per row.
-__global__ void __launch_bounds__(256) k_pruned_spmv(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist,
-                                                     const float* __restrict__ A, const float* __restrict__ x,
-                                                     float* __restrict__ y, int N) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gid >> 3;
-    const int r = threadIdx.x & 7;
-    if (i >= N) return;
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
-    float acc = 0.f;
-    const unsigned n = pn[i];
-    for (unsigned s = 0; s < n; ++s) {
-        const size_t e = (size_t)i * kPrunedCap + s;
-        const unsigned j = plist[e];
-        const float xj = (r < 6) ? x[6 * j + r] : 0.f;
-        const float* Ae = A + e * 36 + (r < 6 ? r : 0) * 6;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const float xc = __shfl_sync(gmask, xj, c, 8);
-            if (r < 6) acc += Ae[c] * xc;
-        }
-    }
-    if (r < 6) y[6 * i + r] = acc;
+// The blocks stay fp32: the lubrication blocks are ill-conditioned (gaps down
+// to 1e-3), and fp16 copies, even scaled per block, raised the outer
+// iteration counts by a quarter.
+
+// Row r of a 6x6 fp32 block times x, summed over a group of eight lanes
+// (lane c < 6 holds x_c in xj).
+__device__ __forceinline__ float block_row(const float* blk, int rr, float xj, unsigned gmask) {
+    const float2* g = reinterpret_cast<const float2*>(blk + rr * 6);
+    const float2 g01 = g[0], g23 = g[1], g45 = g[2];
+    float sum = g01.x * __shfl_sync(gmask, xj, 0, 8);
+    sum = fmaf(g01.y, __shfl_sync(gmask, xj, 1, 8), sum);
+    sum = fmaf(g23.x, __shfl_sync(gmask, xj, 2, 8), sum);
+    sum = fmaf(g23.y, __shfl_sync(gmask, xj, 3, 8), sum);
+    sum = fmaf(g45.x, __shfl_sync(gmask, xj, 4, 8), sum);
+    sum = fmaf(g45.y, __shfl_sync(gmask, xj, 5, 8), sum);
+    return sum;
 }
 
-// y = G x in block CSR.
-__global__ void __launch_bounds__(256) k_bsr_spmv(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                  const float* __restrict__ G, const float* __restrict__ x,
-                                                  float* __restrict__ y, int N) {
+// z = G (u / |u|) in block CSR, |u| read from the device (zero gives zero).
+// Eight lanes per particle row; lane r < 6 owns output component r.
+__global__ void __launch_bounds__(256) k_bsr_spmv_n(const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                    const float* __restrict__ G, const float* __restrict__ u,
+                                                    const double* __restrict__ unrm, float* __restrict__ z, int N) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = gid >> 3;
     const int r = threadIdx.x & 7;
-    if (i >= N) return;
+    if (i >= N) return;  // whole groups of eight leave together
     const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const int rr = r < 6 ? r : 0;
     float acc = 0.f;
-    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+    const int e1 = rowptr[i + 1];
+    for (int e = rowptr[i]; e < e1; ++e) {
         const int j = col[e];
-        const float xj = (r < 6) ? x[6 * j + r] : 0.f;
-        const float* Ge = G + (size_t)e * 36 + (r < 6 ? r : 0) * 6;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-            const float xc = __shfl_sync(gmask, xj, c, 8);
-            if (r < 6) acc += Ge[c] * xc;
-        }
+        const float xj = (r < 6) ? u[6 * j + r] : 0.f;
+        acc += block_row(G + (size_t)e * 36, rr, xj, gmask);
     }
-    if (r < 6) y[6 * i + r] = acc;
+    const double nv = *unrm;
+    const float f = nv > 0.0 ? (float)(1.0 / nv) : 0.f;
+    if (r < 6) z[6 * i + r] = f * acc;
 }
 
 constexpr int kInnerBlocks = 296;
 constexpr int kInnerThreads = 256;
 
-// t = b[0:6N] - b[11N:17N]; part[b] = partial ||t||^2.
-__global__ void __launch_bounds__(kInnerThreads) k_inner_rhs(const float* __restrict__ b, float* __restrict__ t,
-                                                             int N, double* part) {
-    __shared__ double sh[32];
+// u0 = b[0:6N] - b[11N:17N]; |u0| goes to nrm[0] and to H's beta slot.
+__global__ void __launch_bounds__(kInnerThreads) k_inner_rhs(const float* __restrict__ b, float* __restrict__ u0,
+                                                             int N, double* part, unsigned* ticket, double* H,
+                                                             double* nrm) {
     double s = 0.0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 6 * N; k += gridDim.x * blockDim.x) {
         const float v = b[k] - b[11 * (size_t)N + k];
-        t[k] = v;
+        u0[k] = v;
         s += (double)v * v;
     }
-    s = group_sum_d<32>(s);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
+    block_partial(s, part);
+    if (!last_block(ticket)) return;
     if (threadIdx.x < 32) {
-        double v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-        v = group_sum_d<32>(v);
-        if (threadIdx.x == 0) part[blockIdx.x] = v;
+        const double t = sqrt(warp_sum_parts(part, gridDim.x));
+        if (threadIdx.x == 0) {
+            nrm[0] = t;
+            H[(kMaxInner + 1) * kMaxInner] = t;
+            *ticket = 0;
+        }
     }
 }
 
-// part[i * nb + block] = V_i . w over the block's grid-stride share, i < nv.
-__global__ void __launch_bounds__(kInnerThreads) k_inner_dots(const float* __restrict__ V, size_t ld, int nv,
-                                                              const float* __restrict__ w, size_t n, double* part) {
-    __shared__ double sh[kMaxInner + 1][kInnerThreads / 32];
-    double acc[kMaxInner + 1];
-#pragma unroll
-    for (int i = 0; i <= kMaxInner; ++i) acc[i] = 0.0;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        const double wk = w[k];
-#pragma unroll
-        for (int i = 0; i <= kMaxInner; ++i)
-            if (i < nv) acc[i] += (double)V[(size_t)i * ld + k] * wk;
+// w = A z over the pruned list (self included), written to the basis slot
+// U_nv, fused with the dots H[j][q] = (U_q . w) / |U_q| for q < nv = j + 1.
+__global__ void __launch_bounds__(256) k_pruned_spmv_dots(const unsigned* __restrict__ pn,
+                                                          const unsigned* __restrict__ plist,
+                                                          const float* __restrict__ A, const float* __restrict__ z, float* U, size_t ld, int nv,
+                                                          const double* __restrict__ nrm, double* part,
+                                                          unsigned* ticket, double* H, int j, int N) {
+    __shared__ double sh[kMaxInner + 1][8];
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = gid >> 3;
+    const int r = threadIdx.x & 7;
+    const bool act = i < N && r < 6;
+    float acc = 0.f;
+    if (i < N) {  // whole groups of eight; every thread reaches the reductions below
+        const unsigned gmask = 0xffu << (threadIdx.x & 24);
+        const int rr = r < 6 ? r : 0;
+        const unsigned n = pn[i];
+        for (unsigned q = 0; q < n; ++q) {
+            const size_t e = (size_t)i * kPrunedCap + q;
+            const unsigned jj = plist[e];
+            const float xj = (r < 6) ? z[6 * jj + r] : 0.f;
+            acc += block_row(A + e * 36, rr, xj, gmask);
+        }
+        if (act) U[(size_t)nv * ld + 6 * i + r] = acc;
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int i = 0; i <= kMaxInner; ++i) {
-        if (i >= nv) break;
-        const double v = group_sum_d<32>(acc[i]);
-        if (lane == 0) sh[i][wid] = v;
+    for (int q = 0; q < nv; ++q) {
+        double d = act ? (double)U[(size_t)q * ld + 6 * i + r] * (double)acc : 0.0;
+        d = group_sum_d<32>(d);
+        if (lane == 0) sh[q][wid] = d;
     }
     __syncthreads();
     if (threadIdx.x < nv) {
         double v = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += sh[threadIdx.x][q];
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[threadIdx.x][w];
         part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
     }
-}
-
-// H[col j][i] = sum_b part[i * nb + b] for i < nv (one warp per i).  With
-// j < 0 the single sum is the squared norm of the right-hand side, kept in
-// H's beta slot.
-__global__ void k_inner_finish(const double* part, int nb, int nv, double* H, int j) {
-    const int i = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (i >= nv) return;
-    double s = 0.0;
-    for (int b = lane; b < nb; b += 32) s += part[(size_t)i * nb + b];
-    s = group_sum_d<32>(s);
-    if (lane == 0) {
-        if (j < 0) H[(kMaxInner + 1) * kMaxInner] = s;
-        else H[(size_t)j * (kMaxInner + 1) + i] = s;
+    if (!last_block(ticket)) return;
+    for (int q = wid; q < nv; q += blockDim.x >> 5) {
+        const double t = warp_sum_parts(part + (size_t)q * gridDim.x, gridDim.x);
+        if (lane == 0) H[(size_t)j * (kMaxInner + 1) + q] = nrm[q] > 0.0 ? t / nrm[q] : 0.0;
     }
-}
-
-// w -= sum_{i<nv} H[j][i] V_i, and part[b] = partial ||w||^2.
-__global__ void __launch_bounds__(kInnerThreads) k_inner_orth(const float* __restrict__ V, size_t ld, int nv,
-                                                              const double* __restrict__ H, int j, float* w, size_t n,
-                                                              double* part) {
-    __shared__ float hc[kMaxInner + 1];
-    __shared__ double sh[32];
-    if (threadIdx.x < nv) hc[threadIdx.x] = (float)H[(size_t)j * (kMaxInner + 1) + threadIdx.x];
-    __syncthreads();
-    double s = 0.0;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        float acc = w[k];
-        for (int i = 0; i < nv; ++i) acc -= hc[i] * V[(size_t)i * ld + k];
-        w[k] = acc;
-        s += (double)acc * acc;
-    }
-    s = group_sum_d<32>(s);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
-        v = group_sum_d<32>(v);
-        if (threadIdx.x == 0) part[blockIdx.x] = v;
-    }
-}
-
-// dst = src / sqrt(nrm2) with nrm2 = sum of part (every block re-reduces the
-// few partials, so no extra launch is needed); the norm is written to
-// H[j][j+1] (j >= 0) or to the beta slot (j < 0).  A zero norm gives zero.
-__global__ void __launch_bounds__(kInnerThreads) k_inner_scale(const float* __restrict__ src, float* __restrict__ dst,
-                                                               size_t n, const double* __restrict__ part, int nb,
-                                                               double* H, int j) {
-    __shared__ double sh[32];
-    __shared__ double nrm;
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += part[b];
-    s = group_sum_d<32>(s);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double v = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += sh[q];
-        nrm = sqrt(v);
-        if (blockIdx.x == 0) {
-            if (j < 0) H[(kMaxInner + 1) * kMaxInner] = nrm;
-            else H[(size_t)j * (kMaxInner + 1) + j + 1] = nrm;
-        }
-    }
-    __syncthreads();
-    const float f = nrm > 0.0 ? (float)(1.0 / nrm) : 0.0f;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-        dst[k] = f * src[k];
+    if (threadIdx.x == 0) *ticket = 0;
 }
 
 // Least squares min || beta e1 - H y || by Givens rotations in FP64 (one
 // thread; k <= kMaxInner).  Columns after a breakdown (zero subdiagonal or
-// zero pivot) are dropped.  y is written to H's last column block.
-__global__ void k_inner_lsq(double* H, int k) {
-    if (threadIdx.x != 0) return;
+// zero pivot) are dropped.  y is written after H's beta slot.
+__device__ void inner_lsq(double* H, int k) {
     double R[kMaxInner + 1][kMaxInner];
     double g[kMaxInner + 1];
     const double beta = H[(kMaxInner + 1) * kMaxInner];
@@ -335,14 +279,47 @@ __global__ void k_inner_lsq(double* H, int k) {
     for (int c = 0; c < kMaxInner; ++c) out[c] = (c < used) ? y[c] : 0.0;
 }
 
-// x = post(b, sum_j c_j Z_j): x[0:6N] = b - y, x[6N:11N] = b, x[11N:] = y.
+// U_nv -= sum_{q<nv} (H[j][q] / |U_q|) U_q; |U_nv| goes to nrm[nv] and to
+// H[j][nv].  With lsq_k > 0 the last block then solves the k-step least
+// squares problem.
+__global__ void __launch_bounds__(kInnerThreads) k_inner_orth(float* U, size_t ld, int nv, double* H,
+                                                              double* nrm, int j, size_t n, double* part,
+                                                              unsigned* ticket, int lsq_k) {
+    __shared__ float hc[kMaxInner + 1];
+    if (threadIdx.x < nv)
+        hc[threadIdx.x] =
+            nrm[threadIdx.x] > 0.0 ? (float)(H[(size_t)j * (kMaxInner + 1) + threadIdx.x] / nrm[threadIdx.x]) : 0.f;
+    __syncthreads();
+    float* w = U + (size_t)nv * ld;
+    double s = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        float acc = w[k];
+        for (int q = 0; q < nv; ++q) acc = fmaf(-hc[q], U[(size_t)q * ld + k], acc);
+        w[k] = acc;
+        s += (double)acc * acc;
+    }
+    block_partial(s, part);
+    if (!last_block(ticket)) return;
+    if (threadIdx.x < 32) {
+        const double t = sqrt(warp_sum_parts(part, gridDim.x));
+        if (threadIdx.x == 0) {
+            nrm[nv] = t;
+            H[(size_t)j * (kMaxInner + 1) + nv] = t;
+            if (lsq_k > 0) inner_lsq(H, lsq_k);
+            *ticket = 0;
+        }
+    }
+}
+
+// x = post(b, sum_i c_i Z_i): x[0:6N] = b - y, x[6N:11N] = b, x[11N:] = y.
 __global__ void k_inner_post(const float* __restrict__ Z, size_t ld, int k, const double* __restrict__ c,
-                             const float* __restrict__ b, float* __restrict__ x, int N) {
+                             const float* b, float* x, int N) {
     const int kk = blockIdx.x * blockDim.x + threadIdx.x;
     if (kk < 6 * N) {
         float acc = 0.f;
         for (int i = 0; i < k; ++i) acc += (float)c[i] * Z[(size_t)i * ld + kk];
-        x[kk] = b[kk] - acc;
+        const float bk = b[kk];
+        x[kk] = bk - acc;
         x[11 * (size_t)N + kk] = acc;
     } else if (kk < 11 * N) {
         x[kk] = b[kk];
@@ -352,16 +329,16 @@ __global__ void k_inner_post(const float* __restrict__ Z, size_t ld, int k, cons
 static int inner_alloc(fsd_handle* h) {
     LearnedState* s = learned(h);
     if (s->inner_cap >= 0) return FSD_OK;
-    const size_t n6 = 6 * (size_t)h->p.N;
-    FSD_CHECK_CUDA(cudaMalloc(&s->t, sizeof(float) * n6));
-    FSD_CHECK_CUDA(cudaMalloc(&s->w, sizeof(float) * n6));
-    FSD_CHECK_CUDA(cudaMalloc(&s->y, sizeof(float) * n6));
+    const size_t N = h->p.N;
+    const size_t n6 = 6 * N;
     FSD_CHECK_CUDA(cudaMalloc(&s->Vi, sizeof(float) * n6 * (kMaxInner + 1)));
     FSD_CHECK_CUDA(cudaMalloc(&s->Zi, sizeof(float) * n6 * kMaxInner));
-    FSD_CHECK_CUDA(cudaMalloc(&s->part, sizeof(double) * (kMaxInner + 2) * kInnerBlocks));
+    const size_t nb = std::max<size_t>(kInnerBlocks, (8 * N + 255) / 256);
+    FSD_CHECK_CUDA(cudaMalloc(&s->part, sizeof(double) * (kMaxInner + 1) * nb));
     FSD_CHECK_CUDA(cudaMalloc(&s->H, sizeof(double) * ((kMaxInner + 1) * kMaxInner + 1 + kMaxInner)));
-    FSD_CHECK_CUDA(cudaMalloc(&s->tb, sizeof(float) * 17 * (size_t)h->p.N));
-    FSD_CHECK_CUDA(cudaMalloc(&s->tx, sizeof(float) * 17 * (size_t)h->p.N));
+    FSD_CHECK_CUDA(cudaMalloc(&s->nrm, sizeof(double) * (kMaxInner + 1)));
+    FSD_CHECK_CUDA(cudaMalloc(&s->ticket, sizeof(unsigned)));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), h->stream));
     s->inner_cap = kMaxInner;
     return FSD_OK;
 }
@@ -370,57 +347,80 @@ bool precond_is_flexible(const fsd_handle* h) {
     return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0;
 }
 
-// Kernels of one inner solve, enqueued on st (also used for graph capture).
+// Kernels of one inner solve on the right-hand side b into x, enqueued on st
+// (for graph capture).  Basis U_j is kept unnormalised with |U_j| in nrm[j];
+// each kernel applies the 1/|U_j| factors it needs.
 static int inner_enqueue(fsd_handle* h, const float* b, float* x, cudaStream_t st) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
     const int k = h->p.learned_inner;
     const size_t n6 = 6 * (size_t)N;
     const int rows = (8 * N + 255) / 256;
-    const int nb = kInnerBlocks;
-    k_inner_rhs<<<nb, kInnerThreads, 0, st>>>(b, s->t, N, s->part);
-    k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->t, s->Vi, n6, s->part, nb, s->H, -1);
+    k_inner_rhs<<<kInnerBlocks, kInnerThreads, 0, st>>>(b, s->Vi, N, s->part, s->ticket, s->H, s->nrm);
     for (int j = 0; j < k; ++j) {
-        float* vj = s->Vi + (size_t)j * n6;
+        float* uj = s->Vi + (size_t)j * n6;
         float* zj = s->Zi + (size_t)j * n6;
-        k_bsr_spmv<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, vj, zj, N);
-        k_pruned_spmv<<<rows, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, zj, s->w, N);
-        k_inner_dots<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->w, n6, s->part);
-        k_inner_finish<<<1, 32 * (j + 1), 0, st>>>(s->part, nb, j + 1, s->H, j);
-        k_inner_orth<<<nb, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->H, j, s->w, n6, s->part);
-        k_inner_scale<<<nb, kInnerThreads, 0, st>>>(s->w, s->Vi + (size_t)(j + 1) * n6, n6, s->part, nb, s->H, j);
+        k_bsr_spmv_n<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, uj, s->nrm + j, zj, N);
+        k_pruned_spmv_dots<<<rows, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, zj, s->Vi, n6, j + 1,
+                                                 s->nrm, s->part, s->ticket, s->H, j, N);
+        k_inner_orth<<<kInnerBlocks, kInnerThreads, 0, st>>>(s->Vi, n6, j + 1, s->H, s->nrm, j, n6, s->part,
+                                                             s->ticket, j == k - 1 ? k : 0);
     }
-    k_inner_lsq<<<1, 32, 0, st>>>(s->H, k);
     k_inner_post<<<(11 * N + 255) / 256, 256, 0, st>>>(s->Zi, n6, k, s->H + (size_t)(kMaxInner + 1) * kMaxInner + 1,
                                                        b, x, N);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
 }
 
-static int inner_kernels(int k) { return 4 + 6 * k; }
+static int inner_kernels(int k) { return 2 + 3 * k; }
 
-// (Re)capture the inner solve when the arrays it reads were reallocated or k changed.
-static int inner_graph(fsd_handle* h) {
+// (Re)capture the inner solve when the arrays it reads were reallocated or k
+// changed.  The first and last kernel nodes (the only ones that touch b and
+// x) are kept so that each application can point them at its own vectors.
+static int inner_graph(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
     const void* key[8] = {s->g_rowptr, s->g_col, s->g_val, s->a_pn, s->a_plist, s->a_blocks, s->Vi, s->Zi};
     bool same = s->gexec && s->gkey_k == h->p.learned_inner;
     for (int i = 0; i < 8 && same; ++i) same = key[i] == s->gkey[i];
     if (same) return FSD_OK;
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
     s->gexec = nullptr;
+    s->graph = nullptr;
     if (!s->cap_stream) FSD_CHECK_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
     FSD_CHECK_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
-    const int e = inner_enqueue(h, s->tb, s->tx, s->cap_stream);
+    const int e = inner_enqueue(h, b, x, s->cap_stream);
     const cudaError_t ce = cudaStreamEndCapture(s->cap_stream, &g);
     if (e != FSD_OK) {
         if (g) cudaGraphDestroy(g);
         return e;
     }
     FSD_CHECK_CUDA(ce);
+    size_t nn = 0;
+    FSD_CHECK_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    FSD_CHECK_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    s->node_rhs = s->node_post = nullptr;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        FSD_CHECK_CUDA(cudaGraphNodeGetType(nd, &t));
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        FSD_CHECK_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
+        if (kp.func == (void*)k_inner_rhs) s->node_rhs = nd;
+        if (kp.func == (void*)k_inner_post) s->node_post = nd;
+    }
+    if (!s->node_rhs || !s->node_post) {
+        cudaGraphDestroy(g);
+        return FSD_ERR_CUDA;
+    }
     const cudaError_t ie = cudaGraphInstantiate(&s->gexec, g, 0);
-    cudaGraphDestroy(g);
-    FSD_CHECK_CUDA(ie);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        FSD_CHECK_CUDA(ie);
+    }
+    s->graph = g;
     for (int i = 0; i < 8; ++i) s->gkey[i] = key[i];
     s->gkey_k = h->p.learned_inner;
     s->captures += 1;
@@ -428,12 +428,43 @@ static int inner_graph(fsd_handle* h) {
     return FSD_OK;
 }
 
+// Point the graph's first and last kernels at b and x.
+static int inner_bind(fsd_handle* h, const float* b, float* x) {
+    LearnedState* s = learned(h);
+    int N = h->p.N;
+    float* u0 = s->Vi;
+    double* part = s->part;
+    unsigned* ticket = s->ticket;
+    double* H = s->H;
+    double* nrm = s->nrm;
+    void* rhs_args[] = {&b, &u0, &N, &part, &ticket, &H, &nrm};
+    cudaKernelNodeParams kr = {};
+    kr.func = (void*)k_inner_rhs;
+    kr.gridDim = dim3(kInnerBlocks);
+    kr.blockDim = dim3(kInnerThreads);
+    kr.kernelParams = rhs_args;
+    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->gexec, s->node_rhs, &kr));
+    const float* Z = s->Zi;
+    size_t ld = 6 * (size_t)N;
+    int k = h->p.learned_inner;
+    const double* c = s->H + (size_t)(kMaxInner + 1) * kMaxInner + 1;
+    void* post_args[] = {&Z, &ld, &k, &c, &b, &x, &N};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_inner_post;
+    kp.gridDim = dim3((11 * N + 255) / 256);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = post_args;
+    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->gexec, s->node_post, &kp));
+    return FSD_OK;
+}
+
 // x = P^-1 b.  Without inner steps G is applied once (fused with the saddle
 // pre/post steps).  With k inner steps, y ~ (R_FU^pruned + D)^-1 t comes from
 // k steps of GMRES on that matrix from a zero guess, right-preconditioned by
 // G; the map b -> x then depends on b nonlinearly, which the flexible outer
-// GMRES allows.  The inner solve is one CUDA graph launch between a copy of b
-// in and a copy of x out; no host synchronisation.
+// GMRES allows.  The inner solve is one CUDA graph launch reading b and
+// writing x directly; no host synchronisation.  b and x may be the same
+// vector.
 int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
@@ -445,12 +476,11 @@ int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
         FSD_CHECK_CUDA(cudaGetLastError());
         return FSD_OK;
     }
-    const int e = inner_graph(h);
+    int e = inner_graph(h, b, x);
     if (e != FSD_OK) return e;
-    const size_t n17 = 17 * (size_t)N;
-    FSD_CHECK_CUDA(cudaMemcpyAsync(s->tb, b, sizeof(float) * n17, cudaMemcpyDeviceToDevice, st));
+    e = inner_bind(h, b, x);
+    if (e != FSD_OK) return e;
     FSD_CHECK_CUDA(cudaGraphLaunch(s->gexec, st));
-    FSD_CHECK_CUDA(cudaMemcpyAsync(x, s->tx, sizeof(float) * n17, cudaMemcpyDeviceToDevice, st));
     for (int i = 0; i < inner_kernels(k); ++i) count_launch();
     return FSD_OK;
 }

@@ -8,10 +8,12 @@
 // GMRES(m) is right-preconditioned, so the Givens residual is the true residual
 // ||b - A x||; Arnoldi coefficients, Givens rotations and the least-squares
 // solve are FP64; basis vectors are FP32.  Orthogonalisation is classical
-// Gram-Schmidt with one re-orthogonalisation pass.  Everything stays on the
-// device; the host polls a converged flag every few iterations.
+// Gram-Schmidt with one re-orthogonalisation pass, delayed by one iteration
+// so that both passes share their reads of the basis.  Everything stays on
+// the device; the host polls a converged flag every few iterations.
 #include <cmath>
 #include <cstddef>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 
@@ -208,6 +210,14 @@ struct GmresState {
     int total;         // total iterations
     int done;          // converged or broke down this cycle
     int breakdown;
+    // Delayed re-orthogonalisation: the last column waits for the next
+    // iteration's correction (pending = 1), and Tc[c][i] expresses the
+    // vector that was preconditioned at iteration c in the final basis:
+    // v~_c = sum_{i<=c} Tc[c][i] V_i.
+    int pending;
+    int nu_breakdown;
+    double rscale;  // r_{j-1} was stored divided by rscale (= nu of iteration j-1)
+    double Tc[kMaxRestart][kMaxRestart];
 };
 
 // Start of a cycle: r0 norm is in dots[0].
@@ -221,6 +231,8 @@ __global__ void k_cycle_start(GmresState* s, const double* dots, double tol, int
     s->beta2 = beta2;
     s->j = 0;
     s->breakdown = 0;
+    s->pending = 0;
+    s->nu_breakdown = 0;
     for (int i = 0; i <= kMaxRestart; ++i) s->g[i] = 0.0;
     s->g[0] = sqrt(beta2);
     const double bn = s->bnorm2 > 0.0 ? sqrt(s->bnorm2) : 1.0;
@@ -258,13 +270,21 @@ __global__ void k_arnoldi_update(GmresState* s, const double* hcol, int m) {
     if (s->resid <= s->tol || s->j >= m || s->breakdown) s->done = 1;
 }
 
-// Least-squares solve H y = g (upper triangular, size j).
-__global__ void k_lsq(GmresState* s) {
+// Least-squares solve H y = g (upper triangular, size j).  With apply_t the
+// coefficients are mapped from the preconditioned vectors to the final basis:
+// sum_c y_c v~_c = sum_i (T y)_i V_i.
+__global__ void k_lsq(GmresState* s, int apply_t) {
     const int j = s->j;
     for (int i = j - 1; i >= 0; --i) {
         double v = s->g[i];
         for (int k = i + 1; k < j; ++k) v -= s->H[i][k] * s->y[k];
         s->y[i] = (s->H[i][i] != 0.0) ? v / s->H[i][i] : 0.0;
+    }
+    if (!apply_t) return;
+    for (int i = 0; i < j; ++i) {
+        double v = 0.0;
+        for (int c = i; c < j; ++c) v += s->Tc[c][i] * s->y[c];
+        s->y[i] = v;  // y[c] for c > i is still unmapped; y[i] is not read again
     }
 }
 
@@ -279,6 +299,271 @@ __global__ void k_export(const GmresState* s, GmresHost* o) {
     o->done = s->done;
     o->breakdown = s->breakdown;
     o->resid = s->resid;
+}
+
+// ------------------------------------------- delayed re-orthogonalisation
+// Gram-Schmidt with delayed re-orthogonalisation (DCGS2: Bielich, Langou,
+// Thomas, Swirydowicz, Yamazaki, Boman, Parallel Computing 2022).  Iteration
+// j preconditions and multiplies the once-orthogonalised, unnormalised vector
+// v~_j left in slot j by iteration j-1.  One pass reads V_0..V_j against v~_j
+// and w = A M^-1 v~_j (a_i = V_i.v~_j, b_i = V_i.w, alpha = |v~_j|^2,
+// beta = v~_j.w); a second pass writes the re-orthogonalised
+// V_j = (v~_j - sum a_i V_i) / nu with nu^2 = alpha - sum a_i^2, and the next
+// vector r_j = w - sum b_i V_i - h V_j, h = (beta - sum a_i b_i) / nu.  So the
+// basis is read twice per iteration instead of four times.  r_j is stored
+// divided by nu (v~_{j+1} = r_j / nu), so that the lagged vectors keep unit
+// scale instead of compounding the subdiagonal entries (which underflows
+// fp32 within a few dozen iterations).  Column j-1 of H is completed by
+// nu_{j-1} times the a_i and nu of iteration j; column j is committed at
+// once, with |r_j| below it, when its tentative residual meets the tolerance
+// or the cycle is full.
+
+// part[(2i) nb + b] = V_i . V_j and part[(2i+1) nb + b] = V_i . w over block
+// b's slice, i <= j; both slices of V_j and w are staged in shared memory.
+// Slices are `chunk` long, a multiple of 4, and the basis vectors start on
+// 16-byte boundaries, so the basis is read as float4.
+__global__ void __launch_bounds__(kRedThreads) k_dots_pair(const float* __restrict__ V, size_t ld, int j,
+                                                           const float* __restrict__ w, size_t n, size_t chunk,
+                                                           double* part, const int* done) {
+    if (*done) return;
+    extern __shared__ float4 sm4[];
+    float4* sv = sm4;
+    float4* sw = sm4 + chunk / 4;
+    const size_t b0 = (size_t)blockIdx.x * chunk;
+    const size_t len = b0 < n ? min(chunk, n - b0) : 0;
+    const size_t len4 = len / 4;
+    const float* vj = V + (size_t)j * ld + b0;
+    for (size_t k = threadIdx.x; k < len4; k += blockDim.x) {
+        sv[k] = reinterpret_cast<const float4*>(vj)[k];
+        sw[k] = make_float4(w[b0 + 4 * k], w[b0 + 4 * k + 1], w[b0 + 4 * k + 2], w[b0 + 4 * k + 3]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i <= j; i += nw) {
+        const float4* vi = reinterpret_cast<const float4*>(V + (size_t)i * ld + b0);
+        double s1 = 0.0, s2 = 0.0;
+        size_t k = lane;
+        for (; k + 32 < len4; k += 64) {
+            const float4 a = vi[k], c = vi[k + 32];
+            const float4 p = sv[k], q = sw[k], p2 = sv[k + 32], q2 = sw[k + 32];
+            s1 += (double)a.x * p.x + (double)a.y * p.y + (double)a.z * p.z + (double)a.w * p.w +
+                  (double)c.x * p2.x + (double)c.y * p2.y + (double)c.z * p2.z + (double)c.w * p2.w;
+            s2 += (double)a.x * q.x + (double)a.y * q.y + (double)a.z * q.z + (double)a.w * q.w +
+                  (double)c.x * q2.x + (double)c.y * q2.y + (double)c.z * q2.z + (double)c.w * q2.w;
+        }
+        for (; k < len4; k += 32) {
+            const float4 a = vi[k], p = sv[k], q = sw[k];
+            s1 += (double)a.x * p.x + (double)a.y * p.y + (double)a.z * p.z + (double)a.w * p.w;
+            s2 += (double)a.x * q.x + (double)a.y * q.y + (double)a.z * q.z + (double)a.w * q.w;
+        }
+        // the ragged end of the last slice
+        const float* vs = V + (size_t)i * ld + b0;
+        for (size_t t = 4 * len4 + lane; t < len; t += 32) {
+            s1 += (double)vs[t] * vj[t];
+            s2 += (double)vs[t] * w[b0 + t];
+        }
+        s1 = group_sum_d<32>(s1);
+        s2 = group_sum_d<32>(s2);
+        if (lane == 0) {
+            part[(size_t)(2 * i) * gridDim.x + blockIdx.x] = s1;
+            part[(size_t)(2 * i + 1) * gridDim.x + blockIdx.x] = s2;
+        }
+    }
+}
+
+// Givens rotations 0..c-1 applied to column col (rows 0..c, in shared
+// memory) with hsub below it, then a new rotation for (c, c+1), stored in
+// cs/sn[c]; g (rows c, c+1) and the residual are updated in the state.
+__device__ void givens_column(double* col, int c, double hsub, double* cs, double* sn, GmresState* s) {
+    col[c + 1] = hsub;
+    for (int i = 0; i < c; ++i) {
+        const double a = col[i], b = col[i + 1];
+        col[i] = cs[i] * a + sn[i] * b;
+        col[i + 1] = -sn[i] * a + cs[i] * b;
+    }
+    const double a = col[c], b = col[c + 1];
+    const double r = hypot(a, b);
+    const double cc = r > 0.0 ? a / r : 1.0, sv = r > 0.0 ? b / r : 0.0;
+    cs[c] = cc;
+    sn[c] = sv;
+    col[c] = r;
+    col[c + 1] = 0.0;
+    const double gc = s->g[c];
+    s->g[c + 1] = -sv * gc;
+    s->g[c] = cc * gc;
+    const double bn = s->bnorm2 > 0.0 ? sqrt(s->bnorm2) : 1.0;
+    s->resid = fabs(s->g[c + 1]) / bn;
+}
+
+// Residual after raw column col (rows 0..c) with hsub below it, no changes.
+__device__ double tentative_resid(const double* col, int c, double hsub, const double* cs, const double* sn,
+                                  const GmresState* s) {
+    double a = col[0];
+    for (int i = 0; i < c; ++i) a = -sn[i] * a + cs[i] * col[i + 1];
+    const double r = hypot(a, hsub);
+    const double sv = r > 0.0 ? hsub / r : 0.0;
+    const double bn = s->bnorm2 > 0.0 ? sqrt(s->bnorm2) : 1.0;
+    return fabs(sv * s->g[c]) / bn;
+}
+
+// Second pass of iteration j (dots = the 2(j+1) finished sums of the first):
+// V_j re-orthogonalised in place, r_j / nu written to slot j+1, its squared
+// norm reduced by the last block, which then completes column j-1 and
+// commits column j or leaves it pending.  Every block computes the same
+// coefficients.  Only the last block touches the state after every block has
+// read `done`; its serial work runs on shared-memory copies.
+__global__ void __launch_bounds__(kRedThreads, 4) k_dcgs_update(float* V, size_t ld, int j, const float* __restrict__ w,
+                                                             size_t n, const double* __restrict__ dots,
+                                                             GmresState* s, int m, double* part, unsigned* ticket) {
+    if (s->done) return;
+    __shared__ float ca[kMaxRestart + 1], cc[kMaxRestart + 1];
+    __shared__ double sh[2][32];
+    __shared__ double s_nu, s_h;
+    double a2 = 0.0, ab = 0.0;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+        const double a = dots[2 * i], b = dots[2 * i + 1];
+        a2 += a * a;
+        ab += a * b;
+    }
+    a2 = group_sum_d<32>(a2);
+    ab = group_sum_d<32>(ab);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][wid] = a2;
+        sh[1][wid] = ab;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double A2 = 0.0, AB = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            A2 += sh[0][q];
+            AB += sh[1][q];
+        }
+        const double nu2 = dots[2 * j] - A2;
+        const double nu = nu2 > 0.0 ? sqrt(nu2) : 0.0;
+        s_nu = nu;
+        s_h = nu > 0.0 ? (dots[2 * j + 1] - AB) / nu : 0.0;
+    }
+    __syncthreads();
+    const double nu = s_nu, hj = s_h;
+    const double hn = nu > 0.0 ? hj / nu : 0.0;
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+        const double a = dots[2 * i], b = dots[2 * i + 1];
+        ca[i] = (float)a;
+        cc[i] = (float)(b - hn * a);
+    }
+    __syncthreads();
+    const float fv = nu > 0.0 ? (float)(1.0 / nu) : 0.f;
+    const float fh = (float)hn;
+    float4* vj = reinterpret_cast<float4*>(V + (size_t)j * ld);
+    float4* vn = reinterpret_cast<float4*>(V + (size_t)(j + 1) * ld);
+    const float4* w4 = reinterpret_cast<const float4*>(w);
+    const bool w_aligned = (reinterpret_cast<uintptr_t>(w) & 15) == 0;
+    const size_t n4 = (n + 3) / 4;  // the basis stride is padded to 32 floats; w is read element-wise at its end
+    double sig = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n4; k += (size_t)gridDim.x * blockDim.x) {
+        const float4 vt = vj[k];
+        float4 aw;
+        if (w_aligned && 4 * k + 3 < n) {
+            aw = w4[k];
+        } else {
+            aw.x = 4 * k < n ? w[4 * k] : 0.f;
+            aw.y = 4 * k + 1 < n ? w[4 * k + 1] : 0.f;
+            aw.z = 4 * k + 2 < n ? w[4 * k + 2] : 0.f;
+            aw.w = 4 * k + 3 < n ? w[4 * k + 3] : 0.f;
+        }
+        float4 av = vt;
+        for (int i = 0; i < j; ++i) {
+            const float4 vi = reinterpret_cast<const float4*>(V + (size_t)i * ld)[k];
+            const float a = ca[i], c = cc[i];
+            av.x = fmaf(-a, vi.x, av.x);
+            av.y = fmaf(-a, vi.y, av.y);
+            av.z = fmaf(-a, vi.z, av.z);
+            av.w = fmaf(-a, vi.w, av.w);
+            aw.x = fmaf(-c, vi.x, aw.x);
+            aw.y = fmaf(-c, vi.y, aw.y);
+            aw.z = fmaf(-c, vi.z, aw.z);
+            aw.w = fmaf(-c, vi.w, aw.w);
+        }
+        float4 r;
+        r.x = fmaf(-fh, vt.x, aw.x) * fv;
+        r.y = fmaf(-fh, vt.y, aw.y) * fv;
+        r.z = fmaf(-fh, vt.z, aw.z) * fv;
+        r.w = fmaf(-fh, vt.w, aw.w) * fv;
+        float4 v = make_float4(av.x * fv, av.y * fv, av.z * fv, av.w * fv);
+        if (4 * k + 3 >= n) {  // padding past 17N stays zero (it was never written before)
+            if (4 * k + 1 >= n) r.y = v.y = 0.f;
+            if (4 * k + 2 >= n) r.z = v.z = 0.f;
+            r.w = v.w = 0.f;
+        }
+        vj[k] = v;
+        vn[k] = r;
+        sig += (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z + (double)r.w * r.w;
+    }
+    block_partial(sig, part);
+    if (!last_block(ticket)) return;
+    __shared__ double cprev[kMaxRestart + 2], ccur[kMaxRestart + 2], scs[kMaxRestart + 1], ssn[kMaxRestart + 1];
+    __shared__ int commit, drop_j, pend_s;
+    const bool pend = j > 0 && s->pending;
+    const double rs = s->rscale;
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) {
+        if (i < j) {
+            scs[i] = s->cs[i];
+            ssn[i] = s->sn[i];
+            if (pend) cprev[i] = s->H[i][j - 1] + rs * dots[2 * i];
+            s->Tc[j][i] = dots[2 * i];
+        } else {
+            s->Tc[j][j] = nu;
+        }
+        ccur[i] = i < j ? dots[2 * i + 1] : hj;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const double sum = warp_sum_parts(part, gridDim.x);
+        if (threadIdx.x == 0) {
+            s->total += 1;
+            if (pend) givens_column(cprev, j - 1, rs * nu, scs, ssn, s);
+            pend_s = pend;
+            commit = 0;
+            drop_j = 0;
+            const double hsub = nu * sqrt(sum);
+            s->rscale = nu;
+            s->pending = 0;
+            if (!(nu > 1e-300)) {  // v~_j lay in the span of V_0..V_j-1
+                s->breakdown = 1;
+                s->j = j;
+                s->done = 1;
+                drop_j = 1;
+            } else {
+                s->j = j + 1;
+                const double rt = tentative_resid(ccur, j, hsub, scs, ssn, s);
+                const bool bad = !(hsub > 1e-300) || !(rt == rt);
+                if (rt <= s->tol || j + 1 >= m || bad) {
+                    givens_column(ccur, j, hsub, scs, ssn, s);
+                    if (bad) s->breakdown = (hsub > 1e-300) ? 2 : 1;
+                    s->done = 1;
+                    commit = 1;
+                } else {
+                    s->pending = 1;
+                }
+            }
+            *ticket = 0;
+        }
+    }
+    __syncthreads();
+    // Write back: column j-1 rotated, column j rotated (committed) or raw (pending).
+    for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) {
+        if (pend_s && i <= j) s->H[i][j - 1] = cprev[i];
+        if (!drop_j && (i <= j || commit)) s->H[i][j] = ccur[i];
+        if (pend_s && i == j - 1) {
+            s->cs[i] = scs[i];
+            s->sn[i] = ssn[i];
+        }
+        if (commit && i == j) {
+            s->cs[i] = scs[i];
+            s->sn[i] = ssn[i];
+        }
+    }
 }
 
 static const double* gs_y(const GmresState* s) {
@@ -303,7 +588,7 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     cudaStream_t st = h->stream;
     GmresState* gs = (GmresState*)w.gmres_state;
     GmresHost* gh = (GmresHost*)w.gmres_host;
-    const size_t ld = n;
+    const size_t ld = krylov_ld(N);
     float* V = w.V;
     float* r = w.sx;   // residual / work
     float* Ax = w.sy;  // operator output
@@ -318,6 +603,13 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     if (flexible && !w.Z) return FSD_ERR_BAD_PARAMS;
     const size_t chunk = (n + nbl - 1) / nbl;
     const bool staged = chunk * sizeof(float) <= 48 * 1024;
+    // Delayed re-orthogonalisation stages two slices per block, each a
+    // multiple of 4 floats long.
+    const size_t chunk4 = (chunk + 3) & ~(size_t)3;
+    const size_t pair_smem = 2 * chunk4 * sizeof(float);
+    const bool delayed = pair_smem <= 200 * 1024;
+    if (delayed && pair_smem > 48 * 1024)
+        FSD_CHECK_CUDA(cudaFuncSetAttribute(k_dots_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem));
     auto multidot = [&](const float* Vb, size_t ldv, int nv, const float* wv, size_t nn, double* pt, const int* dn) {
         if (staged)
             k_multidot_ws<<<nbl, kRedThreads, chunk * sizeof(float), st>>>(Vb, ldv, nv, wv, nn, chunk, pt, dn);
@@ -366,8 +658,24 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
                 if (e != FSD_OK) return e;
                 e = saddle_multiply(h, pos, zj, Ax, false);
                 if (e != FSD_OK) return e;
-                // CGS2 against V_0..V_j.
                 ProfRegion pk(h, R_KRYLOV);
+                if (delayed) {
+                    count_launch();
+                    k_dots_pair<<<nbl, kRedThreads, pair_smem, st>>>(V, ld, j, Ax, n, chunk4, part, &gs->done);
+                    count_launch();
+                    k_finish_dots<<<(2 * (j + 1) + 7) / 8, 256, 0, st>>>(part, nbl, 2 * (j + 1), dots, false,
+                                                                         &gs->done);
+                    count_launch();
+                    k_dcgs_update<<<vblocks, kRedThreads, 0, st>>>(V, ld, j, Ax, n, dots, gs, m, part, w.ticket);
+                    if ((j % 4) == 3 || j == m - 1) {
+                        count_launch();
+                        k_export<<<1, 1, 0, st>>>(gs, gh);
+                        FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+                        if (gh->done) break;
+                    }
+                    continue;
+                }
+                // CGS2 against V_0..V_j.
                 count_launch();
                 multidot(V, ld, j + 1, Ax, n, part, &gs->done);
                 count_launch();
@@ -407,7 +715,7 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
             total = gh->total;
             if (jc > 0) {
                 count_launch();
-                k_lsq<<<1, 1, 0, st>>>(gs);
+                k_lsq<<<1, 1, 0, st>>>(gs, delayed && !flexible ? 1 : 0);
                 if (flexible) {  // x += Z y
                     count_launch();
                     k_combine<<<vblocks, vthreads, 0, st>>>(w.Z, ld, jc, gs_y(gs), z, n);

@@ -154,12 +154,16 @@ def test_preconditioner_equals_ichol_of_reference_ordering(cuda):
     assert rel(got, O.saddle_precond(b, G, N)) < 1e-4
 
 
-@pytest.mark.parametrize("precond", ["ichol", "none"])
-def test_saddle_solve_matches_dense_solution(cuda, precond):
+@pytest.mark.parametrize("precond,restart,inner", [("ichol", 100, 0), ("none", 100, 0), ("ichol", 7, 0),
+                                                  ("learned", 7, 0), ("learned", 7, 3)])
+def test_saddle_solve_matches_dense_solution(cuda, precond, restart, inner):
+    """Restart 7 runs several GMRES cycles: with a fixed preconditioner the
+    solution is mapped back through the delayed re-orthogonalisation's
+    coefficients, with inner steps (flexible GMRES) through the kept Z basis."""
     N = 80
     pos, Lc = suspension(N, 0.2, 9)
     L = (Lc, Lc, Lc)
-    s, p = solver_for(pos, L, 0.0, precond=precond, solver_tol=1e-6)
+    s, p = solver_for(pos, L, 0.0, precond=precond, solver_tol=1e-6, gmres_restart=restart, learned_inner=inner)
     s.precond_build(p)
     pr = problem(pos, L)
     rhs = np.random.default_rng(10).standard_normal(17 * N)

@@ -1,10 +1,11 @@
 """Velocities and stresslets of one velocity computation (fsd_compute_velocity,
 Integrator_ComputeVelocity at kT = 0) against the FP64 oracle: BASELINE
 config 1 (N = 1000 at phi = 0.2, no shear) and a sheared, tilted dense case.
-GMRES runs to 1e-6 (2e-7 for the dense sheared case, whose small relative
-velocities amplify the solver's residual) so that solver error stays under
-the 1e-4 bar on velocities and stresslets (relative 2-norm); the
-interparticle force must agree to 1e-5."""
+GMRES runs to 1e-6 (5e-7 for the dense sheared case, whose small relative
+velocities amplify the solver's residual: 1e-6 leaves 1.005e-4 there, 5e-7
+leaves 4.5e-5) so that solver error stays under the 1e-4 bar on velocities
+and stresslets (relative 2-norm); the FP32 residual floor near 2e-7 keeps
+the tolerance above that.  The interparticle force must agree to 1e-5."""
 from __future__ import annotations
 
 import numpy as np
@@ -25,7 +26,7 @@ def rel(a, b):
 
 @pytest.mark.parametrize("N,phi,seed,shear,xy,precond,tol", [(1000, 0.2, 1, 0.0, 0.0, "ichol", 1e-6),
                                                                (1000, 0.2, 1, 0.0, 0.0, "learned", 1e-6),
-                                                               (400, 0.35, 2, 1.0, 0.15, "learned", 2e-7)])
+                                                               (400, 0.35, 2, 1.0, 0.15, "learned", 5e-7)])
 def test_velocity_and_stresslet_match_oracle(cuda, N, phi, seed, shear, xy, precond, tol):
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
