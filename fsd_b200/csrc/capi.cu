@@ -49,9 +49,12 @@ template <class T> static int dalloc(T** p, size_t n) {
 static int alloc_nlist(fsd_handle* h, int stride) {
     Workspace& w = h->w;
     if (w.nlist) cudaFree(w.nlist);
+    if (w.lub_list) cudaFree(w.lub_list);
     w.nlist = nullptr;
+    w.lub_list = nullptr;
     w.nl_stride = stride;
-    return dalloc(&w.nlist, (size_t)h->p.N * stride);
+    FSD_TRY(dalloc(&w.nlist, (size_t)h->p.N * stride));
+    return dalloc(&w.lub_list, (size_t)h->p.N * stride);
 }
 
 static int allocate(fsd_handle* h) {
@@ -73,6 +76,9 @@ static int allocate(fsd_handle* h) {
     FSD_TRY(dalloc(&w.cell_start, w.ncell_cap + 1));
     FSD_TRY(dalloc(&w.cell_fill, w.ncell_cap + 1));
     FSD_TRY(dalloc(&w.cell_parts, N));
+    FSD_TRY(dalloc(&w.order, N));
+    FSD_TRY(dalloc(&w.lub_n, N));
+    FSD_TRY(init_particle_order(h));
     FSD_TRY(dalloc(&w.part_origin_key, N));
     FSD_TRY(dalloc(&w.part_origin, 3 * (size_t)N));
     FSD_TRY(dalloc(&w.bin_count, G + 1));
@@ -123,7 +129,7 @@ static int allocate(fsd_handle* h) {
 static void release(fsd_handle* h) {
     Workspace& w = h->w;
     void* dev[] = {w.nneigh, w.nlist, w.nl_overflow, w.scan_scratch, w.part_cell, w.cell_count, w.cell_start,
-                   w.cell_fill, w.cell_parts, w.part_origin_key, w.part_origin, w.bin_count, w.bin_start, w.bin_fill,
+                   w.cell_fill, w.cell_parts, w.order, w.lub_n, w.lub_list, w.part_origin_key, w.part_origin, w.bin_count, w.bin_start, w.bin_fill,
                    w.bin_parts, w.grid, w.gridk, w.twiddle, w.f4, w.c4, w.uwave, w.sx, w.sy, w.sz, w.V, w.Z, w.dred,
                    w.hcol, w.hcol2, w.ticket, w.gmres_state, w.pc_t, w.pc_y, w.rhs, w.sol, w.rfd_rhs, w.rfd_sol, w.psi,
                    w.pos_prime, w.vel, w.force, w.lanczos_V, w.lz_a, w.lz_b, w.lz_c, w.lz_dot, h->d_ewald,
@@ -355,6 +361,7 @@ int fsd_build_neighbor_list(fsd_handle* h, const float* d_pos) {
         FSD_TRY(build_neighbor_list(h, (const float4*)d_pos, &maxc));
         h->info.nlist_max = maxc;
         if (maxc <= h->w.nl_stride) {
+            FSD_TRY(build_lub_list(h, (const float4*)d_pos));
             h->nlist_valid = true;
             h->pc_valid = false;
             return FSD_OK;

@@ -103,11 +103,11 @@ __device__ __forceinline__ double group_sum_d(double v) {
     return v;
 }
 
-// Last-block reduction: every block has written its partials, fenced; the
-// block that takes the last ticket sees all of them and resets the ticket.
+// Last-block reduction: the threads that wrote this block's partials have
+// fenced them; the block that takes the last ticket sees every block's
+// partials and resets the ticket.
 __device__ __forceinline__ bool last_block(unsigned* ticket) {
     __shared__ bool last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     __syncthreads();
@@ -122,7 +122,7 @@ __device__ __forceinline__ double warp_sum_parts(const double* part, int n) {
     return group_sum_d<32>(s);
 }
 
-// Block sum of v written to part[blockIdx.x].
+// Block sum of v written (and fenced) to part[blockIdx.x].
 __device__ __forceinline__ void block_partial(double v, double* part) {
     __shared__ double sh[32];
     v = group_sum_d<32>(v);
@@ -131,7 +131,10 @@ __device__ __forceinline__ void block_partial(double v, double* part) {
     if (threadIdx.x < 32) {
         double t = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
         t = group_sum_d<32>(t);
-        if (threadIdx.x == 0) part[blockIdx.x] = t;
+        if (threadIdx.x == 0) {
+            part[blockIdx.x] = t;
+            __threadfence();
+        }
     }
 }
 

@@ -75,6 +75,13 @@ struct Workspace {
     unsigned* cell_fill = nullptr;
     unsigned* cell_parts = nullptr;
     size_t ncell_cap = 0;
+    // particles in cell order (a permutation of 0..N-1, identity until the
+    // first cell-list build): the order in which per-particle pair kernels
+    // visit particles, so that neighbouring particles share the gathered data
+    unsigned* order = nullptr;
+    // the neighbour list restricted to r < rlub + nlist_buffer (same stride)
+    unsigned* lub_n = nullptr;
+    unsigned* lub_list = nullptr;
     // particles binned by spreading-stencil origin (one bin per grid node)
     unsigned* part_origin_key = nullptr;
     int* part_origin = nullptr;

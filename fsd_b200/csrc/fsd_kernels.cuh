@@ -12,6 +12,8 @@ void counting_sort(const unsigned* key, int n, int nbins, unsigned* count, unsig
                    unsigned* items, unsigned* scan_scratch, cudaStream_t st);
 int3 cell_dims(const Box& b, float rlist);
 int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host);
+int build_lub_list(fsd_handle* h, const float4* pos);
+int init_particle_order(fsd_handle* h);
 
 // mobility.cu
 struct FFTPlan {

@@ -1,12 +1,13 @@
 // Block-sparse preconditioner slot G for FSD_PRECOND_LEARNED.
 //
-// G ~ (R_FU^pruned + relaxer D)^-1 is an explicit block-sparse matrix
-// (6x6 fp32 blocks in block-CSR over particles, original particle order), so
-// one application is a single parallel SpMV instead of the two sequential
-// triangular solves of the IC(0) factor.  The blocks are produced by the
-// message-passing network at each preconditioner build, or set directly through
-// fsd_precond_set_blocks.  The saddle pre/post steps (Saddle.cu:171-264) are
-// fused into the SpMV kernel, exactly as in the IC(0) solve kernels.
+// G ~ (R_FU^pruned + relaxer D)^-1 is an explicit block-sparse matrix (6x6
+// fp32 blocks in block-CSR over particles, original particle order): the
+// two-hop sparse approximate inverse of the pruned matrix (spai.cu), plus the
+// loaded network's correction (mpnn.cu), or blocks set directly through
+// fsd_precond_set_blocks.  Applied once (learned_inner = 0, fused with the
+// saddle pre/post steps of Saddle.cu:171-264) or as the right preconditioner
+// of a few inner GMRES steps on the pruned matrix itself, replayed from a
+// CUDA graph.
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -149,14 +150,25 @@ __global__ void __launch_bounds__(256) k_bsr_spmv_n(const int* __restrict__ rowp
                                                     const float* __restrict__ G, const float* __restrict__ u,
                                                     const double* __restrict__ unrm, float* __restrict__ z, int N) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gid >> 3;
     const int r = threadIdx.x & 7;
-    if (i >= N) return;  // whole groups of eight leave together
+    const int i = gid >> 3;  // rows in storage order: the kernel streams G
+    if (i >= N) return;      // whole groups of eight leave together
     const unsigned gmask = 0xffu << (threadIdx.x & 24);
     const int rr = r < 6 ? r : 0;
     float acc = 0.f;
     const int e1 = rowptr[i + 1];
-    for (int e = rowptr[i]; e < e1; ++e) {
+    int e = rowptr[i];
+    for (; e + 3 < e1; e += 4) {  // four blocks in flight per lane
+        const int j0 = col[e], j1 = col[e + 1], j2 = col[e + 2], j3 = col[e + 3];
+        const float x0 = (r < 6) ? u[6 * j0 + r] : 0.f, x1 = (r < 6) ? u[6 * j1 + r] : 0.f;
+        const float x2 = (r < 6) ? u[6 * j2 + r] : 0.f, x3 = (r < 6) ? u[6 * j3 + r] : 0.f;
+        const float* Ge = G + (size_t)e * 36;
+        acc += block_row(Ge, rr, x0, gmask);
+        acc += block_row(Ge + 36, rr, x1, gmask);
+        acc += block_row(Ge + 72, rr, x2, gmask);
+        acc += block_row(Ge + 108, rr, x3, gmask);
+    }
+    for (; e < e1; ++e) {
         const int j = col[e];
         const float xj = (r < 6) ? u[6 * j + r] : 0.f;
         acc += block_row(G + (size_t)e * 36, rr, xj, gmask);
@@ -195,21 +207,35 @@ __global__ void __launch_bounds__(kInnerThreads) k_inner_rhs(const float* __rest
 // U_nv, fused with the dots H[j][q] = (U_q . w) / |U_q| for q < nv = j + 1.
 __global__ void __launch_bounds__(256) k_pruned_spmv_dots(const unsigned* __restrict__ pn,
                                                           const unsigned* __restrict__ plist,
-                                                          const float* __restrict__ A, const float* __restrict__ z, float* U, size_t ld, int nv,
+                                                          const float* __restrict__ A,
+                                                          const float* __restrict__ z, float* U, size_t ld, int nv,
                                                           const double* __restrict__ nrm, double* part,
                                                           unsigned* ticket, double* H, int j, int N) {
     __shared__ double sh[kMaxInner + 1][8];
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gid >> 3;
+    const int i = gid >> 3;  // rows in storage order: the kernel streams A
+    const bool row_ok = i < N;
     const int r = threadIdx.x & 7;
-    const bool act = i < N && r < 6;
+    const bool act = row_ok && r < 6;
     float acc = 0.f;
-    if (i < N) {  // whole groups of eight; every thread reaches the reductions below
+    if (row_ok) {  // whole groups of eight; every thread reaches the reductions below
         const unsigned gmask = 0xffu << (threadIdx.x & 24);
         const int rr = r < 6 ? r : 0;
         const unsigned n = pn[i];
-        for (unsigned q = 0; q < n; ++q) {
-            const size_t e = (size_t)i * kPrunedCap + q;
+        const size_t e0 = (size_t)i * kPrunedCap;
+        unsigned q = 0;
+        for (; q + 3 < n; q += 4) {  // four blocks in flight per lane
+            const unsigned j0 = plist[e0 + q], j1 = plist[e0 + q + 1], j2 = plist[e0 + q + 2], j3 = plist[e0 + q + 3];
+            const float x0 = (r < 6) ? z[6 * j0 + r] : 0.f, x1 = (r < 6) ? z[6 * j1 + r] : 0.f;
+            const float x2 = (r < 6) ? z[6 * j2 + r] : 0.f, x3 = (r < 6) ? z[6 * j3 + r] : 0.f;
+            const float* Ae = A + (e0 + q) * 36;
+            acc += block_row(Ae, rr, x0, gmask);
+            acc += block_row(Ae + 36, rr, x1, gmask);
+            acc += block_row(Ae + 72, rr, x2, gmask);
+            acc += block_row(Ae + 108, rr, x3, gmask);
+        }
+        for (; q < n; ++q) {
+            const size_t e = e0 + q;
             const unsigned jj = plist[e];
             const float xj = (r < 6) ? z[6 * jj + r] : 0.f;
             acc += block_row(A + e * 36, rr, xj, gmask);
@@ -227,6 +253,7 @@ __global__ void __launch_bounds__(256) k_pruned_spmv_dots(const unsigned* __rest
         double v = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sh[threadIdx.x][w];
         part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = v;
+        __threadfence();
     }
     if (!last_block(ticket)) return;
     for (int q = wid; q < nv; q += blockDim.x >> 5) {

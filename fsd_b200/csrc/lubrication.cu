@@ -2,7 +2,9 @@
 // (Lubrication.cu of the reference).  Each particle owns its output row and
 // sums over its own neighbours, so results are deterministic and no atomics
 // are needed; a group of 8 lanes splits a particle's neighbours and reduces
-// with shuffles.  The resistance scalars are interpolated from the tabulated
+// with shuffles.  The list is the neighbour list cut at rlub plus the list
+// buffer (same order, so the same sums), and particles are visited in cell
+// order so that a block's gathers overlap.  The resistance scalars are interpolated from the tabulated
 // Jeffrey-Onishi functions exactly as the reference does (res_interp).
 #include "fsd_device.cuh"
 #include "fsd_kernels.cuh"
@@ -14,6 +16,7 @@ constexpr int kLubGroup = 8;
 
 struct LubArgs {
     const float4* pos;
+    const unsigned* order;  // particles in cell order
     const unsigned* nneigh;
     const unsigned* nlist;
     int stride;
@@ -59,7 +62,7 @@ __global__ void __launch_bounds__(128) k_rfu(LubArgs a, const float* __restrict_
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLubGroup;
     const int gl = threadIdx.x % kLubGroup;
     const bool valid = gid < a.N;
-    const int i = valid ? gid : a.N - 1;
+    const int i = (int)a.order[valid ? gid : a.N - 1];
     const float4 pi = a.pos[i];
     const float3 ui = make_float3(U[6 * i], U[6 * i + 1], U[6 * i + 2]);
     const float3 wi = make_float3(U[6 * i + 3], U[6 * i + 4], U[6 * i + 5]);
@@ -117,7 +120,7 @@ __global__ void __launch_bounds__(128) k_rfe(LubArgs a, float shear_rate, const 
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLubGroup;
     const int gl = threadIdx.x % kLubGroup;
     const bool valid = gid < a.N;
-    const int i = valid ? gid : a.N - 1;
+    const int i = (int)a.order[valid ? gid : a.N - 1];
     const float4 pi = a.pos[i];
     float Ei[3][3], Ej[3][3];
     strain_block(shear_rate, ori, b2mask, B2, i, Ei);
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(128) k_rsu(LubArgs a, const float* __restrict_
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLubGroup;
     const int gl = threadIdx.x % kLubGroup;
     const bool valid = gid < a.N;
-    const int i = valid ? gid : a.N - 1;
+    const int i = (int)a.order[valid ? gid : a.N - 1];
     const float4 pi = a.pos[i];
     const float3 ui = make_float3(U[6 * i], U[6 * i + 1], U[6 * i + 2]);
     const float3 wi = make_float3(U[6 * i + 3], U[6 * i + 4], U[6 * i + 5]);
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(128) k_rse(LubArgs a, float shear_rate, const 
     const int gid = (blockIdx.x * blockDim.x + threadIdx.x) / kLubGroup;
     const int gl = threadIdx.x % kLubGroup;
     const bool valid = gid < a.N;
-    const int i = valid ? gid : a.N - 1;
+    const int i = (int)a.order[valid ? gid : a.N - 1];
     const float4 pi = a.pos[i];
     float Ei[3][3], Ej[3][3];
     strain_block(shear_rate, ori, b2mask, B2, i, Ei);
@@ -273,8 +276,9 @@ __global__ void __launch_bounds__(128) k_rse(LubArgs a, float shear_rate, const 
 static LubArgs lub_args(fsd_handle* h, const float4* pos) {
     LubArgs a;
     a.pos = pos;
-    a.nneigh = h->w.nneigh;
-    a.nlist = h->w.nlist;
+    a.order = h->w.order;
+    a.nneigh = h->w.lub_n;
+    a.nlist = h->w.lub_list;
     a.stride = h->w.nl_stride;
     a.tab.dist = h->d_res_dist;
     a.tab.vals = h->d_res_vals;

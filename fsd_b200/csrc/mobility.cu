@@ -86,8 +86,24 @@ __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.
 // as constants (conjugated for the inverse).
 // cos and sin of -2 pi m / P for the radices used (m < P); folded to
 // constants once the DFT loops are unrolled.
+// Radix 9 uses cos and sin of 2 pi m / 9, m = 1..4, mirrored.
+__host__ __device__ constexpr float root9_c(int m) {
+    return (m == 0) ? 1.0f
+         : (m == 1 || m == 8) ? 0.76604444311897804f
+         : (m == 2 || m == 7) ? 0.17364817766693035f
+         : (m == 3 || m == 6) ? -0.5f
+         : -0.93969262078590838f;
+}
+__host__ __device__ constexpr float root9_s(int m) {
+    return (m == 0) ? 0.0f
+         : (m == 1) ? -0.64278760968653933f : (m == 8) ? 0.64278760968653933f
+         : (m == 2) ? -0.98480775301220806f : (m == 7) ? 0.98480775301220806f
+         : (m == 3) ? -0.86602540378443865f : (m == 6) ? 0.86602540378443865f
+         : (m == 4) ? -0.34202014332566873f : 0.34202014332566873f;
+}
 __host__ __device__ constexpr float root_c(int P, int m) {
-    return P == 2 ? (m == 0 ? 1.0f : -1.0f)
+    return P == 9 ? root9_c(m)
+         : P == 2 ? (m == 0 ? 1.0f : -1.0f)
          : P == 3 ? (m == 0 ? 1.0f : -0.5f)
          : P == 4 ? (m == 0 ? 1.0f : (m == 2 ? -1.0f : 0.0f))
          : P == 5 ? (m == 0 ? 1.0f : (m == 1 || m == 4) ? 0.30901699437494742f : -0.80901699437494742f)
@@ -95,7 +111,8 @@ __host__ __device__ constexpr float root_c(int P, int m) {
                     : (m == 1 || m == 7) ? 0.70710678118654752f : -0.70710678118654752f);
 }
 __host__ __device__ constexpr float root_s(int P, int m) {
-    return P == 2 ? 0.0f
+    return P == 9 ? root9_s(m)
+         : P == 2 ? 0.0f
          : P == 3 ? (m == 0 ? 0.0f : m == 1 ? -0.86602540378443865f : 0.86602540378443865f)
          : P == 4 ? (m == 1 ? -1.0f : m == 3 ? 1.0f : 0.0f)
          : P == 5 ? (m == 0 ? 0.0f : m == 1 ? -0.95105651629515357f : m == 2 ? -0.58778525229247313f
@@ -189,7 +206,7 @@ __device__ float2* fft_lines(float2* a, float2* b, int nlines, const FFTPlan& pl
 
 // One axis of the 3D transform for all 6 packed grids.  axis 2 (z): batches of
 // B contiguous lines; axes 1 (y) and 0 (x): lines grouped by B consecutive z.
-__global__ void k_fft_axis(float2* __restrict__ data, int Nx, int Ny, int Nz, int axis, int B, FFTPlan pl,
+__global__ void __launch_bounds__(256, 4) k_fft_axis(float2* __restrict__ data, int Nx, int Ny, int Nz, int axis, int B, FFTPlan pl,
                            const float2* __restrict__ tw_global, bool inv, int ngrids) {
     extern __shared__ float2 smem[];
     const int n = pl.n;
@@ -250,6 +267,103 @@ __global__ void k_fft_axis(float2* __restrict__ data, int Nx, int Ny, int Nz, in
     }
 }
 
+// y and z passes of one (grid, x) plane in a single kernel, for Ny = Nz = N =
+// N1 * N2.  The N x N plane (contiguous in global memory, z fastest) sits in
+// shared memory with row stride N + 1.  Each length-N line is transformed in
+// two in-place stages (Cooley-Tukey, N = N1 N2): the N2-point DFTs over the
+// stride-N1 subsequences with the twiddles w_N^(n1 k2), then the N1-point DFTs
+// over contiguous runs of N1, each writing its outputs into the slots it
+// read.  Coefficient k = k2 + N2 k1 of a line therefore ends at slot
+// k1 + N1 k2; the store undoes that order on both axes.  Forward: z lines,
+// then y lines; inverse: y, then z (the order of the separate passes).
+template <int N1, int N2>
+__device__ __forceinline__ int plane_slot(int k) {
+    return k / N2 + N1 * (k % N2);
+}
+
+template <int N1, int N2>
+__device__ __forceinline__ void plane_lines(float2* pl, const float2* tw, bool rows, bool inv) {
+    constexpr int N = N1 * N2, RS = N + 1;
+    // element i of line l: rows (z lines) at l * RS + i, columns (y lines) at i * RS + l
+    const int es = rows ? 1 : RS, ls = rows ? RS : 1;
+    for (int t = threadIdx.x; t < N * N1; t += blockDim.x) {
+        const int l = t % N, n1 = t / N;  // consecutive threads: consecutive lines
+        float2* L = pl + l * ls + n1 * es;
+        float2 y[N2];
+#pragma unroll
+        for (int q = 0; q < N2; ++q) y[q] = L[q * N1 * es];
+        small_dft<N2>(y, inv);
+#pragma unroll
+        for (int q = 0; q < N2; ++q) {
+            float2 w = tw[n1 * q];
+            if (inv) w.y = -w.y;
+            L[q * N1 * es] = q == 0 ? y[0] : cmul(y[q], w);
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < N * N2; t += blockDim.x) {
+        const int l = t % N, k2 = t / N;
+        float2* L = pl + l * ls + k2 * N1 * es;
+        float2 y[N1];
+#pragma unroll
+        for (int q = 0; q < N1; ++q) y[q] = L[q * es];
+        small_dft<N1>(y, inv);
+#pragma unroll
+        for (int q = 0; q < N1; ++q) L[q * es] = y[q];
+    }
+    __syncthreads();
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_fft_yz(float2* __restrict__ data, int Nx, const float2* __restrict__ tw_global,
+                                                bool inv) {
+    constexpr int N = N1 * N2, RS = N + 1;
+    extern __shared__ float2 smem[];
+    float2* tw = smem;
+    float2* pl = smem + N;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_global[i];
+    const size_t base = (size_t)blockIdx.x * N * N;  // blocks are (grid, x) planes in memory order
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        const int y = e / N, z = e - y * N;
+        pl[y * RS + z] = data[base + e];
+    }
+    __syncthreads();
+    if (!inv) {
+        plane_lines<N1, N2>(pl, tw, true, false);
+        plane_lines<N1, N2>(pl, tw, false, false);
+    } else {
+        plane_lines<N1, N2>(pl, tw, false, true);
+        plane_lines<N1, N2>(pl, tw, true, true);
+    }
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+        const int y = e / N, z = e - y * N;
+        data[base + e] = pl[plane_slot<N1, N2>(y) * RS + plane_slot<N1, N2>(z)];
+    }
+}
+
+// Launches the plane kernel when Ny = Nz has a specialisation; false otherwise.
+static bool fft_yz(fsd_handle* h, bool inv, int ngrids, const float2* twyz) {
+    const int Nx = h->g.Nx, N = h->g.Ny;
+    if (h->g.Nz != N) return false;
+    const size_t shm = sizeof(float2) * ((size_t)N + (size_t)N * (N + 1));
+    const int nblocks = ngrids * Nx;
+    auto go = [&](auto kern) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+            attr = true;
+        }
+        count_launch();
+        kern<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, twyz, inv);
+    };
+    switch (N) {
+        case 72: go(k_fft_yz<8, 9>); return true;
+        case 36: go(k_fft_yz<4, 9>); return true;
+        case 27: go(k_fft_yz<3, 9>); return true;
+        default: return false;
+    }
+}
+
 static int fft_batch_z(int Nx, int Ny, int Nz) {
     // Batches must not straddle two grids: pick B dividing Nx*Ny.
     int B = std::max(1, 2048 / Nz);
@@ -294,14 +408,19 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids, bool skip_x = false) {
         count_launch();
         k_fft_axis<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, Ny, Nz, axis, B, pl, tw, inv, ngrids);
     };
+    // y and z twiddles coincide when Ny = Nz (both tables are exp(-2 pi i m / N)).
     if (!inv) {
-        launch(2);
-        launch(1);
+        if (!fft_yz(h, false, ngrids, twz)) {
+            launch(2);
+            launch(1);
+        }
         if (!skip_x) launch(0);
     } else {
         if (!skip_x) launch(0);
-        launch(1);
-        launch(2);
+        if (!fft_yz(h, true, ngrids, twz)) {
+            launch(1);
+            launch(2);
+        }
     }
 }
 
@@ -688,16 +807,23 @@ struct SpreadArgs {
 
 constexpr int kSpreadCap = 384;  // staged particles per pass
 
-struct StagedParticle {
+struct __align__(16) StagedParticle {  // read as four float4: (x, y, z, o), v[0:4], v[4:8], v[8:12]
     float x, y, z;
     int o;  // origin within the extended tile, packed (ox | oy << 10 | oz << 20)
     float v[12];
 };
 
+// Grid nodes of a tile gather from the particles staged in shared memory in
+// cell order; cell_off[c] is the first staged index of extended cell c (the
+// launch's dynamic shared memory, ncell + 1 entries).  The particles that
+// reach a node are those whose stencil origin lies in the P^3 cells below
+// it: for each of its P x P (x, y) rows a contiguous range of P cells, so a
+// node visits exactly its contributors, in staged order.
 __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     __shared__ StagedParticle sp[kSpreadCap];
     __shared__ unsigned scan_sh[32];
     __shared__ unsigned s_total;
+    extern __shared__ unsigned cell_off[];
     const int P = a.P;
     const int ntx = (a.Nx + a.TX - 1) / a.TX, nty = (a.Ny + a.TY - 1) / a.TY;
     int bid = blockIdx.x;
@@ -713,10 +839,12 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     const int cpt = (ncell + nth - 1) / nth;  // extended cells per thread, contiguous
     // Count staged particles per thread (deterministic order: cell order, then bin order).
     unsigned mycount = 0;
-    for (int c = threadIdx.x * cpt; c < min(ncell, (threadIdx.x + 1) * cpt); ++c) {
+    const int c_begin = threadIdx.x * cpt, c_end = min(ncell, (threadIdx.x + 1) * cpt);
+    for (int c = c_begin; c < c_end; ++c) {
         const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
         const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
         const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
+        cell_off[c] = mycount;  // offset within this thread's cells; the block offset is added below
         mycount += a.bin_start[bin + 1] - a.bin_start[bin];
     }
     // Block exclusive scan of counts.
@@ -742,6 +870,8 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     __syncthreads();
     const unsigned myoff = (wid ? scan_sh[wid - 1] : 0u) + x - mycount;
     const unsigned total = s_total;
+    for (int c = c_begin; c < c_end; ++c) cell_off[c] += myoff;
+    if (threadIdx.x == 0) cell_off[ncell] = total;
 
     // This thread's node.
     const int lz = threadIdx.x % a.TZ, ly = (threadIdx.x / a.TZ) % a.TY, lx = threadIdx.x / (a.TZ * a.TY);
@@ -780,18 +910,30 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
             }
         }
         __syncthreads();
-        const int nst = (int)min((unsigned)kSpreadCap, total - chunk);
+        const unsigned cend = chunk + min((unsigned)kSpreadCap, total - chunk);
         if (active) {
-            for (int q = 0; q < nst; ++q) {
-                const int o = sp[q].o;
-                const int dx = lx + P - 1 - (o & 1023), dy = ly + P - 1 - ((o >> 10) & 1023),
-                          dz = lz + P - 1 - (o >> 20);
-                if ((unsigned)dx < (unsigned)P && (unsigned)dy < (unsigned)P && (unsigned)dz < (unsigned)P) {
-                    const float3 r = min_image(make_float3(pg.x - sp[q].x, pg.y - sp[q].y, pg.z - sp[q].z), a.box);
-                    const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
-                    const float wgt = a.prefac * expf(-a.expfac * rsq);
-#pragma unroll
-                    for (int c = 0; c < 11; ++c) acc[c] += wgt * sp[q].v[c];
+            for (int ix = 0; ix < P; ++ix) {
+                for (int iy = 0; iy < P; ++iy) {
+                    const int c0 = ((lx + ix) * EY + (ly + iy)) * EZ + lz;
+                    const unsigned q0 = max(cell_off[c0], chunk), q1 = min(cell_off[c0 + P], cend);
+                    for (unsigned q = q0; q < q1; ++q) {
+                        const float4* s4 = reinterpret_cast<const float4*>(&sp[q - chunk]);
+                        const float4 sx = s4[0], v0 = s4[1], v1 = s4[2], v2 = s4[3];
+                        const float3 r = min_image(make_float3(pg.x - sx.x, pg.y - sx.y, pg.z - sx.z), a.box);
+                        const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
+                        const float wgt = a.prefac * expf(-a.expfac * rsq);
+                        acc[0] += wgt * v0.x;
+                        acc[1] += wgt * v0.y;
+                        acc[2] += wgt * v0.z;
+                        acc[3] += wgt * v0.w;
+                        acc[4] += wgt * v1.x;
+                        acc[5] += wgt * v1.y;
+                        acc[6] += wgt * v1.z;
+                        acc[7] += wgt * v1.w;
+                        acc[8] += wgt * v2.x;
+                        acc[9] += wgt * v2.y;
+                        acc[10] += wgt * v2.z;
+                    }
                 }
             }
         }
@@ -875,6 +1017,7 @@ __global__ void __launch_bounds__(256) k_contract(const float4* __restrict__ pos
 // (Saddle_MakeGeneralizedU_kernel).
 struct RealArgs {
     const float4* pos;
+    const unsigned* order;  // particles in cell order
     const float4* f4;
     const float4* c4;
     const float* uwave;     // may be null
@@ -899,7 +1042,7 @@ __global__ void __launch_bounds__(128) k_real_combine(RealArgs a) {
     const int gl = threadIdx.x % kRealGroup;
     const int N = a.N;
     const bool valid = gid < N;
-    const int i = valid ? gid : N - 1;
+    const int i = (int)a.order[valid ? gid : N - 1];
     float u[3] = {0, 0, 0}, D[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (a.real) {
         const float4 pi = a.pos[i];
@@ -1062,8 +1205,9 @@ static void spread(fsd_handle* h, const float4* pos) {
     a.prefac = (2.0 * xisq / kPiRef / g.eta) * sqrtf(2.0 * xisq / kPiRef / g.eta);
     a.expfac = 2.0 * xisq / g.eta;
     const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
+    const size_t cell_bytes = sizeof(unsigned) * ((size_t)(a.TX + g.P - 1) * (a.TY + g.P - 1) * (a.TZ + g.P - 1) + 1);
     count_launch();
-    k_spread<<<ntiles, a.TX * a.TY * a.TZ, 0, h->stream>>>(a);
+    k_spread<<<ntiles, a.TX * a.TY * a.TZ, cell_bytes, h->stream>>>(a);
 }
 
 static void contract(fsd_handle* h, const float4* pos) {
@@ -1092,6 +1236,7 @@ void mobility_combine(fsd_handle* h, const float4* pos, const float* genF, float
     (void)genF;
     RealArgs r;
     r.pos = pos;
+    r.order = h->w.order;
     r.f4 = h->w.f4;
     r.c4 = h->w.c4;
     r.uwave = wave ? h->w.uwave : nullptr;

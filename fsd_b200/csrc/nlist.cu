@@ -239,6 +239,7 @@ int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host) {
         count_launch();
         k_nlist_cells<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, nc, w.part_cell, w.cell_start, w.cell_parts,
                                                        rlist2, w.nneigh, w.nlist, w.nl_stride, w.nl_overflow);
+        FSD_CHECK_CUDA(cudaMemcpyAsync(w.order, w.cell_parts, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, st));
     } else {
         count_launch();
         k_nlist_allpairs<<<(n + 127) / 128, 128, 0, st>>>(pos, n, h->box, rlist2, w.nneigh, w.nlist, w.nl_stride,
@@ -248,6 +249,51 @@ int build_neighbor_list(fsd_handle* h, const float4* pos, int* max_count_host) {
     FSD_CHECK_CUDA(cudaMemcpyAsync(w.host_flag, w.nl_overflow, sizeof(int), cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaStreamSynchronize(st));
     *max_count_host = *w.host_flag;
+    return FSD_OK;
+}
+
+__global__ void k_iota(unsigned* v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = (unsigned)i;
+}
+
+int init_particle_order(fsd_handle* h) {
+    count_launch();
+    k_iota<<<(h->p.N + 255) / 256, 256, 0, h->stream>>>(h->w.order, h->p.N);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// Entries of each particle's neighbour list closer than sqrt(r2), in list
+// order (so pair sums over them add in the same order as over the full list).
+__global__ void k_sublist(const float4* __restrict__ pos, int n, Box b, const unsigned* __restrict__ nneigh,
+                          const unsigned* __restrict__ nlist, int stride, float r2, unsigned* __restrict__ sub_n,
+                          unsigned* __restrict__ sub) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 pi = pos[i];
+    const unsigned* row = nlist + (size_t)i * stride;
+    unsigned* out = sub + (size_t)i * stride;
+    const unsigned nn = nneigh[i];
+    unsigned k = 0;
+    for (unsigned q = 0; q < nn; ++q) {
+        const unsigned j = row[q];
+        const float4 pj = pos[j];
+        const float3 r = min_image(make_float3(pj.x - pi.x, pj.y - pi.y, pj.z - pi.z), b);
+        if (r.x * r.x + r.y * r.y + r.z * r.z < r2) out[k++] = j;
+    }
+    sub_n[i] = k;
+}
+
+// The lubrication kernels' list: pairs within rlub plus the list buffer, so
+// the sub-list stays complete for as long as the full list does.
+int build_lub_list(fsd_handle* h, const float4* pos) {
+    Workspace& w = h->w;
+    const float r = h->p.rlub + h->p.nlist_buffer;
+    count_launch();
+    k_sublist<<<(h->p.N + 127) / 128, 128, 0, h->stream>>>(pos, h->p.N, h->box, w.nneigh, w.nlist, w.nl_stride,
+                                                           r * r, w.lub_n, w.lub_list);
+    FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
 }
 

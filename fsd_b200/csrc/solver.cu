@@ -412,7 +412,7 @@ __device__ double tentative_resid(const double* col, int c, double hsub, const d
 // commits column j or leaves it pending.  Every block computes the same
 // coefficients.  Only the last block touches the state after every block has
 // read `done`; its serial work runs on shared-memory copies.
-__global__ void __launch_bounds__(kRedThreads, 4) k_dcgs_update(float* V, size_t ld, int j, const float* __restrict__ w,
+__global__ void __launch_bounds__(kRedThreads, 2) k_dcgs_update(float* V, size_t ld, int j, const float* __restrict__ w,
                                                              size_t n, const double* __restrict__ dots,
                                                              GmresState* s, int m, double* part, unsigned* ticket) {
     if (s->done) return;
@@ -666,7 +666,7 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
                     k_finish_dots<<<(2 * (j + 1) + 7) / 8, 256, 0, st>>>(part, nbl, 2 * (j + 1), dots, false,
                                                                          &gs->done);
                     count_launch();
-                    k_dcgs_update<<<vblocks, kRedThreads, 0, st>>>(V, ld, j, Ax, n, dots, gs, m, part, w.ticket);
+                    k_dcgs_update<<<2 * 148, kRedThreads, 0, st>>>(V, ld, j, Ax, n, dots, gs, m, part, w.ticket);
                     if ((j % 4) == 3 || j == m - 1) {
                         count_launch();
                         k_export<<<1, 1, 0, st>>>(gs, gh);
