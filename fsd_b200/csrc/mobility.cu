@@ -583,71 +583,57 @@ __global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gr
 // then the planes z = 0 (and z = Nz / 2 for even Nz), pairing y with -y.
 // Every line lies in exactly one block.  The Green step itself is that of
 // k_green (same unpacking, Nyquist averaging and choice of representative).
-__global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ grid, const float4* __restrict__ gridk,
-                                                    int Nx, int Ny, int Nz, int B, int nzc, FFTPlan pl,
-                                                    const float2* __restrict__ tw_global) {
-    extern __shared__ float2 smem[];
-    __shared__ int ly[64], lz[64], lmir[64];
-    __shared__ int s_nl, s_np;  // lines, primary lines (whose points start the pairs)
-    const int n = Nx;
-    float2* tw = smem;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_global[i];
-    const size_t G = (size_t)Nx * Ny * Nz;
-    if (threadIdx.x == 0) {
-        int nl = 0, np = 0;
-        const int bid = blockIdx.x;
-        if (bid < Ny * nzc) {
-            const int y = bid / nzc, c = bid % nzc;
-            const int h = (Nz + 1) / 2;
-            const int z0 = 1 + c * B, z1 = min(h, z0 + B);
-            const int ym = (Ny - y) % Ny;
-            const int cnt = z1 - z0;
-            for (int k = 0; k < cnt; ++k) {
-                ly[k] = y;
-                lz[k] = z0 + k;
-                lmir[k] = cnt + k;
-                ly[cnt + k] = ym;
-                lz[cnt + k] = Nz - (z0 + k);
-                lmir[cnt + k] = k;
-            }
-            nl = 2 * cnt;
-            np = cnt;
-        } else {
-            const int pb = bid - Ny * nzc;
-            const int ny_half = Ny / 2 + 1;  // y in [0, Ny/2]
-            const int zplane = (pb < ny_half) ? 0 : Nz / 2;
-            const int y = (pb < ny_half) ? pb : pb - ny_half;
-            const int ym = (Ny - y) % Ny;
-            ly[0] = y;
-            lz[0] = zplane;
-            if (ym != y) {
-                ly[1] = ym;
-                lz[1] = zplane;
-                lmir[0] = 1;
-                lmir[1] = 0;
-                nl = 2;
-            } else {
-                lmir[0] = 0;
-                nl = 1;
-            }
-            np = 1;
+// Line set of fused x-pass block `bid`: ly/lz of each line and its mirror
+// line; returns (lines, primary lines).
+__device__ __forceinline__ int2 x_green_lines(int bid, int Ny, int Nz, int B, int nzc, int* ly, int* lz, int* lmir) {
+    int nl = 0, np = 0;
+    if (bid < Ny * nzc) {
+        const int y = bid / nzc, c = bid % nzc;
+        const int h = (Nz + 1) / 2;
+        const int z0 = 1 + c * B, z1 = min(h, z0 + B);
+        const int ym = (Ny - y) % Ny;
+        const int cnt = z1 - z0;
+        for (int k = 0; k < cnt; ++k) {
+            ly[k] = y;
+            lz[k] = z0 + k;
+            lmir[k] = cnt + k;
+            ly[cnt + k] = ym;
+            lz[cnt + k] = Nz - (z0 + k);
+            lmir[cnt + k] = k;
         }
-        s_nl = nl;
-        s_np = np;
+        nl = 2 * cnt;
+        np = cnt;
+    } else {
+        const int pb = bid - Ny * nzc;
+        const int ny_half = Ny / 2 + 1;  // y in [0, Ny/2]
+        const int zplane = (pb < ny_half) ? 0 : Nz / 2;
+        const int y = (pb < ny_half) ? pb : pb - ny_half;
+        const int ym = (Ny - y) % Ny;
+        ly[0] = y;
+        lz[0] = zplane;
+        if (ym != y) {
+            ly[1] = ym;
+            lz[1] = zplane;
+            lmir[0] = 1;
+            lmir[1] = 0;
+            nl = 2;
+        } else {
+            lmir[0] = 0;
+            nl = 1;
+        }
+        np = 1;
     }
-    __syncthreads();
-    const int nl = s_nl, np = s_np;
-    const int L6 = 6 * nl;  // lines in shared memory: grid-major
-    float2* a = smem + n;
-    float2* b = a + (size_t)L6 * n;
-    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
-        const int x = i / L6, q = i - x * L6;  // consecutive threads: consecutive lines (z runs)
-        const int g = q / nl, l = q - g * nl;
-        a[(size_t)q * n + x] = grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]];
-    }
-    __syncthreads();
-    float2* res = fft_lines(a, b, L6, pl, tw, false);
-    // Green's function on the mirror pairs.
+    return make_int2(nl, np);
+}
+
+// Green's function on the mirror pairs of the spectra held in shared memory:
+// line q (grid-major, q = p * nl + l) has row stride ls, and coefficient x of
+// a line sits at slot(x).
+template <class Slot>
+__device__ __forceinline__ void x_green_pairs(float2* res, int nl, int np, int ls, Slot slot, const int* ly,
+                                              const int* lz, const int* lmir, const float4* __restrict__ gridk,
+                                              int Nx, int Ny, int Nz) {
+    const int n = Nx;
     for (int t = threadIdx.x; t < np * n; t += blockDim.x) {
         const int l = t / n, x = t - l * n;
         const int lm = lmir[l];
@@ -665,15 +651,16 @@ __global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ gri
             ml = l;
             mx = x;
         }
+        const int ps = slot(sx), pm = slot(mx);
         float2 ck[6], cm[6], f[11], o[11];
 #pragma unroll
         for (int p = 0; p < 6; ++p) {
-            ck[p] = res[(size_t)(p * nl + sl) * n + sx];
-            cm[p] = res[(size_t)(p * nl + ml) * n + mx];
+            ck[p] = res[(size_t)(p * nl + sl) * ls + ps];
+            cm[p] = res[(size_t)(p * nl + ml) * ls + pm];
         }
         if (idx == 0) {
 #pragma unroll
-            for (int p = 0; p < 6; ++p) res[(size_t)(p * nl + sl) * n + sx] = make_float2(0.f, 0.f);
+            for (int p = 0; p < 6; ++p) res[(size_t)(p * nl + sl) * ls + ps] = make_float2(0.f, 0.f);
             continue;
         }
 #pragma unroll
@@ -695,10 +682,44 @@ __global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ gri
         for (int p = 0; p < 6; ++p) {
             const float2 A = o[packA(p)];
             const float2 Bv = (packB(p) >= 0) ? o[packB(p)] : make_float2(0.f, 0.f);
-            res[(size_t)(p * nl + sl) * n + sx] = make_float2(A.x - Bv.y, A.y + Bv.x);
-            if (m != idx) res[(size_t)(p * nl + ml) * n + mx] = make_float2(A.x + Bv.y, -A.y + Bv.x);
+            res[(size_t)(p * nl + sl) * ls + ps] = make_float2(A.x - Bv.y, A.y + Bv.x);
+            if (m != idx) res[(size_t)(p * nl + ml) * ls + pm] = make_float2(A.x + Bv.y, -A.y + Bv.x);
         }
     }
+}
+
+struct IdentitySlot {
+    __device__ int operator()(int x) const { return x; }
+};
+
+__global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ grid, const float4* __restrict__ gridk,
+                                                    int Nx, int Ny, int Nz, int B, int nzc, FFTPlan pl,
+                                                    const float2* __restrict__ tw_global) {
+    extern __shared__ float2 smem[];
+    __shared__ int ly[64], lz[64], lmir[64];
+    __shared__ int s_nl, s_np;  // lines, primary lines (whose points start the pairs)
+    const int n = Nx;
+    float2* tw = smem;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_global[i];
+    const size_t G = (size_t)Nx * Ny * Nz;
+    if (threadIdx.x == 0) {
+        const int2 c = x_green_lines(blockIdx.x, Ny, Nz, B, nzc, ly, lz, lmir);
+        s_nl = c.x;
+        s_np = c.y;
+    }
+    __syncthreads();
+    const int nl = s_nl, np = s_np;
+    const int L6 = 6 * nl;  // lines in shared memory: grid-major
+    float2* a = smem + n;
+    float2* b = a + (size_t)L6 * n;
+    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
+        const int x = i / L6, q = i - x * L6;  // consecutive threads: consecutive lines (z runs)
+        const int g = q / nl, l = q - g * nl;
+        a[(size_t)q * n + x] = grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]];
+    }
+    __syncthreads();
+    float2* res = fft_lines(a, b, L6, pl, tw, false);
+    x_green_pairs(res, nl, np, n, IdentitySlot(), ly, lz, lmir, gridk, Nx, Ny, Nz);
     __syncthreads();
     float2* other = (res == a) ? b : a;
     float2* out = fft_lines(res, other, L6, pl, tw, true);
@@ -706,6 +727,104 @@ __global__ void __launch_bounds__(256, 3) k_fft_x_green(float2* __restrict__ gri
         const int x = i / L6, q = i - x * L6;
         const int g = q / nl, l = q - g * nl;
         grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]] = out[(size_t)q * n + x];
+    }
+}
+
+// Length-N1*N2 transforms of nlines rows (row stride ls) in place: forward
+// leaves coefficient k = k2 + N2 k1 at slot k1 + N1 k2; the inverse runs the
+// adjoint stages in reverse order, from that order back to natural order.
+template <int N1, int N2>
+__device__ __forceinline__ void rows_fwd(float2* buf, int nlines, int ls, const float2* tw) {
+    for (int t = threadIdx.x; t < nlines * N1; t += blockDim.x) {
+        const int l = t % nlines, n1 = t / nlines;
+        float2* L = buf + l * ls + n1;
+        float2 y[N2];
+#pragma unroll
+        for (int q = 0; q < N2; ++q) y[q] = L[q * N1];
+        small_dft<N2>(y, false);
+#pragma unroll
+        for (int q = 0; q < N2; ++q) L[q * N1] = q == 0 ? y[0] : cmul(y[q], tw[n1 * q]);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nlines * N2; t += blockDim.x) {
+        const int l = t % nlines, k2 = t / nlines;
+        float2* L = buf + l * ls + k2 * N1;
+        float2 y[N1];
+#pragma unroll
+        for (int q = 0; q < N1; ++q) y[q] = L[q];
+        small_dft<N1>(y, false);
+#pragma unroll
+        for (int q = 0; q < N1; ++q) L[q] = y[q];
+    }
+    __syncthreads();
+}
+
+template <int N1, int N2>
+__device__ __forceinline__ void rows_inv(float2* buf, int nlines, int ls, const float2* tw) {
+    for (int t = threadIdx.x; t < nlines * N2; t += blockDim.x) {
+        const int l = t % nlines, k2 = t / nlines;
+        float2* L = buf + l * ls + k2 * N1;
+        float2 y[N1];
+#pragma unroll
+        for (int q = 0; q < N1; ++q) y[q] = L[q];
+        small_dft<N1>(y, true);
+#pragma unroll
+        for (int q = 0; q < N1; ++q) L[q] = y[q];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < nlines * N1; t += blockDim.x) {
+        const int l = t % nlines, n1 = t / nlines;
+        float2* L = buf + l * ls + n1;
+        float2 y[N2];
+#pragma unroll
+        for (int q = 0; q < N2; ++q) y[q] = q == 0 ? L[0] : cmul(L[q * N1], conjf2(tw[n1 * q]));
+        small_dft<N2>(y, true);
+#pragma unroll
+        for (int q = 0; q < N2; ++q) L[q * N1] = y[q];
+    }
+    __syncthreads();
+}
+
+template <int N1, int N2>
+struct DigitSlot {
+    __device__ int operator()(int x) const { return x / N2 + N1 * (x % N2); }
+};
+
+// The fused x-pass for Nx = N1 * N2: one shared buffer, rows padded to N + 1.
+template <int N1, int N2>
+__global__ void __launch_bounds__(256, 2) k_fft_x_green_t(float2* __restrict__ grid, const float4* __restrict__ gridk,
+                                                          int Ny, int Nz, int B, int nzc,
+                                                          const float2* __restrict__ tw_global) {
+    constexpr int n = N1 * N2, LS = n + 1;
+    extern __shared__ float2 smem[];
+    __shared__ int ly[64], lz[64], lmir[64];
+    __shared__ int s_nl, s_np;
+    float2* tw = smem;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tw[i] = tw_global[i];
+    const size_t G = (size_t)n * Ny * Nz;
+    if (threadIdx.x == 0) {
+        const int2 c = x_green_lines(blockIdx.x, Ny, Nz, B, nzc, ly, lz, lmir);
+        s_nl = c.x;
+        s_np = c.y;
+    }
+    __syncthreads();
+    const int nl = s_nl, np = s_np;
+    const int L6 = 6 * nl;
+    float2* a = smem + n;
+    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
+        const int x = i / L6, q = i - x * L6;
+        const int g = q / nl, l = q - g * nl;
+        a[(size_t)q * LS + x] = grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]];
+    }
+    __syncthreads();
+    rows_fwd<N1, N2>(a, L6, LS, tw);
+    x_green_pairs(a, nl, np, LS, DigitSlot<N1, N2>(), ly, lz, lmir, gridk, n, Ny, Nz);
+    __syncthreads();
+    rows_inv<N1, N2>(a, L6, LS, tw);
+    for (int i = threadIdx.x; i < L6 * n; i += blockDim.x) {
+        const int x = i / L6, q = i - x * L6;
+        const int g = q / nl, l = q - g * nl;
+        grid[(size_t)g * G + ((size_t)x * Ny + ly[l]) * Nz + lz[l]] = a[(size_t)q * LS + x];
     }
 }
 
@@ -722,6 +841,23 @@ static void fft_x_green(fsd_handle* h) {
     const int nplanes = (Nz % 2 == 0) ? 2 : 1;
     const int nblocks = Ny * nzc + nplanes * (Ny / 2 + 1);
     const size_t shm = sizeof(float2) * ((size_t)Nx + 2 * 12 * (size_t)B * Nx);
+    // Specialised line lengths keep one padded buffer (rows of Nx + 1).
+    const size_t shm_t = sizeof(float2) * ((size_t)Nx + 12 * (size_t)B * (Nx + 1));
+    auto go = [&](auto kern) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+            attr = true;
+        }
+        count_launch();
+        kern<<<nblocks, 256, shm_t, h->stream>>>(h->w.grid, h->w.gridk, Ny, Nz, B, nzc, h->w.twiddle);
+    };
+    switch (Nx) {
+        case 72: go(k_fft_x_green_t<8, 9>); return;
+        case 36: go(k_fft_x_green_t<4, 9>); return;
+        case 27: go(k_fft_x_green_t<3, 9>); return;
+        default: break;
+    }
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_fft_x_green, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
