@@ -130,7 +130,7 @@ def region_bytes(name, N, G, pairs_real, pairs_lub):
     """Algorithmic DRAM bytes of one launch of a single-kernel region (DESIGN.md
     lists the per-unit figures): each array the kernel must read or write once."""
     if name == "fft":
-        return 2 * 6 * G * 8  # one axis pass over the 6 packed complex grids, read + write
+        return 2 * 6 * G * 8  # y+z plane pass over the 6 packed complex grids, read + write once
     if name == "spread":
         return N * (16 + 48) + 6 * G * 8
     if name == "contract":
@@ -144,7 +144,10 @@ def region_bytes(name, N, G, pairs_real, pairs_lub):
     return None
 
 
-SINGLE_KERNEL_REGIONS = {"fft": 3, "spread": 1, "contract": 1, "green": 1, "real_space": 1, "rfu": 1}
+# Launches per region entry: on the 72^3 grid each FFT region (z+y forward or
+# y+z inverse) is one plane-kernel launch, and the x pass with the Green step
+# is one launch.
+SINGLE_KERNEL_REGIONS = {"fft": 1, "spread": 1, "contract": 1, "green": 1, "real_space": 1, "rfu": 1}
 WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_precond.f32"
 
 
