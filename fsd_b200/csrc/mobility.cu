@@ -939,6 +939,11 @@ struct SpreadArgs {
     int TX, TY, TZ;
     float hx, hy, hz;
     float prefac, expfac;
+    // Tile-relative separations: a staged particle keeps min_image(node(tile
+    // origin) - p) and a node adds its fixed offset within the tile.  Valid
+    // when the tile plus the stencil spans well under half the box on every
+    // axis (so that sum is the minimum image itself); set by the host.
+    bool local;
 };
 
 constexpr int kSpreadCap = 384;  // staged particles per pass
@@ -955,7 +960,7 @@ struct __align__(16) StagedParticle {  // read as four float4: (x, y, z, o), v[0
 // reach a node are those whose stencil origin lies in the P^3 cells below
 // it: for each of its P x P (x, y) rows a contiguous range of P cells, so a
 // node visits exactly its contributors, in staged order.
-__global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
+__global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     __shared__ StagedParticle sp[kSpreadCap];
     __shared__ unsigned scan_sh[32];
     __shared__ unsigned s_total;
@@ -968,6 +973,12 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     const int ty = bid % nty;
     const int tz = bid / nty;
     const int x0 = tx * a.TX, y0 = ty * a.TY, z0 = tz * a.TZ;
+    const float Ld2x0 = a.box.Lx / 2.0f, Ld2y0 = a.box.Ly / 2.0f, Ld2z0 = a.box.Lz / 2.0f;
+    float3 pg0;  // position of the tile's origin node
+    pg0.x = a.hx * x0 - Ld2x0;
+    pg0.y = a.hy * y0 - Ld2y0;
+    pg0.z = a.hz * z0 - Ld2z0;
+    pg0.x = pg0.x + a.box.xy * pg0.y;
     const int EX = a.TX + P - 1, EY = a.TY + P - 1, EZ = a.TZ + P - 1;
     const int ex0 = x0 - (P - 1), ey0 = y0 - (P - 1), ez0 = z0 - (P - 1);
     const int ncell = EX * EY * EZ;
@@ -1019,6 +1030,8 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     pg.y = a.hy * ny - Ld2y;
     pg.z = a.hz * nz - Ld2z;
     pg.x = pg.x + a.box.xy * pg.y;
+    // offset of this node from the tile origin (the grid is sheared with the box)
+    const float3 dn = make_float3(a.hx * lx + a.box.xy * (a.hy * ly), a.hy * ly, a.hz * lz);
     float acc[11];
 #pragma unroll
     for (int c = 0; c < 11; ++c) acc[c] = 0.0f;
@@ -1035,9 +1048,16 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
                 const unsigned p = a.bin_parts[q];
                 StagedParticle& s = sp[k - chunk];
                 const float4 ps = a.pos[p];
-                s.x = ps.x;
-                s.y = ps.y;
-                s.z = ps.z;
+                if (a.local) {
+                    const float3 d = min_image(make_float3(pg0.x - ps.x, pg0.y - ps.y, pg0.z - ps.z), a.box);
+                    s.x = d.x;
+                    s.y = d.y;
+                    s.z = d.z;
+                } else {
+                    s.x = ps.x;
+                    s.y = ps.y;
+                    s.z = ps.z;
+                }
                 s.o = cx | (cy << 10) | (cz << 20);
                 const float4 f = a.f4[p], c0 = a.c4[2 * p], c1 = a.c4[2 * p + 1];
                 // pairs: (Fx,Fy) (Cxx,Cxy) (Cxz,Cyx) (Cyy,Cyz) (Czx,Czy) (Fz,0)
@@ -1055,7 +1075,8 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
                     for (unsigned q = q0; q < q1; ++q) {
                         const float4* s4 = reinterpret_cast<const float4*>(&sp[q - chunk]);
                         const float4 sx = s4[0], v0 = s4[1], v1 = s4[2], v2 = s4[3];
-                        const float3 r = min_image(make_float3(pg.x - sx.x, pg.y - sx.y, pg.z - sx.z), a.box);
+                        const float3 r = a.local ? make_float3(sx.x + dn.x, sx.y + dn.y, sx.z + dn.z)
+                                                 : min_image(make_float3(pg.x - sx.x, pg.y - sx.y, pg.z - sx.z), a.box);
                         const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
                         const float wgt = a.prefac * expf(-a.expfac * rsq);
                         acc[0] += wgt * v0.x;
@@ -1340,6 +1361,11 @@ static void spread(fsd_handle* h, const float4* pos) {
     const float xisq = h->p.xi * h->p.xi;
     a.prefac = (2.0 * xisq / kPiRef / g.eta) * sqrtf(2.0 * xisq / kPiRef / g.eta);
     a.expfac = 2.0 * xisq / g.eta;
+    // Node-particle separations stay below (T + P) cells per axis, plus the
+    // tilt's x shift; below half the box they are their own minimum image.
+    const float tilt = 1.0f + fabsf(h->box.xy);
+    a.local = (a.TX + g.P) * tilt < 0.5f * g.Nx && (a.TY + g.P) * tilt < 0.5f * g.Ny &&
+              (a.TZ + g.P) * tilt < 0.5f * g.Nz;
     const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
     const size_t cell_bytes = sizeof(unsigned) * ((size_t)(a.TX + g.P - 1) * (a.TY + g.P - 1) * (a.TZ + g.P - 1) + 1);
     count_launch();

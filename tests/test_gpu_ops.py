@@ -98,10 +98,12 @@ def test_wave_space_mobility(cuda, case):
 
 
 @pytest.mark.parametrize("N,phi,xy,seed", [(1000, 0.2, 0.0, 1), (400, 0.35, 0.45, 2), (8192, 0.1, 0.0, 3),
-                                            (1024, 0.1, 0.3, 4)])
+                                            (1024, 0.1, 0.3, 4), (8000, 0.1, 0.2, 5)])
 def test_full_mobility(cuda, N, phi, xy, seed):
-    """Grids 27^3, 18^3, 72^3 and 36^3: the y and z FFT passes run as one plane
-    kernel for 27, 36 and 72 and as separate line passes for 18."""
+    """Grids 27^3, 18^3, 72^3, 36^3 and a tilted 72^3: the y and z FFT passes run
+    as one plane kernel for 27, 36 and 72 and as separate line passes for 18;
+    spreading uses tile-relative separations on the two 72^3 grids and the
+    per-node minimum image on the others."""
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
     s, p = solver_for(pos, L, xy)
