@@ -1,0 +1,85 @@
+"""BASELINE config 3 (N = 131072 at phi = 0.3, grid 120^3, applied forces and
+torques ~ N(0, 1), shear rate 0.5).
+
+* Its 4096-particle sub-box (L = 38.53, grid 40^3) against the FP64 oracle: the
+  full mobility to 5e-5, the same bar as the other mobility cases.
+* The full size, where the oracle does not reach, through properties that do
+  not depend on size: the mobility is symmetric and positive along random
+  probes, and linear; the saddle solve with the learned preconditioner reaches
+  1e-4 in true residual.
+
+The full-size configuration is a jittered simple cubic lattice at the same
+density (spacing 2.40, jitter at most 0.15 per axis, so every gap is at least
+0.1). Random sequential addition at this size takes a minute on the host.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ewald_golden
+from fsd_b200.configs import suspension
+from fsd_b200.core import FSD
+from oracle import fsd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64)) / np.linalg.norm(b))
+
+
+def lattice(N, phi, seed):
+    L = (4.0 * np.pi * N / (3.0 * phi)) ** (1.0 / 3.0)
+    n = int(np.ceil(N ** (1.0 / 3.0)))
+    h = L / n
+    g = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), -1).reshape(-1, 3)[:N]
+    jit = np.random.default_rng(seed).uniform(-0.15, 0.15, (N, 3))
+    xyz = (g + 0.5) * h - 0.5 * L + jit
+    pos = np.zeros((N, 4), np.float32)
+    pos[:, :3] = xyz
+    return pos, float(L)
+
+
+def test_config3_subbox_mobility_matches_oracle(cuda):
+    N = 4096
+    pos, Lc = suspension(N, 0.3, 3)
+    s = FSD(N, (Lc, Lc, Lc, 0.0))
+    assert (s.pse_info().Nx, s.pse_info().Ny, s.pse_info().Nz) == (40, 40, 40)
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    s.build_neighbor_list(p)
+    F = np.random.default_rng(31).standard_normal(11 * N)
+    F[6 * N:] = 0.0  # applied forces and torques only, as in the config
+    got = s.mobility(p, torch.as_tensor(F, dtype=torch.float32).cuda()).cpu().numpy()
+    pr = O.Problem(pos, (Lc, Lc, Lc), table=ewald_golden())
+    assert rel(got, pr.mobility(F)) < 5e-5
+    s.close()
+
+
+def test_config3_full_size_properties(cuda):
+    N = 131072
+    pos, L = lattice(N, 0.3, 32)
+    s = FSD(N, (L, L, L, 0.0), T=0.0, dt=1e-4, solver_tol=1e-4, precond="learned", learned_inner=6,
+            gmres_restart=100, gmres_max_iter=3000)
+    assert s.pse_info().Nx == 120
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    s.build_neighbor_list(p)
+    rng = np.random.default_rng(33)
+    u = torch.as_tensor(rng.standard_normal(11 * N), dtype=torch.float32).cuda()
+    v = torch.as_tensor(rng.standard_normal(11 * N), dtype=torch.float32).cuda()
+    Mu = s.mobility(p, u).double()
+    Mv = s.mobility(p, v).double()
+    Muv = s.mobility(p, u + 2.0 * v).double()
+    ud, vd = u.double(), v.double()
+    uMv, vMu = float(ud @ Mv), float(vd @ Mu)
+    assert abs(uMv - vMu) <= 1e-5 * float(ud.norm() * Mv.norm())
+    assert float(vd @ Mv) > 0 and float(ud @ Mu) > 0
+    assert float((Muv - Mu - 2.0 * Mv).norm() / Muv.norm()) < 1e-5
+    s.precond_build(p)
+    rhs = torch.as_tensor(rng.standard_normal(17 * N), dtype=torch.float32).cuda()
+    x, it, res, st = s.saddle_solve(p, rhs)
+    assert st == 0 and res <= 1e-4 and 0 < it < 3000
+    r = rhs.double() - s.saddle_multiply(p, x).double()
+    assert float(r.norm() / rhs.double().norm()) <= 2e-4
+    s.close()
