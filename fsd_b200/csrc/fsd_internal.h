@@ -4,7 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fsd.h"
@@ -129,6 +132,24 @@ struct Workspace {
     double* lz_dot = nullptr;      // device dot results
     double* lz_host = nullptr;     // pinned host copies
 };
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  Function attributes are per device, so the record is kept
+// per (kernel, device); limits at or below the 48 KiB default need no call.
+inline cudaError_t ensure_smem_limit(const void* func, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> set;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = set[std::make_pair(func, dev)];
+    if (cur >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 }  // namespace fsd
 
 // Launch shapes chosen by the autotuner (0 = built-in defaults).

@@ -348,11 +348,7 @@ static bool fft_yz(fsd_handle* h, bool inv, int ngrids, const float2* twyz) {
     const size_t shm = sizeof(float2) * ((size_t)N + (size_t)N * (N + 1));
     const int nblocks = ngrids * Nx;
     auto go = [&](auto kern) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-            attr = true;
-        }
+        ensure_smem_limit((const void*)kern, shm);
         count_launch();
         kern<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, twyz, inv);
     };
@@ -400,11 +396,7 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids, bool skip_x = false) {
         else
             nblocks = ngrids * (axis == 1 ? Nx : Ny) * ((Nz + B - 1) / B);
         const size_t shm = sizeof(float2) * ((size_t)pl.n + 2 * (size_t)B * pl.n);
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaFuncSetAttribute(k_fft_axis, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            attr_set = true;
-        }
+        ensure_smem_limit((const void*)k_fft_axis, shm);
         count_launch();
         k_fft_axis<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, Ny, Nz, axis, B, pl, tw, inv, ngrids);
     };
@@ -844,11 +836,7 @@ static void fft_x_green(fsd_handle* h) {
     // Specialised line lengths keep one padded buffer (rows of Nx + 1).
     const size_t shm_t = sizeof(float2) * ((size_t)Nx + 12 * (size_t)B * (Nx + 1));
     auto go = [&](auto kern) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
-            attr = true;
-        }
+        ensure_smem_limit((const void*)kern, shm_t);
         count_launch();
         kern<<<nblocks, 256, shm_t, h->stream>>>(h->w.grid, h->w.gridk, Ny, Nz, B, nzc, h->w.twiddle);
     };
@@ -858,11 +846,7 @@ static void fft_x_green(fsd_handle* h) {
         case 27: go(k_fft_x_green_t<3, 9>); return;
         default: break;
     }
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_fft_x_green, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
-        attr_set = true;
-    }
+    ensure_smem_limit((const void*)k_fft_x_green, shm);
     count_launch();
     k_fft_x_green<<<nblocks, 256, shm, h->stream>>>(h->w.grid, h->w.gridk, Nx, Ny, Nz, B, nzc, px, h->w.twiddle);
 }

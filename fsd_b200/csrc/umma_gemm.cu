@@ -392,12 +392,8 @@ static size_t dx_smem(int O, int K) { return (size_t)(kRows + K) * O * 2; }
 
 void umma_gemm(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* Wt, int O,
                const float* bias, int relu, const float* resid, float* Y, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_umma_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem(192, 64));
-        cudaFuncSetAttribute(k_umma_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dx_smem(64, 256));
-        attr = true;
-    }
+    ensure_smem_limit((const void*)k_umma_fwd, fwd_smem(192, 64));
+    ensure_smem_limit((const void*)k_umma_dx, dx_smem(64, 256));
     Parts in{};
     for (int i = 0; i < parts; ++i) {
         in.p[i] = p[i];
@@ -409,22 +405,14 @@ void umma_gemm(const float* const* p, const int* const* idx, int width, int part
 }
 
 void umma_gemm_dx(const float* dY, int rows, int O, const float* Wt, int K, float* dX, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_umma_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem(192, 64));
-        cudaFuncSetAttribute(k_umma_dx, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dx_smem(64, 256));
-        attr = true;
-    }
+    ensure_smem_limit((const void*)k_umma_fwd, fwd_smem(192, 64));
+    ensure_smem_limit((const void*)k_umma_dx, dx_smem(64, 256));
     k_umma_dx<<<(rows + kRows - 1) / kRows, kThreads, dx_smem(O, K), st>>>(dY, rows, O, Wt, K, dX);
 }
 
 void umma_gemm_dw(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* dY,
                   int O, float* dW, float* db, float* part, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_umma_dw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dw_smem(256, 64));
-        attr = true;
-    }
+    ensure_smem_limit((const void*)k_umma_dw, dw_smem(256, 64));
     Parts in{};
     for (int i = 0; i < parts; ++i) {
         in.p[i] = p[i];
