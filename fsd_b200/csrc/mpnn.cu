@@ -1060,12 +1060,18 @@ bool mpnn_loaded(fsd_handle* h) {
 void mpnn_use_umma(fsd_handle* h, bool on) { mp(h)->use_umma = on; }
 
 // Inference: graph, forward, head -> correction added to the approximate
-// inverse (precond_build of FSD_PRECOND_LEARNED, after spai_build).
+// inverse (precond_build of FSD_PRECOND_LEARNED, after spai_build).  With
+// the tensor-core layers, a commit wait that ran out is reported here.
 int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist,
                const float* a_blocks) {
     MP_TRY(mp_graph(h, pos, a_pn, a_plist, a_blocks));
     MP_TRY(mp_forward(h));
-    return mp_head(h);
+    MP_TRY(mp_head(h));
+    if (mp(h)->use_umma) {
+        FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        if (umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
+    }
+    return FSD_OK;
 }
 
 // Loss and gradient for given probes z (host P x 6N), or for z = w - A G0 w
