@@ -517,55 +517,6 @@ __device__ __forceinline__ void green_apply(const float4 tk, const float2* f, fl
 __host__ __device__ constexpr int packA(int p) { return p == 0 ? 0 : p == 1 ? 3 : p == 2 ? 5 : p == 3 ? 7 : p == 4 ? 9 : 2; }
 __host__ __device__ constexpr int packB(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 6 : p == 3 ? 8 : p == 4 ? 10 : -1; }
 
-// One thread per mirror pair {k, -k}: unpack the 11 spectra of the real grids,
-// apply the Green's function (averaged with the mirror operator where the
-// mirror wave vector is not -k, i.e. on Nyquist planes, which reproduces the
-// real part the reference keeps after its complex inverse transform), repack.
-__global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gridk, int Nx, int Ny, int Nz) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int G = Nx * Ny * Nz;
-    if (idx >= G) return;
-    const int i = idx / (Ny * Nz), j = (idx / Nz) % Ny, l = idx % Nz;
-    const int im = (Nx - i) % Nx, jm = (Ny - j) % Ny, lm = (Nz - l) % Nz;
-    const int m = (im * Ny + jm) * Nz + lm;
-    if (m < idx) return;
-    float2 f[11], o[11];
-    float2 cm[6], ck[6];
-#pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        ck[p] = grid[(size_t)p * G + idx];
-        cm[p] = grid[(size_t)p * G + m];
-    }
-#pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        // A = (C(k) + conj C(m)) / 2 ; B = -i (C(k) - conj C(m)) / 2
-        const float2 A = make_float2(0.5f * (ck[p].x + cm[p].x), 0.5f * (ck[p].y - cm[p].y));
-        const float2 Bv = make_float2(0.5f * (ck[p].y + cm[p].y), -0.5f * (ck[p].x - cm[p].x));
-        f[packA(p)] = A;
-        if (packB(p) >= 0) f[packB(p)] = Bv;
-    }
-    if (idx == 0) {
-#pragma unroll
-        for (int p = 0; p < 6; ++p) grid[(size_t)p * G] = make_float2(0.f, 0.f);
-        return;
-    }
-    green_apply(gridk[idx], f, o, 1.0f);
-    const bool nyq = (2 * i == Nx) || (2 * j == Ny) || (2 * l == Nz);
-    if (nyq) {
-        float2 o2[11];
-        green_apply(gridk[m], f, o2, -1.0f);
-#pragma unroll
-        for (int c = 0; c < 11; ++c) o[c] = make_float2(0.5f * (o[c].x + o2[c].x), 0.5f * (o[c].y + o2[c].y));
-    }
-#pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        const float2 A = o[packA(p)];
-        const float2 Bv = (packB(p) >= 0) ? o[packB(p)] : make_float2(0.f, 0.f);
-        // C_out(k) = A + i B ; C_out(m) = conj A + i conj B
-        grid[(size_t)p * G + idx] = make_float2(A.x - Bv.y, A.y + Bv.x);
-        if (m != idx) grid[(size_t)p * G + m] = make_float2(A.x + Bv.y, -A.y + Bv.x);
-    }
-}
 
 // Forward x-pass, Green's function and inverse x-pass in one kernel.  A block
 // holds, for all 6 packed grids, a set of x-lines closed under the mirror map
@@ -573,8 +524,7 @@ __global__ void k_green(float2* __restrict__ grid, const float4* __restrict__ gr
 // shared memory.  Blocks [0, Ny * nzc): line y with the z-run
 // {1 + c B, ..} inside [1, ceil(Nz / 2)) and the mirrored lines (-y, -z);
 // then the planes z = 0 (and z = Nz / 2 for even Nz), pairing y with -y.
-// Every line lies in exactly one block.  The Green step itself is that of
-// k_green (same unpacking, Nyquist averaging and choice of representative).
+// Every line lies in exactly one block.
 // Line set of fused x-pass block `bid`: ly/lz of each line and its mirror
 // line; returns (lines, primary lines).
 __device__ __forceinline__ int2 x_green_lines(int bid, int Ny, int Nz, int B, int nzc, int* ly, int* lz, int* lmir) {
@@ -618,9 +568,15 @@ __device__ __forceinline__ int2 x_green_lines(int bid, int Ny, int Nz, int B, in
     return make_int2(nl, np);
 }
 
-// Green's function on the mirror pairs of the spectra held in shared memory:
-// line q (grid-major, q = p * nl + l) has row stride ls, and coefficient x of
-// a line sits at slot(x).
+// Green's function on the mirror pairs {k, -k} of the spectra held in shared
+// memory: line q (grid-major, q = p * nl + l) has row stride ls, and
+// coefficient x of a line sits at slot(x).  Each pair unpacks the 11 spectra
+// of the real grids from the 6 packed complex ones (A = (C(k) + conj C(m)) / 2,
+// B = -i (C(k) - conj C(m)) / 2), applies the Green's function (averaged with
+// the mirror operator where the mirror wave vector is not -k, i.e. on Nyquist
+// planes, which reproduces the real part the reference keeps after its
+// complex inverse transform) and repacks (C(k) = A + i B, C(m) = conj A +
+// i conj B).  The smaller global index represents the pair; k = 0 is zeroed.
 template <class Slot>
 __device__ __forceinline__ void x_green_pairs(float2* res, int nl, int np, int ls, Slot slot, const int* ly,
                                               const int* lz, const int* lmir, const float4* __restrict__ gridk,
@@ -634,7 +590,7 @@ __device__ __forceinline__ void x_green_pairs(float2* res, int nl, int np, int l
         size_t idx = ((size_t)x * Ny + ly[l]) * Nz + lz[l];
         size_t m = ((size_t)xm * Ny + ly[lm]) * Nz + lz[lm];
         int sl = l, sx = x, ml = lm, mx = xm;
-        if (m < idx) {  // the smaller global index represents the pair, as in k_green
+        if (m < idx) {  // the smaller global index represents the pair
             const size_t tmp = idx;
             idx = m;
             m = tmp;
