@@ -517,7 +517,6 @@ __device__ __forceinline__ void green_apply(const float4 tk, const float2* f, fl
 __host__ __device__ constexpr int packA(int p) { return p == 0 ? 0 : p == 1 ? 3 : p == 2 ? 5 : p == 3 ? 7 : p == 4 ? 9 : 2; }
 __host__ __device__ constexpr int packB(int p) { return p == 0 ? 1 : p == 1 ? 4 : p == 2 ? 6 : p == 3 ? 8 : p == 4 ? 10 : -1; }
 
-
 // Forward x-pass, Green's function and inverse x-pass in one kernel.  A block
 // holds, for all 6 packed grids, a set of x-lines closed under the mirror map
 // (y, z) -> (-y, -z), so both points of every mirror pair {k, -k} are in
