@@ -524,6 +524,7 @@ __host__ __device__ constexpr int packB(int p) { return p == 0 ? 1 : p == 1 ? 4 
 // {1 + c B, ..} inside [1, ceil(Nz / 2)) and the mirrored lines (-y, -z);
 // then the planes z = 0 (and z = Nz / 2 for even Nz), pairing y with -y.
 // Every line lies in exactly one block.
+
 // Line set of fused x-pass block `bid`: ly/lz of each line and its mirror
 // line; returns (lines, primary lines).
 __device__ __forceinline__ int2 x_green_lines(int bid, int Ny, int Nz, int B, int nzc, int* ly, int* lz, int* lmir) {
