@@ -1,5 +1,5 @@
-"""BASELINE config 3 (N = 131072 at phi = 0.3, grid 120^3, applied forces and
-torques ~ N(0, 1), shear rate 0.5).
+"""The large suspension: N = 131072 at phi = 0.3 (grid 120^3), applied forces
+and torques ~ N(0, 1), shear rate 0.5.
 
 * Its 4096-particle sub-box (L = 38.53, grid 40^3) against the FP64 oracle: the
   full mobility to 5e-5, the same bar as the other mobility cases.
@@ -42,7 +42,7 @@ def lattice(N, phi, seed):
     return pos, float(L)
 
 
-def test_config3_subbox_mobility_matches_oracle(cuda):
+def test_subbox_n4096_mobility_matches_oracle(cuda):
     N = 4096
     pos, Lc = suspension(N, 0.3, 3)
     s = FSD(N, (Lc, Lc, Lc, 0.0))
@@ -57,7 +57,7 @@ def test_config3_subbox_mobility_matches_oracle(cuda):
     s.close()
 
 
-def test_config3_full_size_properties(cuda):
+def test_n131072_mobility_properties_and_solve(cuda):
     N = 131072
     pos, L = lattice(N, 0.3, 32)
     s = FSD(N, (L, L, L, 0.0), T=0.0, dt=1e-4, solver_tol=1e-4, precond="learned", learned_inner=6,

@@ -1,6 +1,7 @@
 """Velocities and stresslets of one velocity computation (fsd_compute_velocity,
-Integrator_ComputeVelocity at kT = 0) against the FP64 oracle: BASELINE
-config 1 (N = 1000 at phi = 0.2, no shear) and a sheared, tilted dense case.
+Integrator_ComputeVelocity at kT = 0) against the FP64 oracle: the dilute
+suspension of N = 1000 at phi = 0.2 without shear, and a sheared, tilted
+dense case.
 GMRES runs to 1e-6 (5e-7 for the dense sheared case, whose small relative
 velocities amplify the solver's residual: 1e-6 leaves 1.005e-4 there, 5e-7
 leaves 4.5e-5) so that solver error stays under the 1e-4 bar on velocities
