@@ -478,6 +478,15 @@ int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_
 
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x) {
     if (!h || !h->pc_valid || !d_b || !d_x) return FSD_ERR_BAD_PARAMS;
+    // Some applications gather b from neighbouring particles while writing x
+    // (the approximate inverse applied once), so overlapping vectors go
+    // through a copy.  The saddle work vector is free outside a solve.
+    const size_t n17 = 17 * (size_t)h->p.N;
+    const bool overlap = d_b < d_x + n17 && d_x < d_b + n17;
+    if (overlap) {
+        FSD_CHECK_CUDA(cudaMemcpyAsync(h->w.sz, d_b, sizeof(float) * n17, cudaMemcpyDeviceToDevice, h->stream));
+        d_b = h->w.sz;
+    }
     return precond_apply(h, d_b, d_x);
 }
 
