@@ -24,6 +24,25 @@ def test_weight_layout_matches_library():
     assert _lib.lib().fsd_learned_num_weights() == M.layout()[1]
 
 
+def test_approximate_inverse_is_optimal_for_isotropic_probes():
+    """The two-hop approximate inverse minimises ||A G - I||_F on its pattern,
+    which is the loss over isotropic probes (exact here: Z = I); a network
+    correction on the same pattern can only raise it, quadratically in its
+    size (no descent direction at G0)."""
+    N = 60
+    pos, Lc = suspension(N, 0.4, 7)
+    pr = M.problem(pos, (Lc, Lc, Lc), 0.0)
+    Z = np.eye(6 * N)
+    base = M.loss(M.init_weights(0, head_scale=0.0), pr, Z)
+    rng = np.random.default_rng(5)
+    for _ in range(3):
+        seed = int(rng.integers(1 << 30))
+        small = M.loss(M.init_weights(seed, head_scale=1e-4), pr, Z) - base
+        large = M.loss(M.init_weights(seed, head_scale=1e-3), pr, Z) - base
+        assert small > 0 and large > 0
+        assert 30.0 < large / small < 300.0  # quadratic: x100 for x10
+
+
 def _setup(N=200, phi=0.35, seed=4):
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
