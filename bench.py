@@ -127,8 +127,8 @@ def peak_hbm():
 
 
 def region_bytes(name, N, G, pairs_real, pairs_lub):
-    """Algorithmic DRAM bytes of one launch of a single-kernel region (DESIGN.md
-    lists the per-unit figures): each array the kernel must read or write once."""
+    """Algorithmic DRAM bytes of one launch of a single-kernel region: each
+    array the kernel must read or write once."""
     if name == "fft":
         return 2 * 6 * G * 8  # y+z plane pass over the 6 packed complex grids, read + write once
     if name == "spread":

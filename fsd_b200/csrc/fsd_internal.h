@@ -150,6 +150,17 @@ inline cudaError_t ensure_smem_limit(const void* func, size_t bytes) {
     return e;
 }
 
+// ensure_smem_limit for launch sites without a status return: a failure is
+// recorded as the library's last CUDA error and the caller skips the launch
+// (the enclosing entry point then reports FSD_ERR_CUDA through its
+// cudaGetLastError check).
+inline bool smem_limit_ok(const void* func, size_t bytes, const char* what) {
+    const cudaError_t e = ensure_smem_limit(func, bytes);
+    if (e == cudaSuccess) return true;
+    set_last_cuda_error(e, what, __FILE__, __LINE__);
+    return false;
+}
+
 }  // namespace fsd
 
 // Launch shapes chosen by the autotuner (0 = built-in defaults).

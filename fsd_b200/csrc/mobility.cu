@@ -348,7 +348,7 @@ static bool fft_yz(fsd_handle* h, bool inv, int ngrids, const float2* twyz) {
     const size_t shm = sizeof(float2) * ((size_t)N + (size_t)N * (N + 1));
     const int nblocks = ngrids * Nx;
     auto go = [&](auto kern) {
-        ensure_smem_limit((const void*)kern, shm);
+        if (!smem_limit_ok((const void*)kern, shm, "k_fft_yz shared memory")) return;
         count_launch();
         kern<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, twyz, inv);
     };
@@ -396,7 +396,7 @@ static void fft3d(fsd_handle* h, bool inv, int ngrids, bool skip_x = false) {
         else
             nblocks = ngrids * (axis == 1 ? Nx : Ny) * ((Nz + B - 1) / B);
         const size_t shm = sizeof(float2) * ((size_t)pl.n + 2 * (size_t)B * pl.n);
-        ensure_smem_limit((const void*)k_fft_axis, shm);
+        if (!smem_limit_ok((const void*)k_fft_axis, shm, "k_fft_axis shared memory")) return;
         count_launch();
         k_fft_axis<<<nblocks, 256, shm, h->stream>>>(h->w.grid, Nx, Ny, Nz, axis, B, pl, tw, inv, ngrids);
     };
@@ -792,7 +792,7 @@ static void fft_x_green(fsd_handle* h) {
     // Specialised line lengths keep one padded buffer (rows of Nx + 1).
     const size_t shm_t = sizeof(float2) * ((size_t)Nx + 12 * (size_t)B * (Nx + 1));
     auto go = [&](auto kern) {
-        ensure_smem_limit((const void*)kern, shm_t);
+        if (!smem_limit_ok((const void*)kern, shm_t, "k_fft_x_green_t shared memory")) return;
         count_launch();
         kern<<<nblocks, 256, shm_t, h->stream>>>(h->w.grid, h->w.gridk, Ny, Nz, B, nzc, h->w.twiddle);
     };
@@ -802,7 +802,7 @@ static void fft_x_green(fsd_handle* h) {
         case 27: go(k_fft_x_green_t<3, 9>); return;
         default: break;
     }
-    ensure_smem_limit((const void*)k_fft_x_green, shm);
+    if (!smem_limit_ok((const void*)k_fft_x_green, shm, "k_fft_x_green shared memory")) return;
     count_launch();
     k_fft_x_green<<<nblocks, 256, shm, h->stream>>>(h->w.grid, h->w.gridk, Nx, Ny, Nz, B, nzc, px, h->w.twiddle);
 }

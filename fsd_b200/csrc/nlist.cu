@@ -344,7 +344,13 @@ int neighbor_list_noalloc(const float4* pos, int n, Box b, float rlist, unsigned
     const int e = noalloc_scratch(&scratch);
     if (e != FSD_OK) return e;
     const float rlist2 = rlist * rlist;
-    int3 nc = cell_dims(b, rlist);
+    // Cells per axis, clamped to the scratch's cell capacity before the
+    // conversion to int (a large box over a small r_list would overflow it).
+    const float wx = b.Lx / sqrtf(1.0f + b.xy * b.xy);
+    auto axis_cells = [](float len, float r) {
+        return (int)fminf(floorf(len / r), (float)kNoAllocMaxCells);
+    };
+    int3 nc = make_int3(axis_cells(wx, rlist), axis_cells(b.Ly, rlist), axis_cells(b.Lz, rlist));
     // Wider cells than r_list stay correct, so a box with more cells than the
     // scratch holds uses fewer, wider cells along its longest cell axis.
     while ((size_t)nc.x * nc.y * nc.z > (size_t)kNoAllocMaxCells) {

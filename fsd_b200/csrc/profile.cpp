@@ -15,6 +15,7 @@ struct Profiler {
     std::vector<std::pair<int, int>> pairs[R_COUNT];  // recorded (start, end) slots
     double ms[R_COUNT] = {};
     long long count[R_COUNT] = {};
+    long long dropped = 0;  // regions not timed because no event could be had
 };
 
 static Profiler* prof(fsd_handle* h) { return (Profiler*)h->profiler; }
@@ -33,12 +34,18 @@ static void resolve(fsd_handle* h) {
     p->next = 0;
 }
 
+// Next free event.  A full pool is resolved (one stream synchronisation) when
+// no region is open; with regions open it grows instead, so no region is lost.
 static int take(fsd_handle* h) {
     Profiler* p = prof(h);
     bool busy = false;
     for (int r = 0; r < R_COUNT; ++r) busy |= !p->open[r].empty();
     if (p->next >= p->pool.size() && !busy) resolve(h);
-    if (p->next >= p->pool.size()) return -1;
+    if (p->next >= p->pool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return -1;
+        p->pool.push_back(e);
+    }
     return (int)p->next++;
 }
 
@@ -46,7 +53,10 @@ void profile_begin(fsd_handle* h, int region) {
     Profiler* p = prof(h);
     if (!p || !p->on) return;
     const int e = take(h);
-    if (e < 0) return;
+    if (e < 0) {
+        ++p->dropped;
+        return;
+    }
     cudaEventRecord(p->pool[e], h->stream);
     p->open[region].push_back(e);
 }
@@ -57,7 +67,10 @@ void profile_end(fsd_handle* h, int region) {
     const int s = p->open[region].back();
     p->open[region].pop_back();
     const int e = take(h);
-    if (e < 0) return;
+    if (e < 0) {
+        ++p->dropped;
+        return;
+    }
     cudaEventRecord(p->pool[e], h->stream);
     p->pairs[region].push_back({s, e});
 }
@@ -102,6 +115,11 @@ int fsd_profile_read(fsd_handle* h, double* ms, long long* counts, int n, int re
             p->ms[r] = 0.0;
             p->count[r] = 0;
         }
+    }
+    if (n > R_COUNT) {
+        ms[R_COUNT] = 0.0;
+        counts[R_COUNT] = p->dropped;
+        if (reset) p->dropped = 0;
     }
     return FSD_OK;
 }

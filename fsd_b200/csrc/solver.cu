@@ -609,7 +609,7 @@ int saddle_solve(fsd_handle* h, const float4* pos, const float* b, float* x, flo
     const size_t pair_smem = 2 * chunk4 * sizeof(float);
     const bool delayed = pair_smem <= 200 * 1024;
     if (delayed && pair_smem > 48 * 1024)
-        FSD_CHECK_CUDA(cudaFuncSetAttribute(k_dots_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pair_smem));
+        FSD_CHECK_CUDA(ensure_smem_limit((const void*)k_dots_pair, pair_smem));
     auto multidot = [&](const float* Vb, size_t ldv, int nv, const float* wv, size_t nn, double* pt, const int* dn) {
         if (staged)
             k_multidot_ws<<<nbl, kRedThreads, chunk * sizeof(float), st>>>(Vb, ldv, nv, wv, nn, chunk, pt, dn);

@@ -255,8 +255,7 @@ int spai_build(fsd_handle* h) {
         FSD_CHECK_CUDA(cudaMalloc(&s->sp_bucket, sizeof(int) * (size_t)kBuckets * N));
         FSD_CHECK_CUDA(cudaMalloc(&s->sp_cnt, sizeof(unsigned) * (kBuckets + 2)));
         FSD_CHECK_CUDA(cudaMallocHost(&s->sp_host, sizeof(unsigned) * 4));
-        FSD_CHECK_CUDA(cudaFuncSetAttribute(k_spai_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)spai_smem(kBucketMax[kBuckets - 1])));
+        FSD_CHECK_CUDA(ensure_smem_limit((const void*)k_spai_solve, spai_smem(kBucketMax[kBuckets - 1])));
     }
     // counters: buckets [0, kBuckets), then truncated sets, then failed rows
     FSD_CHECK_CUDA(cudaMemsetAsync(s->sp_cnt, 0, sizeof(unsigned) * (kBuckets + 2), st));

@@ -392,8 +392,7 @@ static size_t dx_smem(int O, int K) { return (size_t)(kRows + K) * O * 2; }
 
 void umma_gemm(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* Wt, int O,
                const float* bias, int relu, const float* resid, float* Y, cudaStream_t st) {
-    ensure_smem_limit((const void*)k_umma_fwd, fwd_smem(192, 64));
-    ensure_smem_limit((const void*)k_umma_dx, dx_smem(64, 256));
+    if (!smem_limit_ok((const void*)k_umma_fwd, fwd_smem(192, 64), "k_umma_fwd shared memory")) return;
     Parts in{};
     for (int i = 0; i < parts; ++i) {
         in.p[i] = p[i];
@@ -405,14 +404,13 @@ void umma_gemm(const float* const* p, const int* const* idx, int width, int part
 }
 
 void umma_gemm_dx(const float* dY, int rows, int O, const float* Wt, int K, float* dX, cudaStream_t st) {
-    ensure_smem_limit((const void*)k_umma_fwd, fwd_smem(192, 64));
-    ensure_smem_limit((const void*)k_umma_dx, dx_smem(64, 256));
+    if (!smem_limit_ok((const void*)k_umma_dx, dx_smem(64, 256), "k_umma_dx shared memory")) return;
     k_umma_dx<<<(rows + kRows - 1) / kRows, kThreads, dx_smem(O, K), st>>>(dY, rows, O, Wt, K, dX);
 }
 
 void umma_gemm_dw(const float* const* p, const int* const* idx, int width, int parts, int rows, const float* dY,
                   int O, float* dW, float* db, float* part, cudaStream_t st) {
-    ensure_smem_limit((const void*)k_umma_dw, dw_smem(256, 64));
+    if (!smem_limit_ok((const void*)k_umma_dw, dw_smem(256, 64), "k_umma_dw shared memory")) return;
     Parts in{};
     for (int i = 0; i < parts; ++i) {
         in.p[i] = p[i];

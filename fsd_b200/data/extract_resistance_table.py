@@ -31,7 +31,9 @@ N_FUNC = 22
 
 
 def main() -> int:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "source" / "Stokes_ResistanceTable.cc"
+    # default: a sibling checkout named `reference` next to this repository
+    default = Path(__file__).resolve().parents[3] / "reference"
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else default) / "source" / "Stokes_ResistanceTable.cc"
     text = ref.read_text(errors="replace")
     dist = np.full(N_DIST, np.nan, np.float32)
     vals = np.full(N_DIST * N_FUNC, np.nan, np.float32)

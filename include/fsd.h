@@ -177,7 +177,9 @@ int fsd_get_pse_info(const fsd_handle* h, fsd_pse_info* info);
  * Regions, in order: neighbour list, preconditioner build, spread, FFT,
  * Green, contract, real space, R_FU, preconditioner apply, Krylov vector ops,
  * Lanczos vector ops, wave-space noise, other lubrication, integration.
- * fsd_profile_read fills ms[] and counts[] (n >= 14) and optionally resets. */
+ * fsd_profile_read fills ms[] and counts[] (n >= 14) and optionally resets;
+ * with n >= 15, counts[14] receives the number of regions left untimed
+ * because no CUDA event could be created (0 in normal operation). */
 int fsd_profile_enable(fsd_handle* h, int on);
 int fsd_profile_read(fsd_handle* h, double* ms, long long* counts, int n, int reset);
 int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info);
@@ -215,6 +217,9 @@ int fsd_get_neighbor_list(const fsd_handle* h, unsigned int* host_nneigh, unsign
  *
  * The first call on each device looks up the array's device address (with
  * that device current); make that first call before any stream capture.
+ * The address is kept for the life of the process: after cudaDeviceReset (or
+ * anything else that destroys the device's primary context) it is stale, so
+ * do not call this entry point on a device that was reset.
  * All calls on a device share the array: calls whose GPU work overlaps
  * (different streams without ordering between them) race and corrupt each
  * other's lists.  Order them on one stream or with events. */

@@ -1,7 +1,7 @@
 """Recipe: compile self-contained pieces of the reference for the host.
 
-Test infrastructure only.  It reads the reference checkout (default
-``/root/reference``; override with ``FSD_REFERENCE_DIR``), extracts the named
+Test infrastructure only.  It reads the reference checkout (``FSD_REFERENCE_DIR``,
+else a sibling directory ``reference`` next to this repository), extracts the named
 per-thread device functions and two host set-up blocks verbatim into
 ``oracle/_ref/`` (git-ignored), and compiles them together with
 ``ref_harness.cpp`` and the reference's standalone ``rcm.cpp`` into
@@ -24,7 +24,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "_ref"
-REF = Path(os.environ.get("FSD_REFERENCE_DIR", "/root/reference")) / "source"
+REF = Path(os.environ.get("FSD_REFERENCE_DIR", str(HERE.parents[2] / "reference"))) / "source"
 
 # (file, function name) for every device function compiled for the host.
 KERNELS = [

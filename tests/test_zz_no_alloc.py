@@ -70,6 +70,26 @@ def test_noalloc_matches_handle_list_on_two_calls_in_a_row(cuda):
 
 
 @pytest.mark.gpu
+def test_noalloc_wider_cells_when_the_cell_grid_exceeds_its_scratch(cuda):
+    """A 60-wide box over r_list = 1 would need 60^3 = 216000 cells, more than
+    the scratch's 65536: the call falls back to fewer, wider cells, which must
+    still give every pair (brute-force sets from the oracle)."""
+    from oracle import fsd_oracle as O
+    rng = np.random.default_rng(11)
+    N, Lc = 4000, 60.0
+    pos = np.zeros((N, 4), np.float32)
+    pos[:, :3] = (rng.random((N, 3)) - 0.5) * Lc
+    rlist = 1.0
+    ref = O.neighbor_list(pos, (Lc, Lc, Lc), 0.0, rlist)
+    stride = max(8, max(len(r) for r in ref) + 4)
+    for _ in range(2):  # twice in a row: nothing may carry over in the shared scratch
+        nneigh, nlist, mx = _noalloc(pos, (Lc, Lc, Lc), 0.0, rlist, stride)
+        assert mx == max(len(r) for r in ref)
+        got = _rows(nneigh, nlist, stride)
+        assert all(np.array_equal(a, np.sort(b)) for a, b in zip(got, ref))
+
+
+@pytest.mark.gpu
 def test_noalloc_reports_truncated_rows(cuda):
     pos, Lc = suspension(2000, 0.3, 7)
     L = (Lc, Lc, Lc)
