@@ -115,6 +115,8 @@ _SIGS = {
     "fsd_brownian_farfield": (C.c_int, [H, P, C.c_uint, P]),
     "fsd_brownian_nearfield": (C.c_int, [H, P, C.c_uint, P]),
     "fsd_rfd_drift": (C.c_int, [H, P, P, C.c_uint, P]),
+    "fsd_draw_normals": (C.c_int, [H, C.c_uint, C.c_uint, C.c_size_t, C.c_float, P]),
+    "fsd_integrate_euler": (C.c_int, [H, C.POINTER(fsd_step_args)]),
     "fsd_compute_velocity": (C.c_int, [H, C.POINTER(fsd_step_args)]),
     "fsd_step": (C.c_int, [H, C.POINTER(fsd_step_args)]),
     "fsd_step_batch": (C.c_int, [P, P, C.c_int, C.c_int, P]),

@@ -281,6 +281,21 @@ class FSD:
         check(lib().fsd_rfd_drift(self._h, _ptr(pos), _ptr(image), timestep, _ptr(out)), "fsd_rfd_drift")
         return out
 
+    def draw_normals(self, stream_id: int, timestep: int, n: int, scale: float = 1.0) -> torch.Tensor:
+        """The library's counter-based normals of one random stream (fsd_draw_normals)."""
+        self._sync_stream()
+        out = self._new(n)
+        check(lib().fsd_draw_normals(self._h, int(stream_id), int(timestep), int(n), float(scale), _ptr(out)),
+              "fsd_draw_normals")
+        return out
+
+    def integrate_euler(self, timestep, shear_rate, pos, ori, image, velocity, pos_gb=None, noise_ang=None,
+                        b1_mask=None):
+        """Euler + shear update from the velocity in `velocity` (fsd_integrate_euler)."""
+        self._sync_stream()
+        a = self._args(timestep, shear_rate, pos, ori, pos_gb, image, None, velocity, noise_ang, b1_mask, None)
+        return check(lib().fsd_integrate_euler(self._h, C.byref(a)), "fsd_integrate_euler")
+
     def step_args(self, timestep, shear_rate, pos, ori, image, force, velocity, pos_gb=None, noise_ang=None,
                   b1_mask=None, b2_mask=None):
         return self._args(timestep, shear_rate, pos, ori, pos_gb, image, force, velocity, noise_ang, b1_mask, b2_mask)

@@ -195,10 +195,9 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
     return lanczos_status;
 }
 
-int step(fsd_handle* h, const fsd_step_args* a) {
+// Euler + shear from the velocity in a->d_velocity (Integrator.cu:126-228).
+int integrate_euler(fsd_handle* h, const fsd_step_args* a) {
     const int N = h->p.N;
-    int e = compute_velocity(h, a);
-    if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
     ProfRegion pr(h, R_INTEGRATE);
     const float3* noise = (const float3*)a->d_noise_ang;
     if (!noise && h->p.rot_diff > 0.f) {
@@ -210,6 +209,14 @@ int step(fsd_handle* h, const fsd_step_args* a) {
                                                            a->d_velocity, h->p.sqm_B1, a->d_b1_mask, noise,
                                                            (int3*)a->d_image, N, h->box, h->p.dt, a->shear_rate);
     FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+int step(fsd_handle* h, const fsd_step_args* a) {
+    int e = compute_velocity(h, a);
+    if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+    const int ee = integrate_euler(h, a);
+    if (ee != FSD_OK) return ee;
     // Carried solver state (Stokes.cc:1658-1666).
     const unsigned t = a->timestep;
     if (t % 100 == 0 || h->m_lanczos_ff > 50) h->m_lanczos_ff = 3;
@@ -239,6 +246,21 @@ int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigne
     (void)d_image;
     if (!h || !h->nlist_valid || !h->pc_valid || !d_pos || !d_drift6) return FSD_ERR_BAD_PARAMS;
     return rfd_drift(h, (const float4*)d_pos, timestep, d_drift6);
+}
+
+int fsd_draw_normals(fsd_handle* h, unsigned int stream_id, unsigned int timestep, size_t n, float scale,
+                     float* d_out) {
+    if (!h || !d_out || stream_id < 1 || stream_id > kStreamRot) return FSD_ERR_BAD_PARAMS;
+    if (n == 0) return FSD_OK;
+    gaussian(h, d_out, n, timestep, stream_id, scale);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+int fsd_integrate_euler(fsd_handle* h, const fsd_step_args* a) {
+    if (!h || !a || !a->d_pos || !a->d_velocity || !a->d_image) return FSD_ERR_BAD_PARAMS;
+    h->nlist_valid = false;  // the particles move
+    return integrate_euler(h, a);
 }
 
 int fsd_compute_velocity(fsd_handle* h, const fsd_step_args* a) {

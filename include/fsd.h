@@ -292,6 +292,22 @@ int fsd_saddle_solve(fsd_handle* h, const float* d_pos, const float* d_rhs, floa
 int fsd_brownian_farfield(fsd_handle* h, const float* d_pos, unsigned int timestep, float* d_slip11);
 int fsd_brownian_nearfield(fsd_handle* h, const float* d_pos, unsigned int timestep, float* d_force6);
 int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigned int timestep, float* d_drift6);
+/* The normals behind those draws: n values of stream `stream_id` at
+ * `timestep`, times `scale`, from the counter-based Philox4x32-10 generator
+ * keyed by the handle's hashed seed.  Streams: 1 far-field real-space (11N),
+ * 2 wave-space field, 3 near-field (6N), 4 drift direction psi (6N),
+ * 5 rotational noise (3N).  The reference draws these with cuRAND
+ * (Integrator.cu:591-596, Brownian_FarField.cu:864-874,
+ * Brownian_NearField.cu:438-444), so this has no counterpart there; it lets a
+ * caller reproduce the noise of any step. */
+int fsd_draw_normals(fsd_handle* h, unsigned int stream_id, unsigned int timestep, size_t n, float scale,
+                     float* d_out);
+/* Explicit Euler update with simple shear, director rotation, image and
+ * unwrapped-position bookkeeping from the velocity already in a->d_velocity
+ * (Integrator_ExplicitEuler_Shear_kernel, Integrator.cu:126-228, launched at
+ * Stokes.cu:248).  Rotational noise comes from a->d_noise_ang, or is drawn
+ * from stream 5 when it is NULL and rot_diff > 0, as fsd_step does. */
+int fsd_integrate_euler(fsd_handle* h, const fsd_step_args* a);
 
 /* Velocities and stresslets for the current configuration without moving
  * particles (Integrator_ComputeVelocity, Integrator.cu:744). */

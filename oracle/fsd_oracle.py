@@ -23,6 +23,25 @@ F32 = np.float32
 
 _TABLE_BIN = Path(__file__).resolve().parents[1] / "fsd_b200" / "data" / "resistance_table.bin"
 
+# Host threads the oracle's FFTs may use (scipy.fft workers); 1 by default.
+FFT_WORKERS = 1
+
+
+def _fftn(a, axes, inverse=False):
+    import scipy.fft as sf
+    f = sf.ifftn if inverse else sf.fftn
+    return f(a, axes=axes, workers=FFT_WORKERS)
+
+
+def scatter_add(out, idx, vals):
+    """out[idx[k]] += vals[k] along the first axis (np.add.at semantics), by
+    bincount per trailing component."""
+    idx = np.asarray(idx).ravel()
+    v = np.asarray(vals, np.float64)
+    for c in np.ndindex(*out.shape[1:]):
+        out[(slice(None),) + c] += np.bincount(idx, weights=v[(slice(None),) + c], minlength=out.shape[0])
+    return out
+
 
 # ---------------------------------------------------------------------- data
 def resistance_table():
@@ -120,6 +139,25 @@ def neighbor_list(pos, L, xy, rlist):
         m[i] = False
         rows.append(np.nonzero(m)[0].astype(np.uint32))
     return rows
+
+
+def neighbor_list_kdtree(pos, L, rlist):
+    """neighbor_list for an untilted box by a k-d tree (same sorted rows;
+    for large N, where the all-pairs scan is slow)."""
+    from scipy.spatial import cKDTree
+    Lb = np.asarray(L, np.float64)
+    x = np.mod(xyz(pos) + Lb / 2, Lb)
+    x = np.where(x >= Lb, x - Lb, x)
+    pairs = cKDTree(x, boxsize=Lb).query_pairs(rlist, output_type="ndarray")
+    # query_pairs keeps d <= r; the list keeps d < r
+    d = min_image(xyz(pos)[pairs[:, 0]] - xyz(pos)[pairs[:, 1]], L, 0.0)
+    pairs = pairs[np.einsum("ij,ij->i", d, d) < rlist * rlist]
+    i = np.concatenate([pairs[:, 0], pairs[:, 1]])
+    j = np.concatenate([pairs[:, 1], pairs[:, 0]])
+    order = np.lexsort((j, i))
+    i, j = i[order], j[order]
+    starts = np.searchsorted(i, np.arange(len(x) + 1))
+    return [j[starts[k]:starts[k + 1]].astype(np.uint32) for k in range(len(x))]
 
 
 def pair_arrays(rows):
@@ -263,15 +301,15 @@ def wave_space(pos, F, C, L, xy, gp, xi, pi_typo=True):
     grids = np.zeros((12, G))
     vals = np.concatenate([F, C.reshape(N, 9)], 1)  # X Y Z, then C row-major
     for c in range(12):
-        np.add.at(grids[c], flat.ravel(), (wgt * vals[:, c:c + 1]).ravel())
-    spec = np.fft.fftn(grids.reshape(12, *Nxyz), axes=(1, 2, 3))
+        grids[c] += np.bincount(flat.ravel(), weights=(wgt * vals[:, c:c + 1]).ravel(), minlength=G)
+    spec = _fftn(grids.reshape(12, *Nxyz), (1, 2, 3))
     Fh = spec[:3]
     Ch = spec[3:].reshape(3, 3, *Nxyz)
     Ch[2, 2] = -(Ch[0, 0] + Ch[1, 1])
     kx, ky, kz, w = gridk(Nxyz, L, xy, xi, eta, pi_typo)
     Uh, Dh = green(Fh, Ch, kx, ky, kz, w)
-    Ur = np.fft.ifftn(Uh, axes=(1, 2, 3)).real * G
-    Dr = np.fft.ifftn(Dh, axes=(2, 3, 4)).real * G
+    Ur = _fftn(Uh, (1, 2, 3), inverse=True).real * G
+    Dr = _fftn(Dh, (2, 3, 4), inverse=True).real * G
     quadW = h[0] * h[1] * h[2]
     cw = quadW * wgt
     u = np.einsum("np,cnp->nc", cw, Ur.reshape(3, G)[:, flat])
@@ -324,8 +362,8 @@ def real_space(pos, F, C, L, xy, rows, table, self_x, self_y, ewald_cut, ewald_n
            + h2[:, None, None] * (R[:, :, None] * CR[:, None, :] - RCR[:, None, None] * RR)
            + h3[:, None, None] * (RCR[:, None, None] * I3 + CR[:, :, None] * R[:, None, :] + R[:, :, None] * RC[:, None, :]
                                   + RC[:, :, None] * R[:, None, :] - 6.0 * RCR[:, None, None] * RR - CT))
-    np.add.at(u, i, du)
-    np.add.at(D, i, dD)
+    scatter_add(u, i, du)
+    scatter_add(D, i, dD)
     return u, D
 
 
@@ -435,7 +473,7 @@ def rfu(pos, U6, L, xy, rows, tdist, tvals, rlub=4.0):
         + ((XC11 - YC11) * dot(r, wi))[:, None] * r + YC11[:, None] * wi \
         + ((XC12 - YC12) * dot(r, wj))[:, None] * r + YC12[:, None] * wj
     out = np.zeros((N, 6))
-    np.add.at(out, i, np.concatenate([F, T], 1))
+    scatter_add(out, i, np.concatenate([F, T], 1))
     return out.ravel()
 
 
@@ -455,7 +493,7 @@ def rfe(pos, shear_rate, L, xy, rows, tdist, tvals, ori=None, b2mask=None, B2=0.
         + ((XG21 - 2 * YG21) * -rErj)[:, None] * r - 2 * YG21[:, None] * Erj
     T = 2 * YH11[:, None] * np.cross(Eri, r) + 2 * YH12[:, None] * np.cross(Erj, r)
     out = np.zeros((N, 6))
-    np.add.at(out, i, np.concatenate([F, T], 1))
+    scatter_add(out, i, np.concatenate([F, T], 1))
     return out.ravel()
 
 
@@ -482,7 +520,7 @@ def rsu(pos, U6, L, xy, rows, tdist, tvals, rlub=4.0):
                    + YH11 * (r[:, a] * ewi[:, b] + ewi[:, a] * r[:, b])
                    + YH12 * (r[:, a] * ewj[:, b] + ewj[:, a] * r[:, b]))
     out = np.zeros((N, 5))
-    np.add.at(out, i, S)
+    scatter_add(out, i, S)
     return -out.ravel()
 
 
@@ -509,7 +547,7 @@ def rse(pos, shear_rate, L, xy, rows, tdist, tvals, ori=None, b2mask=None, B2=0.
                    + 0.5 * ZM12 * (2 * E[j][:, a, b] + (dab + r[:, a] * r[:, b]) * rErj
                                    - 2 * r[:, a] * Erj[:, b] - 2 * r[:, b] * Erj[:, a]))
     out = np.zeros((N, 5))
-    np.add.at(out, i, S)
+    scatter_add(out, i, S)
     return out.ravel()
 
 
@@ -518,7 +556,7 @@ class Problem:
     """Everything the oracle needs about one configuration."""
 
     def __init__(self, pos, L, xy=0.0, xi=0.5, error=1e-3, max_strain=0.5, table=None, rlub=4.0, rp=2.1,
-                 pi_typo=True):
+                 pi_typo=True, rows=None):
         self.pos = xyz(pos)
         self.N = len(self.pos)
         self.L = tuple(float(v) for v in L)
@@ -528,7 +566,7 @@ class Problem:
         if table is None:
             raise ValueError("an Ewald table (reference golden or harness) is required")
         self.table, self.self_x, self.self_y, self.ewald_cut, self.ewald_n = table
-        self.rows = neighbor_list(self.pos, self.L, self.xy, self.ewald_cut + 0.4)
+        self.rows = rows if rows is not None else neighbor_list(self.pos, self.L, self.xy, self.ewald_cut + 0.4)
         self.tdist, self.tvals = resistance_table()
         self.rlub, self.rp = rlub, rp
         self.pi_typo = pi_typo
@@ -772,7 +810,7 @@ def pruned_rfu_sparse(pos, L, xy, tdist, tvals, rows=None, rp=2.1, relaxer=1.0):
     slf[:, 3:, :3] = w(YB11) * eps
     slf[:, 3:, 3:] = w(XC11) * rr + w(YC11) * Im
     diag = np.zeros((N, 6, 6))
-    np.add.at(diag, i, slf)
+    scatter_add(diag, i, slf)
     d = np.array([1.0, 1.0, 1.0] + [float(F32(1.33333333))] * 3)
     diag[:, np.arange(6), np.arange(6)] += relaxer * d
     bi = np.concatenate([i, np.arange(N)])
@@ -824,6 +862,26 @@ def spai2(A, N, cap=32):
             cols.append((6 * c + q).ravel())
             vals.append(X[6 * a:6 * a + 6].ravel())
     return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=A.shape)
+
+
+def spai2_columns(A, N, cols, cap=32):
+    """The blocks of spai2 in the given block columns only: {(s, c): 6x6}
+    for c in cols and every s whose set holds c (same rule as spai2)."""
+    import scipy.sparse as sp
+    Ab = sp.bsr_matrix(A, blocksize=(6, 6))
+    Ab.sort_indices()
+    sets = spai_sets(Ab, N, cap)
+    Ac = A.tocsc()
+    out = {}
+    for c in cols:
+        S = sets[c]
+        idx = np.concatenate([np.arange(6 * s, 6 * s + 6) for s in S])
+        As = Ac[:, idx].toarray()
+        X = np.linalg.solve(As.T @ As, As[6 * c:6 * c + 6].T)
+        for a, s in enumerate(S):
+            if c in sets[s]:
+                out[(s, c)] = X[6 * a:6 * a + 6]
+    return out
 
 
 def ichol0_dense(A, pattern):
@@ -880,7 +938,7 @@ def pair_force(pos, L, xy, rows, ndsr=0.1, k_n=1e4, kappa=20.0, beta=0.0, epsq=1
     m2 = gap < 0
     mag[m2] = H / (12.0 * epsq) - F0 - k_n * np.abs(gap[m2])
     out = np.zeros((N, 6))
-    np.add.at(out[:, :3], i, mag[:, None] * R / dist[:, None])
+    scatter_add(out[:, :3], i, mag[:, None] * R / dist[:, None])
     out[:, 5] = T_ext
     return out.ravel()
 

@@ -57,6 +57,64 @@ def test_subbox_n4096_mobility_matches_oracle(cuda):
     s.close()
 
 
+def test_subbox_n4096_velocity_and_stresslet_match_oracle(cuda):
+    """The precision study's sub-box: FP32 spreading, FFT and lubrication with
+    FP64 Krylov scalars against the FP64 oracle, for applied forces and torques
+    ~ N(0, 1) and shear rate 0.5 at kT = 0: velocities and stresslets to 1e-4
+    (GMRES to 5e-7, where the FP32 residual floor leaves a few 1e-5)."""
+    N, rate = 4096, 0.5
+    pos, Lc = suspension(N, 0.3, 3)
+    L = (Lc, Lc, Lc)
+    s = FSD(N, (Lc, Lc, Lc, 0.0), T=0.0, dt=1e-4, period=1, solver_tol=5e-7, precond="learned", learned_inner=6,
+            gmres_restart=100, gmres_max_iter=4000, force_mode="user")
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    Fu = np.random.default_rng(34).standard_normal(6 * N).astype(np.float32)
+    F = torch.as_tensor(Fu).cuda()
+    ori = torch.tensor([0.0, 0.0, 1.0], device="cuda").repeat(N)
+    img = torch.zeros(3 * N, dtype=torch.int32, device="cuda")
+    V = torch.zeros(11 * N, device="cuda")
+    s.compute_velocity(0, rate, p, ori, img, F, V)
+    v = V.cpu().numpy().astype(np.float64)
+    table = ewald_golden()
+    pr = O.Problem(pos, L, table=table, rows=O.neighbor_list_kdtree(pos, L, table[3] + 0.4))
+    rhs = O.strain_rhs(rate, N)
+    rhs[11 * N:] -= Fu
+    rhs[11 * N:] += O.rfe(pr.pos, rate, L, 0.0, pr.rows, pr.tdist, pr.tvals)
+    x = pr.solve(rhs, tol=1e-8)
+    U = x[11 * N:]
+    S = x[6 * N:11 * N] + O.rsu(pr.pos, U, L, 0.0, pr.rows, pr.tdist, pr.tvals) \
+        + O.rse(pr.pos, rate, L, 0.0, pr.rows, pr.tdist, pr.tvals)
+    eu, es = rel(v[:6 * N], U), rel(v[6 * N:], S)
+    print(f"sub-box N=4096 phi=0.3: velocity rel err {eu:.2e}, stresslet rel err {es:.2e}")
+    assert eu < 1e-4 and es < 1e-4
+    s.close()
+
+
+def test_subbox_n4096_lanczos_iterations_to_1e3(cuda):
+    """Brownian samples of the sub-box at the Lanczos tolerance 1e-3 against the
+    same draws converged to 1e-5: the far-field real-space square root and the
+    near-field R_FU square root each stay within 2e-3 of the converged sample,
+    and the iteration counts are reported.  (The covariance of the samples
+    against 2kT/dt M and 2kT/dt R_FU is checked in test_brownian.py.)"""
+    N = 4096
+    pos, Lc = suspension(N, 0.3, 3)
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    out = {}
+    for tol in (1e-3, 1e-5):
+        s = FSD(N, (Lc, Lc, Lc, 0.0), T=1.0, dt=1e-4, seed=5, lanczos_tol=tol, lanczos_max=100)
+        s.build_neighbor_list(p)
+        ff = s.brownian_farfield(p, 3).cpu().numpy()
+        nf = s.brownian_nearfield(p, 3).cpu().numpy()
+        info = s.solve_info()
+        out[tol] = (ff, nf, info["lanczos_ff_iters"], info["lanczos_nf_iters"])
+        s.close()
+    eff, enf = rel(out[1e-3][0], out[1e-5][0]), rel(out[1e-3][1], out[1e-5][1])
+    print(f"sub-box N=4096 Lanczos to 1e-3: far field {out[1e-3][2]} iterations (rel err {eff:.1e}), "
+          f"near field {out[1e-3][3]} iterations (rel err {enf:.1e}); to 1e-5: {out[1e-5][2]} / {out[1e-5][3]}")
+    assert eff < 2e-3 and enf < 2e-3
+    assert out[1e-3][2] < out[1e-5][2] and out[1e-3][3] < out[1e-5][3]
+
+
 def test_n131072_mobility_properties_and_solve(cuda):
     N = 131072
     pos, L = lattice(N, 0.3, 32)
