@@ -278,12 +278,22 @@ def run_fsd(args, ws, rank, local):
     # Per-region breakdown and the roofline's launch times: a separate pass over
     # the next steps of the same trajectory with the CUDA-event profiler on.
     prof = timed_steps(args, s, state, max(1, min(3, args.steps)), 0, dev, ws, profile=True)
-    # --- end to end through the C ABI with host buffers: every step uploads the
-    # state the previous step left in host memory and reads back the velocity
-    # and the new state, with the same L2 flush (outside the events) as above.
+    # --- end to end through the C ABI with host buffers: the same warm-up and
+    # timed steps of the same trajectory on a second handle (the step is
+    # deterministic, so the iteration counts repeat the headline's), every
+    # step uploading the state the previous step left in host memory and
+    # reading back the velocity and the new state, with the same L2 flush
+    # (outside the events) as above.
     e2e = None
     if not args.no_e2e:
-        p, ori, img, F, V, step_no = state
+        s.close()
+        s, _ = make_solver(args, args.precond, N, L, dev, 1 + rank)
+        p, ori, img, F, V, step_no = fresh_state()
+        for _ in range(args.warmup):
+            st = s.step(step_no[0], 1.0, p, ori, img, F, V, raise_on_error=False)
+            step_no[0] += 1
+            if st not in (0, 4):
+                raise RuntimeError(f"fsd_step status {st}")
         stream = torch.cuda.current_stream(dev)
         pin = lambda t: t.detach().cpu().pin_memory()
         h_pos, h_ori, h_img = pin(p), pin(ori), pin(img)

@@ -39,7 +39,7 @@ class fsd_params(C.Structure):
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
         ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
-        ("learned_inner", C.c_int), ("autotune", C.c_int),
+        ("learned_inner", C.c_int), ("learned_poly", C.c_int), ("autotune", C.c_int),
     ]
 
 
@@ -110,6 +110,10 @@ _SIGS = {
     "fsd_learned_get_state": (C.c_int, [H, P, C.c_int, C.POINTER(C.c_int)]),
     "fsd_learned_set_state": (C.c_int, [H, P, C.c_int, C.c_int]),
     "fsd_learned_train_step": (C.c_int, [H, P, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float), P]),
+    "fsd_learned_set_poly": (C.c_int, [H, P, C.c_int]),
+    "fsd_learned_get_poly": (C.c_int, [H, P, C.c_int]),
+    "fsd_learned_poly_train_step": (C.c_int, [H, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float),
+                                              C.POINTER(C.c_float), P, P, P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),
     "fsd_saddle_solve": (C.c_int, [H, P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "fsd_brownian_farfield": (C.c_int, [H, P, C.c_uint, P]),

@@ -228,6 +228,37 @@ class FSD:
         check(lib().fsd_learned_set_state(self._h, buf.ctypes.data_as(C.c_void_p), int(buf.size), int(t)),
               "fsd_learned_set_state")
 
+    def learned_set_poly(self, coef):
+        """Fixed Chebyshev coefficients of the inner polynomial (learned_poly mode)."""
+        c = np.ascontiguousarray(coef, np.float32)
+        check(lib().fsd_learned_set_poly(self._h, c.ctypes.data_as(C.c_void_p), int(c.size)), "fsd_learned_set_poly")
+
+    def learned_get_poly(self):
+        """(coefficients in use, spectral bound lambda of AG of the last build)."""
+        buf = np.zeros(17, np.float32)
+        check(lib().fsd_learned_get_poly(self._h, buf.ctypes.data_as(C.c_void_p), 17), "fsd_learned_get_poly")
+        k = self.params.learned_poly
+        return buf[:k].copy(), float(buf[16])
+
+    def learned_poly_train_step(self, pos, n_probes=4, step=0, lr=0.0, want_grad=False):
+        """Inner-polynomial loss of this configuration with the network's
+        coefficients, its least-squares optimum, both coefficient sets, the
+        weight gradient (when want_grad) and, for lr > 0, one Adam step."""
+        self._sync_stream()
+        k = self.params.learned_poly
+        loss, loss_opt = C.c_float(0.0), C.c_float(0.0)
+        coef, copt = np.zeros(k, np.float32), np.zeros(k, np.float32)
+        g = np.zeros(lib().fsd_learned_num_weights(), np.float32) if want_grad else None
+        check(lib().fsd_learned_poly_train_step(self._h, _ptr(pos), int(n_probes), int(step), float(lr),
+                                                C.byref(loss), C.byref(loss_opt),
+                                                g.ctypes.data_as(C.c_void_p) if want_grad else None,
+                                                coef.ctypes.data_as(C.c_void_p), copt.ctypes.data_as(C.c_void_p)),
+              "fsd_learned_poly_train_step")
+        out = {"loss": loss.value, "loss_opt": loss_opt.value, "coef": coef, "coef_opt": copt}
+        if want_grad:
+            out["grad"] = g
+        return out
+
     def learned_tensor_cores(self, on: bool):
         check(lib().fsd_learned_tensor_cores(self._h, int(bool(on))), "fsd_learned_tensor_cores")
 

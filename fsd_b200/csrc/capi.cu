@@ -181,6 +181,7 @@ void fsd_default_params(fsd_params* p) {
     p->ichol_local_shift = 1;
     p->ichol_gain_limit = 100.0f;
     p->learned_inner = 4;
+    p->learned_poly = 0;
 }
 
 const char* fsd_status_string(int status) {
@@ -246,6 +247,7 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
         return FSD_ERR_BAD_PARAMS;
     if (p->gmres_restart < 1 || p->gmres_restart > kMaxRestart || p->lanczos_max < 4) return FSD_ERR_BAD_PARAMS;
     if (p->learned_inner < 0 || p->learned_inner > kMaxInner) return FSD_ERR_BAD_PARAMS;
+    if (p->learned_poly < 0 || p->learned_poly == 1 || p->learned_poly > kMaxPoly) return FSD_ERR_BAD_PARAMS;
     fsd_handle* h = new fsd_handle();
     h->p = *p;
     h->stream = (cudaStream_t)stream;
@@ -468,6 +470,26 @@ int fsd_learned_tensor_cores(fsd_handle* h, int on) {
     if (!h) return FSD_ERR_BAD_PARAMS;
     mpnn_use_umma(h, on != 0);
     return FSD_OK;
+}
+
+int fsd_learned_set_poly(fsd_handle* h, const float* host_c, int k) {
+    if (!h) return FSD_ERR_BAD_PARAMS;
+    return poly_set_coefficients(h, host_c, k);
+}
+
+int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n) {
+    if (!h) return FSD_ERR_BAD_PARAMS;
+    return poly_get_coefficients(h, host_c, n);
+}
+
+int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
+                                float* loss, float* loss_opt, float* host_grad, float* host_coef,
+                                float* host_coef_opt) {
+    if (!h || !d_pos || !h->nlist_valid || n_probes < 1 || n_probes > 64) return FSD_ERR_BAD_PARAMS;
+    const int k = h->p.learned_poly;
+    if (k < 2) return FSD_ERR_BAD_PARAMS;
+    return mpnn_poly_train_step(h, (const float4*)d_pos, n_probes, step, lr, k, loss, loss_opt, host_grad, host_coef,
+                                host_coef_opt);
 }
 
 int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,

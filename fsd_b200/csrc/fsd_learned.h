@@ -43,6 +43,18 @@ struct LearnedState {
     const void* gkey[8] = {};
     int gkey_k = -1;
     int captures = 0;
+    // learned Chebyshev polynomial inner solve (poly.cu)
+    float* pc = nullptr;      // kMaxPoly coefficients, then the spectral bound lambda of AG
+    float* pbuf = nullptr;    // 5 x 6N: t, G products, three Clenshaw slots
+    double* ppart = nullptr;  // block partial sums of the power iteration
+    double* pnrm = nullptr;
+    unsigned* pticket = nullptr;
+    bool poly_user = false;   // coefficients set through fsd_learned_set_poly (else the network's)
+    cudaGraph_t pgraph = nullptr;
+    cudaGraphExec_t pexec = nullptr;
+    cudaGraphNode_t pnode_first = nullptr, pnode_last = nullptr;
+    const void* pkey[8] = {};
+    int pkey_k = -1;
 };
 
 LearnedState* learned(fsd_handle* h);
@@ -55,6 +67,15 @@ int learned_set_weights(fsd_handle* h, const float* host_w, int n);
 bool precond_is_flexible(const fsd_handle* h);
 int spai_build(fsd_handle* h);
 
+// poly.cu
+int poly_alloc(fsd_handle* h);
+void poly_free(LearnedState* s);
+bool poly_active(const fsd_handle* h);
+int poly_lambda(fsd_handle* h);
+int poly_apply(fsd_handle* h, const float* b, float* x);
+int poly_set_coefficients(fsd_handle* h, const float* host_c, int k);
+int poly_get_coefficients(fsd_handle* h, float* host_c, int n);
+
 // mpnn.cu
 void mpnn_free(fsd_handle* h);
 int mpnn_set_weights(fsd_handle* h, const float* host_w, int n);
@@ -66,5 +87,10 @@ void mpnn_use_umma(fsd_handle* h, bool on);
 int mpnn_infer(fsd_handle* h, const float4* pos, const unsigned* a_pn, const unsigned* a_plist, const float* a_blocks);
 int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, int P, uint32_t step, float lr,
                     float* loss_out, float* host_grad);
+// Polynomial coefficients for this configuration from the network (mean over
+// particles of the node head's first k outputs) into pc[0:k].
+int mpnn_poly_coeffs(fsd_handle* h, const float4* pos, float* pc, int k);
+int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, float* loss_out,
+                         float* loss_opt_out, float* host_grad, float* host_coef, float* host_coef_opt);
 
 }  // namespace fsd

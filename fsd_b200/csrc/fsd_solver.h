@@ -7,6 +7,7 @@ namespace fsd {
 
 constexpr int kMaxRestart = 400;
 constexpr int kMaxInner = 16;    // inner GMRES steps of the learned preconditioner
+constexpr int kMaxPoly = 16;     // coefficients of the learned inner polynomial
 constexpr int kPrunedCap = 32;   // pruned (r < rp) neighbours per particle, self included
 constexpr int kSpaiCap = 32;     // members of a two-hop approximate-inverse set
 

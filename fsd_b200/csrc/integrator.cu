@@ -250,7 +250,7 @@ int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigne
 
 int fsd_draw_normals(fsd_handle* h, unsigned int stream_id, unsigned int timestep, size_t n, float scale,
                      float* d_out) {
-    if (!h || !d_out || stream_id < 1 || stream_id > kStreamRot) return FSD_ERR_BAD_PARAMS;
+    if (!h || !d_out || stream_id < 1 || stream_id > kStreamLearned) return FSD_ERR_BAD_PARAMS;
     if (n == 0) return FSD_OK;
     gaussian(h, d_out, n, timestep, stream_id, scale);
     FSD_CHECK_CUDA(cudaGetLastError());

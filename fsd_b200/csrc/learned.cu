@@ -37,6 +37,7 @@ void learned_free(fsd_handle* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->sp_host) cudaFreeHost(s->sp_host);
+    poly_free(s);
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
@@ -371,7 +372,7 @@ static int inner_alloc(fsd_handle* h) {
 }
 
 bool precond_is_flexible(const fsd_handle* h) {
-    return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0;
+    return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_inner > 0 && !poly_active(h);
 }
 
 // Kernels of one inner solve on the right-hand side b into x, enqueued on st
@@ -496,6 +497,7 @@ int precond_apply_learned(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
     cudaStream_t st = h->stream;
+    if (poly_active(h)) return poly_apply(h, b, x);
     const int k = h->p.learned_inner;
     if (k == 0) {
         count_launch();
@@ -519,17 +521,30 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
     LearnedState* s = learned(h);
     ProfRegion pr(h, R_PRECOND_BUILD);
     int e = FSD_OK;
-    if (h->p.learned_inner > 0) e = inner_alloc(h);
+    const bool poly = h->p.learned_poly >= 2;
+    if (poly && !s->poly_user && !mpnn_loaded(h)) return FSD_ERR_BAD_PARAMS;  // no coefficients to use
+    if (poly) e = poly_alloc(h);
+    else if (h->p.learned_inner > 0) e = inner_alloc(h);
     if (e != FSD_OK) return e;
     e = precond_assemble_pruned(h, pos, 1.0f, &s->a_pn, &s->a_plist, &s->a_blocks);
     if (e != FSD_OK) return e;
     if (!s->g_user) {
         e = spai_build(h);
         if (e != FSD_OK) return e;
-        if (mpnn_loaded(h)) {
+        // The network either predicts the inner polynomial (learned_poly) or
+        // corrects G on its own pattern.
+        if (mpnn_loaded(h) && !poly) {
             e = mpnn_infer(h, pos, s->a_pn, s->a_plist, s->a_blocks);
             if (e != FSD_OK) return e;
         }
+    }
+    if (poly) {
+        if (!s->poly_user) {
+            e = mpnn_poly_coeffs(h, pos, s->pc, h->p.learned_poly);
+            if (e != FSD_OK) return e;
+        }
+        e = poly_lambda(h);
+        if (e != FSD_OK) return e;
     }
     h->pc_valid = true;
     return FSD_OK;
@@ -537,7 +552,10 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
 
 int learned_set_weights(fsd_handle* h, const float* host_w, int n) {
     const int e = mpnn_set_weights(h, host_w, n);
-    if (e == FSD_OK) learned(h)->g_user = false;
+    if (e == FSD_OK) {
+        learned(h)->g_user = false;
+        learned(h)->poly_user = false;  // the network's coefficients from now on
+    }
     return e;
 }
 

@@ -631,6 +631,13 @@ struct MpState {
     int P_cap = 0;
     double* part = nullptr;
     double* loss = nullptr;
+    // inner-polynomial training: Chebyshev basis images W_m = AG T_m(S) t
+    // (k x P x 6N), three recurrence slots (3 x P x 6N), Gram partials
+    float* pw = nullptr;
+    float* pb = nullptr;
+    size_t pw_cap = 0, pb_cap = 0;
+    double* gpart = nullptr;
+    size_t gpart_cap = 0;
     bool use_umma = true;
     std::vector<unsigned> h_cnt;
 };
@@ -660,7 +667,7 @@ void mpnn_free(fsd_handle* h) {
     MpState* s = (MpState*)ls->mp;
     void* ptrs[] = {s->cnt, s->scan, s->src, s->dst, s->rev, s->rhat, s->x, s->J, s->oe, s->on, s->dX, s->dXn, s->de,
                     s->dm, s->dh, s->dh2, s->dA, s->du, s->doe, s->don, s->dG, s->dwpart, s->w, s->gw, s->mw, s->vw,
-                    s->Zp, s->Up, s->Vp, s->part, s->loss};
+                    s->Zp, s->Up, s->Vp, s->part, s->loss, s->pw, s->pb, s->gpart};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int l = 0; l <= kMpLayers; ++l) {
@@ -1120,6 +1127,262 @@ int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, 
     FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
     if (s->use_umma && umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
     if (loss_out) *loss_out = (float)loss;
+    return FSD_OK;
+}
+
+// ---------------------------------------------------- learned inner polynomial
+// The network's use in the polynomial inner solve (poly.cu): the Chebyshev
+// coefficients of q for a configuration are the means over particles of the
+// node head's first k outputs.  Training minimises, for probe vectors t,
+//   L(c) = E_t ||t - AG q_c(AG) t||^2 / ||t||^2 = E_t (t.t - 2 c.g + c^T M c) / t.t
+// with W_m = AG T_m(S) t, g_m = W_m . t, M_ml = W_m . W_l: W and the Gram
+// entries are formed on the device, dL/dc on the host, and dL/dc / N is fed
+// to every particle's node head output for the network's backward pass.
+
+// pc[m] = mean_i on[i][m] for m < k (one warp per m, fixed order).
+__global__ void k_poly_pool(const float* __restrict__ on, int N, int k, float* pc) {
+    const int m = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (m >= k) return;
+    double sum = 0.0;
+    for (int i = lane; i < N; i += 32) sum += on[(size_t)i * kMpHeadN + m];
+    sum = group_sum_d<32>(sum);
+    if (lane == 0) pc[m] = (float)(sum / N);
+}
+
+// out = f ((2/lambda) W - Bm) - Bprev (Bprev may be null): the Chebyshev step
+// T_{m+1}(S) t = 2 S T_m(S) t - T_{m-1}(S) t with S = (2/lambda) AG - I.
+__global__ void k_cheb_next(const float* __restrict__ Wm, const float* __restrict__ Bm,
+                            const float* __restrict__ Bprev, size_t n, const float* __restrict__ pc, float f,
+                            float* __restrict__ out) {
+    const float s2 = 2.0f / pc[kMaxPoly];
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        float v = f * fmaf(s2, Wm[q], -Bm[q]);
+        if (Bprev) v -= Bprev[q];
+        out[q] = v;
+    }
+}
+
+constexpr int kGramChunk = 128;
+constexpr int kGramBlocks = 32;
+
+// Partial dot products of the k + 1 vectors (t_p, W_0p .. W_{k-1}p) of probe
+// p = blockIdx.y: pair q = (a <= b) in row-major order of the upper triangle;
+// part[(p * npairs + q) * gridDim.x + blockIdx.x].
+__global__ void __launch_bounds__(256) k_poly_gram(const float* __restrict__ T, const float* __restrict__ Wb, int k,
+                                                   int P, size_t n6, double* part) {
+    __shared__ float xs[kMaxPoly + 1][kGramChunk];
+    const int p = blockIdx.y;
+    const int nvec = k + 1, npairs = nvec * (nvec + 1) / 2;
+    int a = -1, b = -1;
+    if ((int)threadIdx.x < npairs) {
+        int q = threadIdx.x;
+        for (int r = 0; r < nvec; ++r) {
+            if (q < nvec - r) {
+                a = r;
+                b = r + q;
+                break;
+            }
+            q -= nvec - r;
+        }
+    }
+    double acc = 0.0;
+    for (size_t c0 = (size_t)blockIdx.x * kGramChunk; c0 < n6; c0 += (size_t)gridDim.x * kGramChunk) {
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < nvec * kGramChunk; idx += blockDim.x) {
+            const int v = idx / kGramChunk, e = idx % kGramChunk;
+            const size_t g = c0 + e;
+            float val = 0.f;
+            if (g < n6) val = v == 0 ? T[(size_t)p * n6 + g] : Wb[((size_t)(v - 1) * P + p) * n6 + g];
+            xs[v][e] = val;
+        }
+        __syncthreads();
+        if (a >= 0)
+            for (int e = 0; e < kGramChunk; ++e) acc += (double)xs[a][e] * (double)xs[b][e];
+    }
+    if (a >= 0) part[((size_t)p * npairs + threadIdx.x) * gridDim.x + blockIdx.x] = acc;
+}
+
+struct PolyGrad {
+    float g[kMpHeadN];
+};
+
+// dL/d on[i][m] = g[m] for every particle i.
+__global__ void k_fill_don(float* don, int N, PolyGrad pg) {
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (q < (size_t)N * kMpHeadN) don[q] = pg.g[q % kMpHeadN];
+}
+
+int mpnn_poly_coeffs(fsd_handle* h, const float4* pos, float* pc, int k) {
+    LearnedState* ls = learned(h);
+    MP_TRY(mp_graph(h, pos, ls->a_pn, ls->a_plist, ls->a_blocks));
+    MP_TRY(mp_forward(h));
+    MpState* s = mp(h);
+    count_launch();
+    k_poly_pool<<<1, 32 * kMaxPoly, 0, h->stream>>>(s->on, s->N, k, pc);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    if (s->use_umma) {
+        FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+        if (umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
+    }
+    return FSD_OK;
+}
+
+// Small dense solve M c = g (partial pivoting, FP64); false if singular.
+static bool solve_small(std::vector<double> M, std::vector<double> g, int k, std::vector<double>& c) {
+    for (int col = 0; col < k; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < k; ++r)
+            if (std::fabs(M[r * k + col]) > std::fabs(M[piv * k + col])) piv = r;
+        if (!(std::fabs(M[piv * k + col]) > 0.0)) return false;
+        if (piv != col) {
+            for (int q = 0; q < k; ++q) std::swap(M[col * k + q], M[piv * k + q]);
+            std::swap(g[col], g[piv]);
+        }
+        for (int r = col + 1; r < k; ++r) {
+            const double f = M[r * k + col] / M[col * k + col];
+            for (int q = col; q < k; ++q) M[r * k + q] -= f * M[col * k + q];
+            g[r] -= f * g[col];
+        }
+    }
+    c.assign(k, 0.0);
+    for (int r = k - 1; r >= 0; --r) {
+        double v = g[r];
+        for (int q = r + 1; q < k; ++q) v -= M[r * k + q] * c[q];
+        c[r] = v / M[r * k + r];
+    }
+    return true;
+}
+
+int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, float* loss_out,
+                         float* loss_opt_out, float* host_grad, float* host_coef, float* host_coef_opt) {
+    LearnedState* ls = learned(h);
+    if (!mpnn_loaded(h) || P < 1 || k < 2 || k > kMaxPoly) return FSD_ERR_BAD_PARAMS;
+    MpState* s = mp(h);
+    cudaStream_t st = h->stream;
+    MP_TRY(poly_alloc(h));
+    MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
+    MP_TRY(spai_build(h));
+    MP_TRY(poly_lambda(h));
+    MP_TRY(mpnn_poly_coeffs(h, pos, ls->pc, k));
+    MP_TRY(mp_probes(h, P));
+    const int N = s->N;
+    const size_t n6 = 6 * (size_t)N, nP = (size_t)P * n6;
+    if ((size_t)k * nP > s->pw_cap) {
+        MP_TRY(grow(&s->pw, (size_t)k * nP));
+        s->pw_cap = (size_t)k * nP;
+    }
+    if (3 * nP > s->pb_cap) {
+        MP_TRY(grow(&s->pb, 3 * nP));
+        s->pb_cap = 3 * nP;
+    }
+    const int nvec = k + 1, npairs = nvec * (nvec + 1) / 2;
+    const size_t ngp = (size_t)P * npairs * kGramBlocks;
+    if (ngp > s->gpart_cap) {
+        MP_TRY(grow(&s->gpart, ngp));
+        s->gpart_cap = ngp;
+    }
+    // probes t and the images W_m = AG B_m of the Chebyshev vectors B_m = T_m(S) t
+    gaussian(h, s->Zp, nP, step, kStreamLearned, 1.0f);
+    const int rows = (8 * N + 255) / 256;
+    const float* Bprev = nullptr;
+    const float* Bm = s->Zp;
+    for (int m = 0; m < k; ++m) {
+        float* Wm = s->pw + (size_t)m * nP;
+        count_launch();
+        k_bsr_multi<<<rows, 256, 0, st>>>(ls->g_rowptr, ls->g_col, ls->g_val, Bm, s->Up, N, P);
+        count_launch();
+        k_pruned_multi<<<rows, 256, 0, st>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Up, Wm, N, P);
+        if (m + 1 < k) {
+            float* out = s->pb + (size_t)(m % 3) * nP;
+            count_launch();
+            k_cheb_next<<<nblk(nP), kThreads, 0, st>>>(Wm, Bm, Bprev, nP, ls->pc, m == 0 ? 1.0f : 2.0f, out);
+            Bprev = Bm;
+            Bm = out;
+        }
+    }
+    count_launch();
+    k_poly_gram<<<dim3(kGramBlocks, P), 256, 0, st>>>(s->Zp, s->pw, k, P, n6, s->gpart);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    std::vector<double> part(ngp);
+    std::vector<float> c32(kMaxPoly + 1);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(part.data(), s->gpart, sizeof(double) * ngp, cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(c32.data(), ls->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    // Gram entries per probe, loss, gradient and the least-squares optimum
+    auto pair_index = [&](int a, int b) {
+        if (a > b) std::swap(a, b);
+        return a * nvec - a * (a - 1) / 2 + (b - a);
+    };
+    std::vector<double> c(k), grad(k, 0.0), Ms(k * k, 0.0), gs(k, 0.0);
+    for (int m = 0; m < k; ++m) c[m] = c32[m];
+    double loss = 0.0;
+    std::vector<std::vector<double>> Mp(P, std::vector<double>(k * k)), gp(P, std::vector<double>(k));
+    std::vector<double> ttp(P);
+    for (int p = 0; p < P; ++p) {
+        auto entry = [&](int a, int b) {
+            const double* q = part.data() + ((size_t)p * npairs + pair_index(a, b)) * kGramBlocks;
+            double v = 0.0;
+            for (int blk = 0; blk < kGramBlocks; ++blk) v += q[blk];
+            return v;
+        };
+        const double tt = entry(0, 0);
+        ttp[p] = tt;
+        for (int m = 0; m < k; ++m) {
+            gp[p][m] = entry(0, 1 + m);
+            for (int l = 0; l < k; ++l) Mp[p][m * k + l] = entry(1 + m, 1 + l);
+        }
+        double cMc = 0.0, cg = 0.0;
+        for (int m = 0; m < k; ++m) {
+            cg += c[m] * gp[p][m];
+            double Mc = 0.0;
+            for (int l = 0; l < k; ++l) Mc += Mp[p][m * k + l] * c[l];
+            cMc += c[m] * Mc;
+            grad[m] += 2.0 * (Mc - gp[p][m]) / (tt * P);
+            gs[m] += gp[p][m] / tt;
+            for (int l = 0; l < k; ++l) Ms[m * k + l] += Mp[p][m * k + l] / tt;
+        }
+        loss += (tt - 2.0 * cg + cMc) / (tt * P);
+    }
+    std::vector<double> copt;
+    double loss_opt = -1.0;
+    if (solve_small(Ms, gs, k, copt)) {
+        loss_opt = 0.0;
+        for (int p = 0; p < P; ++p) {
+            double cMc = 0.0, cg = 0.0;
+            for (int m = 0; m < k; ++m) {
+                cg += copt[m] * gp[p][m];
+                for (int l = 0; l < k; ++l) cMc += copt[m] * Mp[p][m * k + l] * copt[l];
+            }
+            loss_opt += (ttp[p] - 2.0 * cg + cMc) / (ttp[p] * P);
+        }
+    }
+    // backward: the node head's outputs each carry dL/dc / N
+    MP_TRY(mp_alloc_backward(h));
+    PolyGrad pg{};
+    for (int m = 0; m < k; ++m) pg.g[m] = (float)(grad[m] / N);
+    count_launch();
+    k_fill_don<<<(unsigned)(((size_t)N * kMpHeadN + 255) / 256), 256, 0, st>>>(s->don, N, pg);
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->doe, 0, sizeof(float) * (size_t)s->E_cap * kMpHeadE, st));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->gw, 0, sizeof(float) * MpLayout::total, st));
+    MP_TRY(mp_backward(h));
+    if (lr > 0.f) {
+        s->adam_t += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)s->adam_t), c2 = 1.f - powf(b2, (float)s->adam_t);
+        count_launch();
+        k_adam<<<(MpLayout::total + 255) / 256, 256, 0, st>>>(s->w, s->gw, s->mw, s->vw, MpLayout::total, lr, b1, b2,
+                                                             c1, c2, 1e-8f, 1.0f);
+    }
+    if (host_grad)
+        FSD_CHECK_CUDA(cudaMemcpyAsync(host_grad, s->gw, sizeof(float) * MpLayout::total, cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (s->use_umma && umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
+    if (loss_out) *loss_out = (float)loss;
+    if (loss_opt_out) *loss_opt_out = (float)loss_opt;
+    for (int m = 0; m < k; ++m) {
+        if (host_coef) host_coef[m] = (float)c[m];
+        if (host_coef_opt) host_coef_opt[m] = copt.empty() ? 0.f : (float)copt[m];
+    }
     return FSD_OK;
 }
 

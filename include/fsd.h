@@ -97,6 +97,11 @@ typedef struct fsd_params {
     int learned_inner;           /* FSD_PRECOND_LEARNED: inner GMRES steps on R_FU^pruned + D per application,
                                     right-preconditioned by the learned block-sparse G (4; 0 = apply G once).
                                     With inner steps the outer solve is flexible GMRES. */
+    int learned_poly;            /* FSD_PRECOND_LEARNED: when >= 2 (at most 16) and coefficients are available
+                                    (network weights, or fsd_learned_set_poly), y ~ (R_FU^pruned + D)^-1 t is
+                                    G q(AG) t with a Chebyshev polynomial q of this many coefficients on the
+                                    spectrum of AG, predicted per configuration by the network; the outer
+                                    solve stays plain GMRES.  0 (default): learned_inner decides. */
     int autotune;                /* 1: time candidate spreading tiles and FFT line batches on the first mobility
                                     call and keep the fastest (cached per process and grid shape).  Results then
                                     depend on the choice through the summation order, so runs in different
@@ -280,6 +285,24 @@ int fsd_learned_get_state(fsd_handle* h, float* host, int n, int* adam_step);
 int fsd_learned_set_state(fsd_handle* h, const float* host, int n, int adam_step);
 int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,
                            unsigned int step, float lr, float* loss, float* host_grad);
+/* Learned inner polynomial (learned_poly >= 2; no counterpart in the
+ * reference).  fsd_learned_set_poly fixes the k Chebyshev coefficients c of
+ * q (k = learned_poly, 2..16) instead of the network's prediction, until
+ * weights are set again; fsd_learned_get_poly copies the coefficients in use
+ * and, at index 16, the spectral bound lambda of AG of the last build
+ * (n >= 17 floats).
+ * fsd_learned_poly_train_step: for this configuration (neighbour list current
+ * for d_pos), the loss E_t ||t - AG q(AG) t||^2 / ||t||^2 over n_probes
+ * (1..64) normal probe vectors drawn from (seed, step), with q's coefficients
+ * from the network; its least-squares optimum over all coefficients
+ * (loss_opt, host_coef_opt, both optional); the network's coefficients
+ * (host_coef, optional, k floats); the weight gradient (host_grad,
+ * optional); and, when lr > 0, one Adam step. */
+int fsd_learned_set_poly(fsd_handle* h, const float* host_c, int k);
+int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n);
+int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
+                                float* loss, float* loss_opt, float* host_grad, float* host_coef,
+                                float* host_coef_opt);
 /* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x);
 /* Preconditioned GMRES on the saddle system (Solvers_Saddle, Solvers.cu:55).
@@ -296,7 +319,9 @@ int fsd_rfd_drift(fsd_handle* h, const float* d_pos, const int* d_image, unsigne
  * `timestep`, times `scale`, from the counter-based Philox4x32-10 generator
  * keyed by the handle's hashed seed.  Streams: 1 far-field real-space (11N),
  * 2 wave-space field, 3 near-field (6N), 4 drift direction psi (6N),
- * 5 rotational noise (3N).  The reference draws these with cuRAND
+ * 5 rotational noise (3N), 6 start vectors of spectral estimates, 7 probe
+ * vectors of the learned preconditioner's training.  The reference draws
+ * the first five with cuRAND
  * (Integrator.cu:591-596, Brownian_FarField.cu:864-874,
  * Brownian_NearField.cu:438-444), so this has no counterpart there; it lets a
  * caller reproduce the noise of any step. */

@@ -183,3 +183,56 @@ def loss(wv, pr, Z):
     G = g_matrix(wv, pr)
     R = (pr["A"] @ (G @ Z.T)).T - Z
     return float(np.sum(R * R) / (Z.shape[0] * 6 * pr["N"]))
+
+
+# ------------------------------------------------ learned inner polynomial
+def cheb_images(A, G, T, lam, k):
+    """W_m = A G T_m(S) t for m < k, S = (2/lam) A G - I, probes T (P, 6N);
+    returns (k, 6N, P)."""
+    B = [T.T]
+    W = []
+    for m in range(k):
+        Wm = A @ (G @ B[m])
+        W.append(Wm)
+        if m + 1 < k:
+            if m == 0:
+                B.append((2.0 / lam) * Wm - B[0])
+            else:
+                B.append(2.0 * ((2.0 / lam) * Wm - B[m]) - B[m - 1])
+    return np.stack(W)
+
+
+def poly_coeffs(wv, pr, k):
+    """Chebyshev coefficients the network predicts: mean over particles of the
+    node head's first k outputs (mpnn.cu k_poly_pool)."""
+    _, on = forward(wv, pr["x"], pr["i"], pr["j"], pr["N"])
+    return on[:, :k].mean(0)
+
+
+def poly_loss_c(c, W, T):
+    """E_t ||t - sum_m c_m W_m t||^2 / ||t||^2 over the probes."""
+    R = T.T - np.einsum("m,mnp->np", c, W)
+    return float(np.mean(np.sum(R * R, 0) / np.sum(T.T * T.T, 0)))
+
+
+def poly_loss(wv, pr, T, lam, k):
+    return poly_loss_c(poly_coeffs(wv, pr, k), cheb_images(pr["A"], pr["G0"], T, lam, k), T)
+
+
+def poly_apply(b, c, lam, A, G, N):
+    """Saddle preconditioner with y = G q(AG) t, q = sum c_m T_m(2x/lam - 1),
+    evaluated in FP64 by Clenshaw's recurrence (poly.cu)."""
+    b = np.asarray(b, np.float64)
+    t = b[: 6 * N] - b[11 * N:]
+    k = len(c)
+    S = lambda v: (2.0 / lam) * (A @ (G @ v)) - v
+    b1 = c[k - 1] * t
+    b2 = np.zeros_like(t)
+    for m in range(k - 2, 0, -1):
+        b1, b2 = c[m] * t + 2.0 * S(b1) - b2, b1
+    v = c[0] * t + S(b1) - b2
+    y = G @ v
+    x = b.copy()
+    x[: 6 * N] = b[: 6 * N] - y
+    x[11 * N:] = y
+    return x

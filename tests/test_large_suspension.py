@@ -92,25 +92,37 @@ def test_subbox_n4096_velocity_and_stresslet_match_oracle(cuda):
 
 def test_subbox_n4096_lanczos_iterations_to_1e3(cuda):
     """Brownian samples of the sub-box at the Lanczos tolerance 1e-3 against the
-    same draws converged to 1e-5: the far-field real-space square root and the
-    near-field R_FU square root each stay within 2e-3 of the converged sample,
-    and the iteration counts are reported.  (The covariance of the samples
-    against 2kT/dt M and 2kT/dt R_FU is checked in test_brownian.py.)"""
+    same draws run to a 1e-5 change (up to 400 iterations; the near-field
+    R_FU is ill-conditioned enough that FP32 Lanczos may stop just short of
+    it, which the library reports as FSD_ERR_LANCZOS_MAXIT with the last
+    change): the far-field real-space square root and the near-field R_FU
+    square root each stay within 2e-3 of the long runs, and the iteration
+    counts are reported.  (The covariance of the samples against 2kT/dt M and
+    2kT/dt R_FU is checked in test_brownian.py.)"""
+    import ctypes as C
+    from fsd_b200 import _lib
     N = 4096
     pos, Lc = suspension(N, 0.3, 3)
     p = torch.as_tensor(pos).cuda().view(-1).contiguous()
     out = {}
     for tol in (1e-3, 1e-5):
-        s = FSD(N, (Lc, Lc, Lc, 0.0), T=1.0, dt=1e-4, seed=5, lanczos_tol=tol, lanczos_max=100)
+        s = FSD(N, (Lc, Lc, Lc, 0.0), T=1.0, dt=1e-4, seed=5, lanczos_tol=tol, lanczos_max=400)
         s.build_neighbor_list(p)
-        ff = s.brownian_farfield(p, 3).cpu().numpy()
-        nf = s.brownian_nearfield(p, 3).cpu().numpy()
+        ff = torch.zeros(11 * N, device="cuda")
+        nf = torch.zeros(6 * N, device="cuda")
+        st_ff = _lib.lib().fsd_brownian_farfield(s._h, p.data_ptr(), 3, ff.data_ptr())
+        st_nf = _lib.lib().fsd_brownian_nearfield(s._h, p.data_ptr(), 3, nf.data_ptr())
         info = s.solve_info()
-        out[tol] = (ff, nf, info["lanczos_ff_iters"], info["lanczos_nf_iters"])
+        assert st_ff in (0, 4) and st_nf in (0, 4)
+        if tol == 1e-3:
+            assert st_ff == 0 and st_nf == 0
+        else:
+            assert info["lanczos_ff_err"] < 1e-4 and info["lanczos_nf_err"] < 1e-4
+        out[tol] = (ff.cpu().numpy(), nf.cpu().numpy(), info["lanczos_ff_iters"], info["lanczos_nf_iters"])
         s.close()
     eff, enf = rel(out[1e-3][0], out[1e-5][0]), rel(out[1e-3][1], out[1e-5][1])
     print(f"sub-box N=4096 Lanczos to 1e-3: far field {out[1e-3][2]} iterations (rel err {eff:.1e}), "
-          f"near field {out[1e-3][3]} iterations (rel err {enf:.1e}); to 1e-5: {out[1e-5][2]} / {out[1e-5][3]}")
+          f"near field {out[1e-3][3]} iterations (rel err {enf:.1e}); long runs: {out[1e-5][2]} / {out[1e-5][3]}")
     assert eff < 2e-3 and enf < 2e-3
     assert out[1e-3][2] < out[1e-5][2] and out[1e-3][3] < out[1e-5][3]
 
