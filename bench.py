@@ -61,6 +61,9 @@ def parse():
                          "phi uniform in [0.1, 0.5], shear rate uniform in [0, 2], stepped concurrently and then "
                          "one by one (prints its own JSON line)")
     ap.add_argument("--ichol-steps", type=int, default=2)
+    ap.add_argument("--config5", action="store_true",
+                    help="learned vs IChol vs SPAI + inner GMRES on held-out dense suspensions (own JSON line)")
+    ap.add_argument("--config5-phis", type=float, nargs="+", default=[0.45, 0.5, 0.55])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -550,11 +553,76 @@ def run_reference(args, ws, rank):
             "wall_s": time.time() - t_all}
 
 
+POLY_WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_poly_k8.f32"
+
+
+def run_config5(args, local):
+    """Learned preconditioner on dense suspensions (N = 32768 at phi 0.45,
+    0.5, 0.55, shear rate 1, kT = 1) on held-out seeds: one velocity
+    computation (RFD +/- and main saddle solves to 1e-4) per preconditioner,
+    with the outer GMRES iterations of each solve and the device time."""
+    import torch
+
+    from fsd_b200 import _lib
+    from fsd_b200.configs import suspension
+    from fsd_b200.core import FSD
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N = args.N
+    forms = {
+        "ichol": dict(precond="ichol", gmres_restart=200, learned_inner=0),
+        "spai_gmres6": dict(precond="learned", gmres_restart=100, learned_inner=6),
+        "learned_poly8": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=8),
+    }
+    w = np.fromfile(POLY_WEIGHTS, "<f4") if POLY_WEIGHTS.exists() else None
+    results = {}
+    for phi in args.config5_phis:
+        pos, L = suspension(N, phi, seed=1000 + int(round(phi * 100)))  # seeds the training never used
+        res = {}
+        for name, kw in forms.items():
+            if name == "learned_poly8" and w is None:
+                continue
+            s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=7, solver_tol=1e-4, lanczos_tol=1e-3,
+                    rfd_epsilon=1e-3, period=0, gmres_max_iter=4000, **kw)
+            if name == "learned_poly8":
+                s.learned_set_weights(w)
+            times, iters, resid = [], [], []
+            for rep in range(2):  # the first call also captures graphs and tunes
+                p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
+                ori = torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev)
+                img = torch.zeros(3 * N, dtype=torch.int32, device=dev)
+                F = torch.zeros(6 * N, device=dev)
+                V = torch.zeros(11 * N, device=dev)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(dev)
+                e0.record()
+                a = s.step_args(0, 1.0, p, ori, img, F, V)
+                st = _lib.lib().fsd_compute_velocity(s._h, C.byref(a))
+                e1.record()
+                torch.cuda.synchronize(dev)
+                if st not in (0, 4):
+                    raise RuntimeError(f"{name} phi={phi}: status {st}")
+                si = s.solve_info()
+                times.append(e0.elapsed_time(e1))
+                iters.append(si["gmres_iters"])
+                resid.append(si["gmres_resid"])
+            s.close()
+            res[name] = {"outer_iterations": iters[-1], "residuals": resid[-1], "ms": times[-1]}
+        results[str(phi)] = res
+    return {"metric": "config 5: learned preconditioner on held-out dense suspensions, one velocity computation "
+                      "(three saddle solves to 1e-4)", "unit": "ms", "N": N, "higher_is_better": False,
+            "data": "synthetic: seeded random sequential addition + overlap relaxation, seeds not used in training",
+            "results": results}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
     if args.impl == "reference":
         out = run_reference(args, ws, rank)
+    elif args.config5:
+        out = run_config5(args, local) if rank == 0 else None
     elif args.replicas > 0:
         out = run_replicas(args, rank, local)
     else:

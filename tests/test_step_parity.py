@@ -11,8 +11,9 @@ against the FP64 oracle.
   drift direction psi (fsd_draw_normals, stream 4): (kT/eps)(U(x + eps psi/2)
   - U(x - eps psi/2)) with A(x') U = (0; -psi), solved by the oracle at the
   same FP32 displaced positions.  The difference of two solutions divided by
-  eps = 1e-3 amplifies the solver residual (3e-7 here) and FP32 rounding of
-  the operator by 1e3, so the bar is 2e-3.
+  eps = 1e-3 amplifies the solver residual (1e-6 here, just above the FP32
+  residual floor of these right-hand sides) and FP32 rounding of the operator
+  by 1e3, so the bar is 5e-3.
 * One full step at kT = 1 with shear (fsd_step, Stokes_StepOne, Stokes.cu:119)
   against the oracle's right-hand side, saddle solve, stresslet and Euler
   update, given the library's own Brownian vectors for that step (far-field
@@ -20,7 +21,8 @@ against the FP64 oracle.
   fsd_rfd_drift at the same timestep on a fresh handle, which draw the same
   counter-based normals).  Once without and once with the active terms
   (squirmer B1/B2 with masks, rotational noise, external torque).  Velocities
-  and stresslets to 1e-4, displacements to 1e-4, images exactly.
+  and stresslets to 1e-4 (GMRES to 1e-6), displacements to 1e-4, images
+  exactly.
 """
 from __future__ import annotations
 
@@ -92,7 +94,7 @@ def test_rfd_drift_matches_oracle(cuda):
     N, phi, seed, eps, T = 200, 0.3, 5, 1e-3, 1.0
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
-    s = FSD(N, (Lc, Lc, Lc, 0.0), T=T, dt=1e-4, seed=9, rfd_epsilon=eps, solver_tol=3e-7, gmres_max_iter=4000,
+    s = FSD(N, (Lc, Lc, Lc, 0.0), T=T, dt=1e-4, seed=9, rfd_epsilon=eps, solver_tol=1e-6, gmres_max_iter=4000,
             precond="learned")
     p = dev(pos)
     img = torch.zeros(3 * N, dtype=torch.int32, device="cuda")
@@ -108,7 +110,9 @@ def test_rfd_drift_matches_oracle(cuda):
         rhs[11 * N:] = -psi
         U.append(pr.solve(rhs, tol=1e-11)[11 * N:])
     ref = (T / eps) * (U[0] - U[1])
-    assert rel(drift, ref) < 2e-3
+    err = rel(drift, ref)
+    print(f"RFD drift N={N}: rel err {err:.2e}")
+    assert err < 5e-3
     s.close()
 
 
@@ -118,7 +122,7 @@ def test_full_brownian_step_matches_oracle(cuda, active):
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
     rng = np.random.default_rng(seed)
-    kw = dict(T=T, dt=dt, seed=11, solver_tol=5e-7, gmres_max_iter=4000, period=1, precond="learned",
+    kw = dict(T=T, dt=dt, seed=11, solver_tol=1e-6, gmres_max_iter=4000, period=1, precond="learned",
               lanczos_tol=1e-4)
     ori = np.tile([0.0, 0.0, 1.0], (N, 1)).astype(np.float32)
     b1m = b2m = None
@@ -162,8 +166,10 @@ def test_full_brownian_step_matches_oracle(cuda, active):
     U = x[11 * N:] + drift
     S = x[6 * N:11 * N] + O.rsu(pr.pos, U, L, xy, pr.rows, pr.tdist, pr.tvals) \
         + O.rse(pr.pos, rate, L, xy, pr.rows, pr.tdist, pr.tvals, ori=ori, b2mask=b2m, B2=B2)
-    assert rel(v[:6 * N], U) < 1e-4
-    assert rel(v[6 * N:], S) < 1e-4
+    eu, es = rel(v[:6 * N], U), rel(v[6 * N:], S)
+    print(f"full step active={active}: velocity rel err {eu:.2e}, stresslet rel err {es:.2e}, "
+          f"GMRES {s.solve_info()['gmres_iters']} residuals {s.solve_info()['gmres_resid']}")
+    assert eu < 1e-4 and es < 1e-4
     noise = rot.reshape(N, 3) if active else None
     rp, rori, rgb, rimg = O.euler_shear(pos, ori, pos, U, np.zeros((N, 3), np.int64), L, xy, dt, rate, B1=B1,
                                         b1mask=b1m, noise=noise)
