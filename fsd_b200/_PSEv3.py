@@ -229,8 +229,22 @@ class Stokes:
         self._table_set = True
 
     def setFriction(self, friction_type, h0, alpha):  # noqa: N802
-        if str(friction_type).upper() != "NONE":
-            raise NotImplementedError("friction tables (Stokes.cc:1132-1191) are not part of this build")
+        """Frictional contact terms in the resistance table (Stokes.cc:1132-1191):
+        "NONE" or "TYPE1" with the contact range h0 and the six strengths
+        alpha (YA11, YA12, YB11, YB12, YC11, YC12); applied when the
+        workspaces are allocated."""
+        kind = str(friction_type).upper()
+        if kind not in ("NONE", "TYPE1"):
+            raise RuntimeError("Invalid Friction Type. Allowable types are: None, Type1")
+        if self.fsd is not None:
+            raise RuntimeError("setFriction must precede AllocateWorkSpaces")
+        if kind == "TYPE1":
+            alpha = [float(a) for a in alpha]
+            if len(alpha) != 6:
+                raise RuntimeError("TYPE1 friction takes six strengths")
+            self.solver.update(friction_type=1, friction_h0=float(h0), friction_alpha=alpha)
+        else:
+            self.solver.update(friction_type=0)
 
     def setSparseMath(self):  # noqa: N802
         """Sparse storage is created with the workspaces (Stokes.cc:1066-1130)."""

@@ -40,6 +40,8 @@ class fsd_params(C.Structure):
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
         ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
         ("learned_inner", C.c_int), ("learned_poly", C.c_int), ("autotune", C.c_int),
+        ("friction_type", C.c_int), ("friction_h0", C.c_float), ("friction_alpha", C.c_float * 6),
+        ("integrator", C.c_int),
     ]
 
 
@@ -80,6 +82,7 @@ _SIGS = {
     "fsd_status_string": (C.c_char_p, [C.c_int]),
     "fsd_pse_setup": (C.c_int, [C.POINTER(fsd_params), C.POINTER(fsd_pse_info), P, C.c_size_t]),
     "fsd_rcm_order": (C.c_int, [C.c_int, P, P, P]),
+    "fsd_resistance_table": (C.c_int, [C.POINTER(fsd_params), P, P]),
     "fsd_create": (C.c_int, [C.POINTER(fsd_params), P, C.POINTER(H)]),
     "fsd_destroy": (None, [H]),
     "fsd_set_stream": (C.c_int, [H, P]),

@@ -71,6 +71,12 @@ class FSD:
                 v = _lib.PRECOND[v] if isinstance(v, str) else int(v)
             elif k == "force_mode":
                 v = _lib.FORCE_MODE[v] if isinstance(v, str) else int(v)
+            elif k == "friction_alpha" and not isinstance(v, C.Array):
+                v = (C.c_float * 6)(*[float(a) for a in v])
+            elif k == "friction_type" and isinstance(v, str):
+                v = {"NONE": 0, "TYPE1": 1}[v.upper()]
+            elif k == "integrator" and isinstance(v, str):
+                v = {"euler": 0, "rk2": 1}[v.lower()]
             if not hasattr(p, k):
                 raise TypeError(f"unknown parameter {k}")
             setattr(p, k, v)

@@ -122,6 +122,14 @@ static int allocate(fsd_handle* h) {
     FSD_TRY(dalloc(&w.lz_dot, 4096));
     FSD_CHECK_CUDA(cudaMallocHost(&w.lz_host, sizeof(double) * 4096));
     FSD_CHECK_CUDA(cudaMemsetAsync(w.sol, 0, sizeof(float) * n17, h->stream));
+    if (h->p.integrator == 1) {
+        FSD_TRY(dalloc(&w.rk_pos, N));
+        FSD_TRY(dalloc(&w.rk_posw, N));
+        FSD_TRY(dalloc(&w.rk_ori, 3 * (size_t)N));
+        FSD_TRY(dalloc(&w.rk_vel, 11 * (size_t)N));
+        FSD_TRY(dalloc(&w.rk_u1, 6 * (size_t)N));
+        FSD_TRY(dalloc(&w.rk_noise, 3 * (size_t)N));
+    }
     FSD_TRY(precond_alloc(h));
     return FSD_OK;
 }
@@ -133,7 +141,7 @@ static void release(fsd_handle* h) {
                    w.bin_parts, w.grid, w.gridk, w.twiddle, w.f4, w.c4, w.uwave, w.sx, w.sy, w.sz, w.V, w.Z, w.dred,
                    w.hcol, w.hcol2, w.ticket, w.gmres_state, w.pc_t, w.pc_y, w.rhs, w.sol, w.rfd_rhs, w.rfd_sol, w.psi,
                    w.pos_prime, w.vel, w.force, w.lanczos_V, w.lz_a, w.lz_b, w.lz_c, w.lz_dot, h->d_ewald,
-                   h->d_res_dist, h->d_res_vals};
+                   h->d_res_dist, h->d_res_vals, w.rk_pos, w.rk_posw, w.rk_ori, w.rk_vel, w.rk_u1, w.rk_noise};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (w.host_flag) cudaFreeHost(w.host_flag);
@@ -182,6 +190,48 @@ void fsd_default_params(fsd_params* p) {
     p->ichol_gain_limit = 100.0f;
     p->learned_inner = 4;
     p->learned_poly = 0;
+    p->friction_type = 0;
+    p->friction_h0 = 0.0f;
+    for (int k = 0; k < 6; ++k) p->friction_alpha[k] = 0.0f;
+    p->integrator = 0;
+}
+
+// The resistance table with the TYPE1 friction patch (Stokes::setFriction,
+// Stokes.cc:1132-1191): for every tabulated distance whose gap h = r - 2 is
+// at most h0, alpha_k (2 h^2/h0^3 - 3 h/h0^2 + 1/h) is added in magnitude to
+// YA11, YA12, YB11, YB12, YC11 and YC12 (entries 3, 4, 5, 6, 9, 10; the signs
+// follow the tabulated functions' signs).  The bracket is evaluated in double
+// from single-precision h and powers of h0, then rounded to single precision,
+// as the reference's float/double mix does.
+static void resistance_table_for(const fsd_params* p, std::vector<float>& dist, std::vector<float>& vals) {
+    dist.assign(resistance_table_dist(), resistance_table_dist() + kResRows);
+    vals.assign(resistance_table_vals(), resistance_table_vals() + (size_t)kResRows * kResFuncs);
+    if (p->friction_type != 1) return;
+    const float h0 = p->friction_h0;
+    const float h02 = h0 * h0;
+    const float h03 = h0 * h02;
+    const int slot[6] = {3, 4, 5, 6, 9, 10};
+    const float sign[6] = {1.f, -1.f, -1.f, 1.f, 1.f, 1.f};
+    for (int i = 0; i < kResRows; ++i) {
+        const float h = (float)((double)dist[i] - 2.0);
+        if (!(h <= h0)) continue;
+        const float h2 = h * h;
+        const double bracket = 2.0 / h03 * h2 - 3.0 / h02 * h + 1.0 / h;
+        for (int k = 0; k < 6; ++k) {
+            const float add = (float)(p->friction_alpha[k] * bracket);
+            float& v = vals[(size_t)kResFuncs * i + slot[k]];
+            v = sign[k] > 0 ? v + add : v - add;
+        }
+    }
+}
+
+int fsd_resistance_table(const fsd_params* p, float* dist, float* vals) {
+    if (!p || !dist || !vals || p->friction_type < 0 || p->friction_type > 1) return FSD_ERR_BAD_PARAMS;
+    std::vector<float> d, v;
+    resistance_table_for(p, d, v);
+    std::copy(d.begin(), d.end(), dist);
+    std::copy(v.begin(), v.end(), vals);
+    return FSD_OK;
 }
 
 const char* fsd_status_string(int status) {
@@ -248,6 +298,9 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
     if (p->gmres_restart < 1 || p->gmres_restart > kMaxRestart || p->lanczos_max < 4) return FSD_ERR_BAD_PARAMS;
     if (p->learned_inner < 0 || p->learned_inner > kMaxInner) return FSD_ERR_BAD_PARAMS;
     if (p->learned_poly < 0 || p->learned_poly == 1 || p->learned_poly > kMaxPoly) return FSD_ERR_BAD_PARAMS;
+    if (p->friction_type < 0 || p->friction_type > 1 || (p->friction_type == 1 && !(p->friction_h0 > 0.f)))
+        return FSD_ERR_BAD_PARAMS;
+    if (p->integrator < 0 || p->integrator > 1) return FSD_ERR_BAD_PARAMS;
     fsd_handle* h = new fsd_handle();
     h->p = *p;
     h->stream = (cudaStream_t)stream;
@@ -273,10 +326,11 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
             st = FSD_ERR_ALLOC;
         } else {
             cudaMemcpyAsync(h->d_ewald, h->ewald_host.data(), tb, cudaMemcpyHostToDevice, h->stream);
-            cudaMemcpyAsync(h->d_res_dist, resistance_table_dist(), sizeof(float) * kResRows, cudaMemcpyHostToDevice,
+            std::vector<float> tdist, tvals;
+            resistance_table_for(p, tdist, tvals);
+            cudaMemcpyAsync(h->d_res_dist, tdist.data(), sizeof(float) * kResRows, cudaMemcpyHostToDevice, h->stream);
+            cudaMemcpyAsync(h->d_res_vals, tvals.data(), sizeof(float) * kResRows * kResFuncs, cudaMemcpyHostToDevice,
                             h->stream);
-            cudaMemcpyAsync(h->d_res_vals, resistance_table_vals(), sizeof(float) * kResRows * kResFuncs,
-                            cudaMemcpyHostToDevice, h->stream);
             fill_twiddles(h);
             mobility_set_gridk(h);
             if (cudaStreamSynchronize(h->stream) != cudaSuccess) st = FSD_ERR_CUDA;

@@ -131,6 +131,13 @@ struct Workspace {
     float* lz_c = nullptr;
     double* lz_dot = nullptr;      // device dot results
     double* lz_host = nullptr;     // pinned host copies
+    // two-stage Runge-Kutta (integrator = 1 only)
+    float4* rk_pos = nullptr;      // predictor positions, unwrapped
+    float4* rk_posw = nullptr;     // predictor positions wrapped into the box (velocity evaluation)
+    float* rk_ori = nullptr;       // predictor directors, 3N
+    float* rk_vel = nullptr;       // velocity at the predictor, 11N
+    float* rk_u1 = nullptr;        // velocity at the start of the step, 6N
+    float* rk_noise = nullptr;     // angular noise of the step, 3N
 };
 // Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
 // current device.  Function attributes are per device, so the record is kept

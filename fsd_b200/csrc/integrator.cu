@@ -135,6 +135,128 @@ __global__ void k_euler_shear(float4* pos, float3* ori, float4* pos_gb, const fl
     }
 }
 
+// Quaternion rotation of director pv about w by |w| t, renormalised.
+__device__ __forceinline__ float3 rotate_director(float3 pv, float3 w, float t) {
+    float q0 = 1.0f;
+    float3 qv = make_float3(0.f, 0.f, 0.f);
+    const float aw = sqrtf(w.x * w.x + w.y * w.y + w.z * w.z);
+    if (aw > 1e-6f) {
+        const float ang = aw * t;
+        q0 = cosf(ang / 2.f);
+        const float s = sinf(ang / 2.f) / aw;
+        qv = make_float3(w.x * s, w.y * s, w.z * s);
+    }
+    const float qq = qv.x * qv.x + qv.y * qv.y + qv.z * qv.z;
+    const float qp = qv.x * pv.x + qv.y * pv.y + qv.z * pv.z;
+    float3 pn = make_float3((q0 * q0 - qq) * pv.x, (q0 * q0 - qq) * pv.y, (q0 * q0 - qq) * pv.z);
+    pn.x += 2.f * qp * qv.x + 2.f * q0 * (qv.y * pv.z - qv.z * pv.y);
+    pn.y += 2.f * qp * qv.y + 2.f * q0 * (qv.z * pv.x - qv.x * pv.z);
+    pn.z += 2.f * qp * qv.z + 2.f * q0 * (qv.x * pv.y - qv.y * pv.x);
+    const float nm = sqrtf(pn.x * pn.x + pn.y * pn.y + pn.z * pn.z);
+    return make_float3(pn.x / nm, pn.y / nm, pn.z / nm);
+}
+
+// Stage 1 of the two-stage Runge-Kutta step (Integrator_ExplicitEuler1_Shear_kernel,
+// Integrator.cu:232-330): the Euler predictor x* = x + U dt, kept unwrapped
+// for the average of stage 2 (and wrapped into the box for the velocity at
+// x*), the director rotated by the full step, and half a step of the
+// unwrapped positions.
+__global__ void k_rk_stage1(const float4* __restrict__ pos, const float3* ori, float4* __restrict__ pos_star,
+                            float4* __restrict__ pos_star_w, float3* ori_star, float4* pos_gb,
+                            const float* __restrict__ vel, float B1, const float* b1mask, const float3* noise, int N,
+                            Box b, float dt, float shear_rate) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 p4 = pos[i];
+    float3 p = make_float3(p4.x, p4.y, p4.z);
+    float3 v = make_float3(vel[6 * i], vel[6 * i + 1], vel[6 * i + 2]);
+    float3 w = make_float3(vel[6 * i + 3], vel[6 * i + 4], vel[6 * i + 5]);
+    v.x += shear_rate * p.y;
+    w.z -= shear_rate / 2.f;
+    if (noise) {
+        const float3 n = noise[i];
+        w.x += n.x;
+        w.y += n.y;
+        w.z += n.z;
+    }
+    const float3 pv = ori ? ori[i] : make_float3(0.f, 0.f, 1.f);
+    const float ab = -2.f / 3.f * B1 * (b1mask ? b1mask[i] : 1.0f);
+    v.x -= ab * pv.x;
+    v.y -= ab * pv.y;
+    v.z -= ab * pv.z;
+    if (pos_gb) {
+        float4 g = pos_gb[i];
+        g.x += (v.x - shear_rate * p.y + shear_rate * g.y) * 0.5f * dt;
+        g.y += v.y * 0.5f * dt;
+        g.z += v.z * 0.5f * dt;
+        pos_gb[i] = g;
+    }
+    p.x += v.x * dt;
+    p.y += v.y * dt;
+    p.z += v.z * dt;
+    pos_star[i] = make_float4(p.x, p.y, p.z, p4.w);
+    int3 img = make_int3(0, 0, 0);
+    wrap_position(p, img, b);
+    pos_star_w[i] = make_float4(p.x, p.y, p.z, p4.w);
+    if (ori) ori_star[i] = rotate_director(pv, w, dt);
+}
+
+// Stage 2 (Integrator_RK_Shear_kernel, Integrator.cu:333-438): from the
+// combination c1 x + c2 x* (directors likewise, renormalised) move by
+// c3 dt with the velocity at the predictor, rotate by c3 dt, add half a step
+// to the unwrapped positions and wrap.
+__global__ void k_rk_stage2(float4* pos, float3* ori, const float4* __restrict__ pos_star,
+                            const float3* __restrict__ ori_star, float4* pos_gb, const float* __restrict__ vel,
+                            float B1, const float* b1mask, const float3* noise, int3* image, int N, Box b, float dt,
+                            float shear_rate, float c1, float c2, float c3) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 p1 = pos[i], p2 = pos_star[i];
+    float3 p = make_float3(c1 * p1.x + c2 * p2.x, c1 * p1.y + c2 * p2.y, c1 * p1.z + c2 * p2.z);
+    float3 v = make_float3(vel[6 * i], vel[6 * i + 1], vel[6 * i + 2]);
+    float3 w = make_float3(vel[6 * i + 3], vel[6 * i + 4], vel[6 * i + 5]);
+    v.x += shear_rate * p.y;
+    w.z -= shear_rate / 2.f;
+    if (noise) {
+        const float3 n = noise[i];
+        w.x += n.x;
+        w.y += n.y;
+        w.z += n.z;
+    }
+    float3 pv = make_float3(0.f, 0.f, 1.f);
+    if (ori) {
+        const float3 a = ori[i], c = ori_star[i];
+        pv = make_float3(a.x * c1 + c.x * c2, a.y * c1 + c.y * c2, a.z * c1 + c.z * c2);
+        const float m0 = sqrtf(pv.x * pv.x + pv.y * pv.y + pv.z * pv.z);
+        pv = make_float3(pv.x / m0, pv.y / m0, pv.z / m0);
+    }
+    const float ab = -2.f / 3.f * B1 * (b1mask ? b1mask[i] : 1.0f);
+    v.x -= ab * pv.x;
+    v.y -= ab * pv.y;
+    v.z -= ab * pv.z;
+    if (pos_gb) {
+        float4 g = pos_gb[i];
+        g.x += (v.x - shear_rate * p.y + shear_rate * g.y) * 0.5f * dt;
+        g.y += v.y * 0.5f * dt;
+        g.z += v.z * 0.5f * dt;
+        pos_gb[i] = g;
+    }
+    p.x += v.x * dt * c3;
+    p.y += v.y * dt * c3;
+    p.z += v.z * dt * c3;
+    int3 img = image[i];
+    wrap_position(p, img, b);
+    pos[i] = make_float4(p.x, p.y, p.z, p1.w);
+    image[i] = img;
+    if (ori) ori[i] = rotate_director(pv, w, dt * c3);
+}
+
+// out = (a + b) / 2 on n entries (the step's reported velocity with two stages).
+__global__ void k_mean2(float* out, const float* __restrict__ a, const float* __restrict__ b, size_t n) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        out[k] = 0.5f * (a[k] + b[k]);
+}
+
 static int vb(size_t n) { return (int)std::min<size_t>(4 * 148, (n + 255) / 256); }
 
 // Integrator_ComputeVelocity: velocity (11N) for the current positions.
@@ -212,11 +334,64 @@ int integrate_euler(fsd_handle* h, const fsd_step_args* a) {
     return FSD_OK;
 }
 
-int step(fsd_handle* h, const fsd_step_args* a) {
+// Two-stage Runge-Kutta (Heun) step of Integrator.cu:232-438: velocity at
+// x, Euler predictor x*, velocity at x* with the same step's random draws,
+// then the average of x and x* moved by half a step at the velocity of x*.
+// The reported velocity is the mean of the two stages'; stresslets (on
+// output steps) are those of the first stage.
+static int step_rk2(fsd_handle* h, const fsd_step_args* a) {
+    Workspace& w = h->w;
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
     int e = compute_velocity(h, a);
     if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
-    const int ee = integrate_euler(h, a);
-    if (ee != FSD_OK) return ee;
+    int status = e;
+    const float3* noise = (const float3*)a->d_noise_ang;
+    if (!noise && h->p.rot_diff > 0.f) {
+        gaussian(h, w.rk_noise, 3 * (size_t)N, a->timestep, kStreamRot, sqrtf(2.0f * h->p.rot_diff / h->p.dt));
+        noise = (const float3*)w.rk_noise;
+    }
+    FSD_CHECK_CUDA(cudaMemcpyAsync(w.rk_u1, a->d_velocity, sizeof(float) * 6 * N, cudaMemcpyDeviceToDevice, st));
+    {
+        ProfRegion pr(h, R_INTEGRATE);
+        count_launch();
+        k_rk_stage1<<<(N + 127) / 128, 128, 0, st>>>((const float4*)a->d_pos, (const float3*)a->d_ori, w.rk_pos,
+                                                      w.rk_posw, (float3*)w.rk_ori, (float4*)a->d_pos_gb,
+                                                      a->d_velocity, h->p.sqm_B1, a->d_b1_mask, noise, N, h->box,
+                                                      h->p.dt, a->shear_rate);
+        FSD_CHECK_CUDA(cudaGetLastError());
+    }
+    fsd_step_args a2 = *a;
+    a2.d_pos = (float*)w.rk_posw;
+    a2.d_ori = a->d_ori ? w.rk_ori : nullptr;
+    a2.d_pos_gb = nullptr;
+    a2.d_velocity = w.rk_vel;
+    e = compute_velocity(h, &a2);
+    if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+    if (e != FSD_OK) status = e;
+    ProfRegion pr(h, R_INTEGRATE);
+    count_launch();
+    k_rk_stage2<<<(N + 127) / 128, 128, 0, st>>>((float4*)a->d_pos, (float3*)a->d_ori, w.rk_pos,
+                                                  (const float3*)w.rk_ori, (float4*)a->d_pos_gb, w.rk_vel,
+                                                  h->p.sqm_B1, a->d_b1_mask, noise, (int3*)a->d_image, N, h->box,
+                                                  h->p.dt, a->shear_rate, 0.5f, 0.5f, 0.5f);
+    count_launch();
+    k_mean2<<<vb(6 * N), 256, 0, st>>>(a->d_velocity, w.rk_u1, w.rk_vel, 6 * (size_t)N);
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return status;
+}
+
+int step(fsd_handle* h, const fsd_step_args* a) {
+    int e;
+    if (h->p.integrator == 1) {
+        e = step_rk2(h, a);
+        if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+    } else {
+        e = compute_velocity(h, a);
+        if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+        const int ee = integrate_euler(h, a);
+        if (ee != FSD_OK) return ee;
+    }
     // Carried solver state (Stokes.cc:1658-1666).
     const unsigned t = a->timestep;
     if (t % 100 == 0 || h->m_lanczos_ff > 50) h->m_lanczos_ff = 3;
@@ -272,6 +447,7 @@ int fsd_compute_velocity(fsd_handle* h, const fsd_step_args* a) {
 
 int fsd_step(fsd_handle* h, const fsd_step_args* a) {
     if (!h || !a || !a->d_pos || !a->d_force || !a->d_velocity) return FSD_ERR_BAD_PARAMS;
+    if (h->p.integrator == 1 && !a->d_image) return FSD_ERR_BAD_PARAMS;
     const int st = step(h, a);
     h->info.status = st;
     return st;

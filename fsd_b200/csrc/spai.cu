@@ -158,43 +158,107 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
         for (int k = 0; k < 36; ++k) R[(size_t)(6 * a + k / 6) * 6 + k % 6] = blk ? (double)blk[k] : 0.0;
     }
     __syncthreads();
-    // Right-looking Cholesky in place, with the forward substitution L y = R
-    // carried along: row j of R is scaled by the pivot and eliminated from the
-    // rows below in the same parallel update as the trailing matrix.
+    // Right-looking block Cholesky on the 6x6 blocks of the particles, in
+    // place, with the forward substitution L y = R carried along: per block
+    // column, one thread factors the diagonal block, the rows below take
+    // their panel entries (one row per thread), then the trailing rows and
+    // right-hand sides are updated (one row per thread).  Three barriers per
+    // block column instead of three per scalar column.
     __shared__ int bad;
+    __shared__ double bsum[kSpaiThreads];
     if (threadIdx.x == 0) bad = 0;
     __syncthreads();
-    for (int j = 0; j < n; ++j) {
+    for (int jb = 0; jb < m; ++jb) {
+        const int j0 = 6 * jb;
         if (threadIdx.x == 0) {
-            const double d = H[tri(j, j)];
-            if (!(d > 0.0)) bad = 1;
-            H[tri(j, j)] = d > 0.0 ? sqrt(d) : 1.0;
+            for (int j = j0; j < j0 + 6; ++j) {
+                double d = H[tri(j, j)];
+                for (int q = j0; q < j; ++q) d -= H[tri(j, q)] * H[tri(j, q)];
+                if (!(d > 0.0)) {
+                    bad = 1;
+                    d = 1.0;
+                }
+                d = sqrt(d);
+                H[tri(j, j)] = d;
+                for (int i = j + 1; i < j0 + 6; ++i) {
+                    double v = H[tri(i, j)];
+                    for (int q = j0; q < j; ++q) v -= H[tri(i, q)] * H[tri(j, q)];
+                    H[tri(i, j)] = v / d;
+                }
+            }
         }
         __syncthreads();
-        const double piv = H[tri(j, j)];
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) H[tri(i, j)] /= piv;
-        if (threadIdx.x < 6) R[(size_t)j * 6 + threadIdx.x] /= piv;
-        __syncthreads();
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
-            const double lij = H[tri(i, j)];
-            for (int k = j + 1; k <= i; ++k) H[tri(i, k)] -= lij * H[tri(k, j)];
+        // panel: L[i][j0:j0+6] = H[i][j0:j0+6] L_jj^-T for the rows below
+        for (int i = j0 + 6 + threadIdx.x; i < n; i += blockDim.x) {
+            double l[6];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) R[(size_t)i * 6 + q] -= lij * R[(size_t)j * 6 + q];
+            for (int q = 0; q < 6; ++q) {
+                double v = H[tri(i, j0 + q)];
+                for (int p2 = 0; p2 < q; ++p2) v -= l[p2] * H[tri(j0 + q, j0 + p2)];
+                l[q] = v / H[tri(j0 + q, j0 + q)];
+            }
+#pragma unroll
+            for (int q = 0; q < 6; ++q) H[tri(i, j0 + q)] = l[q];
+        }
+        // right-hand side rows of this block: y = L_jj^-1 R (one column per thread)
+        if (threadIdx.x >= blockDim.x - 6) {
+            const int c = threadIdx.x - (blockDim.x - 6);
+            for (int q = 0; q < 6; ++q) {
+                double v = R[(size_t)(j0 + q) * 6 + c];
+                for (int p2 = 0; p2 < q; ++p2) v -= H[tri(j0 + q, j0 + p2)] * R[(size_t)(j0 + p2) * 6 + c];
+                R[(size_t)(j0 + q) * 6 + c] = v / H[tri(j0 + q, j0 + q)];
+            }
+        }
+        __syncthreads();
+        // trailing update of rows i >= j0 + 6 and their right-hand sides
+        for (int i = j0 + 6 + threadIdx.x; i < n; i += blockDim.x) {
+            double li[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) li[q] = H[tri(i, j0 + q)];
+            for (int k = j0 + 6; k <= i; ++k) {
+                const double* lk = H + tri(k, j0);
+                H[tri(i, k)] -= li[0] * lk[0] + li[1] * lk[1] + li[2] * lk[2] + li[3] * lk[3] + li[4] * lk[4] +
+                                li[5] * lk[5];
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                double v = 0.0;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) v += li[q] * R[(size_t)(j0 + q) * 6 + c];
+                R[(size_t)i * 6 + c] -= v;
+            }
         }
         __syncthreads();
     }
-    // Backward substitution L^T x = y, one warp per right-hand side.
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int q = warp; q < 6; q += blockDim.x >> 5) {
-        for (int i = n - 1; i >= 0; --i) {
-            double s = 0.0;
-            for (int k = i + 1 + lane; k < n; k += 32) s += H[tri(k, i)] * R[(size_t)k * 6 + q];
-            s = group_sum_d<32>(s);
-            if (lane == 0) R[(size_t)i * 6 + q] = (R[(size_t)i * 6 + q] - s) / H[tri(i, i)];
-            __syncwarp();
+    // Backward substitution L^T x = y by blocks: the coupling of block jb to
+    // the solved blocks below is summed by all threads ((q, c) pairs times
+    // four row ranges), then the 6x6 triangular solve (one column per thread).
+    for (int jb = m - 1; jb >= 0; --jb) {
+        const int j0 = 6 * jb;
+        const int t = threadIdx.x;
+        const int pc = t % 36, part = t / 36;  // parts 0..2 with 128 threads (t >= 108 idle)
+        double v = 0.0;
+        if (part < 3) {
+            const int q = pc / 6, c = pc % 6;
+            for (int i = j0 + 6 + part; i < n; i += 3) v += H[tri(i, j0 + q)] * R[(size_t)i * 6 + c];
         }
+        bsum[t] = v;
+        __syncthreads();
+        if (t < 36) {
+            const int q = t / 6, c = t % 6;
+            R[(size_t)(j0 + q) * 6 + c] -= bsum[t] + bsum[t + 36] + bsum[t + 72];
+        }
+        __syncthreads();
+        if (t < 6) {
+            const int c = t;
+            for (int q = 5; q >= 0; --q) {
+                double w = R[(size_t)(j0 + q) * 6 + c];
+                for (int p2 = q + 1; p2 < 6; ++p2) w -= H[tri(j0 + p2, j0 + q)] * R[(size_t)(j0 + p2) * 6 + c];
+                R[(size_t)(j0 + q) * 6 + c] = w / H[tri(j0 + q, j0 + q)];
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
     // Column c of G: block (s_a, c) = X block a, stored in row s_a at the
     // position of c in that row's set (the sets are mutual unless one was
     // truncated; a block without a slot is dropped).  A failed factorisation

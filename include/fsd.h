@@ -106,6 +106,14 @@ typedef struct fsd_params {
                                     call and keep the fastest (cached per process and grid shape).  Results then
                                     depend on the choice through the summation order, so runs in different
                                     processes may differ in the last bits.  0 (default): fixed shapes. */
+    int friction_type;           /* 0: none (default); 1: TYPE1, the frictional contact terms added to the
+                                    tabulated YA, YB, YC functions for gaps h <= friction_h0
+                                    (Stokes::setFriction, Stokes.cc:1132-1191) */
+    float friction_h0;           /* largest gap with frictional contact */
+    float friction_alpha[6];     /* strengths for YA11, YA12, YB11, YB12, YC11, YC12 */
+    int integrator;              /* 0: explicit Euler (Integrator_ExplicitEuler_Shear_kernel, the live path);
+                                    1: two-stage Runge-Kutta (Heun) of Integrator.cu:232-438, which evaluates
+                                    the velocity again at the Euler predictor with the same step's draws */
 } fsd_params;
 
 /* Derived PSE parameters (Stokes::setParams, Stokes.cc:118-696). */
@@ -154,6 +162,12 @@ const char* fsd_status_string(int status);
  * host_table when it is non-NULL and n_floats is large enough).  Touches no
  * GPU. */
 int fsd_pse_setup(const fsd_params* p, fsd_pse_info* info, float* host_table, size_t n_floats);
+
+/* The tabulated near-field resistance functions a handle with these
+ * parameters uses: dist (1000 floats) and vals (1000 x 22 floats), with the
+ * friction patch of Stokes::setFriction (Stokes.cc:1132-1191) applied when
+ * friction_type is 1.  Host only. */
+int fsd_resistance_table(const fsd_params* p, float* dist, float* vals);
 
 /* Reverse Cuthill-McKee ordering of an n-node graph given as 0-based CSR
  * adjacency (rows may include self loops); perm[new] = old.  Replaces the

@@ -1023,3 +1023,85 @@ def euler_shear(pos, ori, pos_gb, vel, image, L, xy, dt, shear_rate, B1=0.0, b1m
     pn = (q0 * q0 - qq)[:, None] * pv + 2 * qp[:, None] * qv + 2 * q0[:, None] * np.cross(qv, pv)
     pn /= np.linalg.norm(pn, axis=1, keepdims=True)
     return p, pn, gb, img
+
+
+# --------------------------------------------------- friction, Runge-Kutta
+def friction_table(tdist, tvals, h0, alpha):
+    """Stokes::setFriction TYPE1 (Stokes.cc:1132-1191): for gaps h = r - 2 <= h0
+    add alpha_k (2 h^2/h0^3 - 3 h/h0^2 + 1/h) in magnitude to YA11, YA12, YB11,
+    YB12, YC11, YC12 (entries 3, 4, 5, 6, 9, 10).  Single-precision h and
+    powers of h0, the bracket in double, the sum rounded to single precision,
+    as the reference's mix of float variables and double literals."""
+    vals = np.array(tvals, np.float32, copy=True).reshape(-1, 22)
+    h0 = F32(h0)
+    h02 = F32(h0 * h0)
+    h03 = F32(h0 * h02)
+    slots = (3, 4, 5, 6, 9, 10)
+    signs = (1, -1, -1, 1, 1, 1)
+    for i, d in enumerate(np.asarray(tdist, np.float32)):
+        h = F32(float(d) - 2.0)
+        if not h <= h0:
+            continue
+        h2 = F32(h * h)
+        bracket = 2.0 / float(h03) * float(h2) - 3.0 / float(h02) * float(h) + 1.0 / float(h)
+        for a, slot, sg in zip(alpha, slots, signs):
+            add = F32(float(F32(a)) * bracket)
+            vals[i, slot] = F32(vals[i, slot] + add) if sg > 0 else F32(vals[i, slot] - add)
+    return vals
+
+
+def _rotate(pv, w, t):
+    aw = np.linalg.norm(w, axis=1)
+    rot = aw > 1e-6
+    q0 = np.ones(len(pv))
+    qv = np.zeros_like(pv)
+    q0[rot] = np.cos(aw[rot] * t / 2)
+    qv[rot] = w[rot] / aw[rot, None] * np.sin(aw[rot] * t / 2)[:, None]
+    qq = np.einsum("ij,ij->i", qv, qv)
+    qp = np.einsum("ij,ij->i", qv, pv)
+    pn = (q0 * q0 - qq)[:, None] * pv + 2 * qp[:, None] * qv + 2 * q0[:, None] * np.cross(qv, pv)
+    return pn / np.linalg.norm(pn, axis=1, keepdims=True)
+
+
+def rk_stage1(pos, ori, pos_gb, vel, dt, shear_rate, B1=0.0, b1mask=None, noise=None):
+    """Integrator_ExplicitEuler1_Shear_kernel (Integrator.cu:232-330): the
+    unwrapped predictor, the director rotated by dt, half a step of pos_gb."""
+    p = xyz(pos).copy()
+    N = len(p)
+    V = np.asarray(vel, np.float64)[: 6 * N].reshape(N, 6)
+    v, w = V[:, :3].copy(), V[:, 3:].copy()
+    v[:, 0] += shear_rate * p[:, 1]
+    w[:, 2] -= shear_rate / 2.0
+    if noise is not None:
+        w += np.asarray(noise, np.float64)
+    pv = np.asarray(ori, np.float64)
+    m = np.ones(N) if b1mask is None else np.asarray(b1mask, np.float64)
+    v -= (-2.0 / 3.0 * B1 * m)[:, None] * pv
+    gb = np.asarray(pos_gb, np.float64).copy()
+    gb[:, 0] += (v[:, 0] - shear_rate * p[:, 1] + shear_rate * gb[:, 1]) * 0.5 * dt
+    gb[:, 1] += v[:, 1] * 0.5 * dt
+    gb[:, 2] += v[:, 2] * 0.5 * dt
+    return p + v * dt, _rotate(pv, w, dt), gb
+
+
+def rk_stage2(pos, ori, pos_star, ori_star, pos_gb, vel, image, L, xy, dt, shear_rate, B1=0.0, b1mask=None,
+              noise=None, c1=0.5, c2=0.5, c3=0.5):
+    """Integrator_RK_Shear_kernel (Integrator.cu:333-438)."""
+    p = c1 * xyz(pos) + c2 * xyz(pos_star)
+    N = len(p)
+    V = np.asarray(vel, np.float64)[: 6 * N].reshape(N, 6)
+    v, w = V[:, :3].copy(), V[:, 3:].copy()
+    v[:, 0] += shear_rate * p[:, 1]
+    w[:, 2] -= shear_rate / 2.0
+    if noise is not None:
+        w += np.asarray(noise, np.float64)
+    pv = c1 * np.asarray(ori, np.float64) + c2 * np.asarray(ori_star, np.float64)
+    pv /= np.linalg.norm(pv, axis=1, keepdims=True)
+    m = np.ones(N) if b1mask is None else np.asarray(b1mask, np.float64)
+    v -= (-2.0 / 3.0 * B1 * m)[:, None] * pv
+    gb = np.asarray(pos_gb, np.float64).copy()
+    gb[:, 0] += (v[:, 0] - shear_rate * p[:, 1] + shear_rate * gb[:, 1]) * 0.5 * dt
+    gb[:, 1] += v[:, 1] * 0.5 * dt
+    gb[:, 2] += v[:, 2] * 0.5 * dt
+    pn, img = wrap(p + v * dt * c3, np.asarray(image, np.int64), L, xy)
+    return pn, _rotate(pv, w, dt * c3), gb, img

@@ -87,6 +87,24 @@ def test_invalid_neighbour_list_kind_is_rejected():
         PSEv3(sysm.all, T=1.0, nlist_type="octree", system=sysm)
 
 
+def test_set_friction_follows_the_reference_types():
+    """setFriction (Stokes.cc:1132-1191) takes NONE or TYPE1 with six
+    strengths and must precede AllocateWorkSpaces; other types raise as the
+    reference does."""
+    from fsd_b200 import _PSEv3
+    from fsd_b200.system import System
+    sysm = System(np.zeros((2, 4)), (20.0, 20.0, 20.0, 0.0), dt=1e-4, device="cpu")
+    st = _PSEv3.Stokes(sysm, sysm.all, lambda t: 1.0, 0, "CELL", 0.5, 1e-3, "stresslet", 0, 0.1, 20.0, 1e4, 0.0, 1e-5,
+                       0.0, 0.0, 1, 1.0, 1.0, 0.0, 0.0, 0.0)
+    st.setFriction("TYPE1", 0.05, [0.5, 0.3, 0.2, 0.1, 0.4, 0.25])
+    assert st.solver["friction_type"] == 1 and st.solver["friction_h0"] == 0.05
+    assert st.solver["friction_alpha"] == [0.5, 0.3, 0.2, 0.1, 0.4, 0.25]
+    st.setFriction("none", 0.0, [0.0] * 6)
+    assert st.solver["friction_type"] == 0
+    with pytest.raises(RuntimeError):
+        st.setFriction("TYPE2", 0.05, [0.0] * 6)
+
+
 @pytest.mark.gpu
 def test_psev3_steps_and_writes_output(cuda, tmp_path):
     from fsd_b200.configs import suspension

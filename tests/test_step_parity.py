@@ -21,8 +21,9 @@ against the FP64 oracle.
   fsd_rfd_drift at the same timestep on a fresh handle, which draw the same
   counter-based normals).  Once without and once with the active terms
   (squirmer B1/B2 with masks, rotational noise, external torque).  Velocities
-  and stresslets to 1e-4 (GMRES to 1e-6), displacements to 1e-4, images
-  exactly.
+  and stresslets to 1e-4 (GMRES to 3e-6: the random finite difference
+  solves of this sheared, tilted case stop at an FP32 residual floor near
+  1.5e-6), displacements to 1e-4, images exactly.
 """
 from __future__ import annotations
 
@@ -122,7 +123,7 @@ def test_full_brownian_step_matches_oracle(cuda, active):
     pos, Lc = suspension(N, phi, seed)
     L = (Lc, Lc, Lc)
     rng = np.random.default_rng(seed)
-    kw = dict(T=T, dt=dt, seed=11, solver_tol=1e-6, gmres_max_iter=4000, period=1, precond="learned",
+    kw = dict(T=T, dt=dt, seed=11, solver_tol=3e-6, gmres_max_iter=4000, period=1, precond="learned",
               lanczos_tol=1e-4)
     ori = np.tile([0.0, 0.0, 1.0], (N, 1)).astype(np.float32)
     b1m = b2m = None
