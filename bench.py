@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--phi", type=float, default=0.4)
     ap.add_argument("--precond", default="learned", choices=["ichol", "none", "learned"])
     ap.add_argument("--inner", type=int, default=6, help="inner GMRES steps of the learned preconditioner")
+    ap.add_argument("--poly", type=int, default=10,
+                    help="terms of the learned inner polynomial (0: inner GMRES steps instead)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the no-network forms")
     ap.add_argument("--no-ichol", action="store_true", help="skip the IChol comparison run")
     ap.add_argument("--no-net", action="store_true", help="learned preconditioner without the network correction")
     ap.add_argument("--no-autotune", action="store_true", help="fixed spreading tiles and FFT batches")
@@ -154,25 +157,42 @@ SINGLE_KERNEL_REGIONS = {"fft": 1, "spread": 1, "contract": 1, "green": 1, "real
 WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_precond.f32"
 
 
-def precond_form(args, net):
+def precond_form(args, net, form=None):
     if args.precond == "ichol":
         return "RCM + block IC(0) of the pruned lubrication block (the reference's preconditioner)"
     if args.precond == "none":
         return "identity"
-    form = f"two-hop sparse approximate inverse + {args.inner} inner GMRES steps, flexible outer GMRES"
-    return form + (", trained network correction" if net else ", no network")
+    form = form or ("poly" if args.poly >= 2 else "gmres")
+    if form == "poly":
+        src = ("coefficients predicted by the trained message-passing network (checked on a probe at every build)"
+               if net else "coefficients fitted to four probe vectors at every build (no network)")
+        return (f"two-hop sparse approximate inverse G, inner Chebyshev polynomial y = G q(AG) t of "
+                f"{args.poly} terms, {src}; plain outer GMRES")
+    return (f"two-hop sparse approximate inverse + {args.inner} inner GMRES steps, flexible outer GMRES"
+            + (", trained network correction" if net else ", no network"))
 
 
-def make_solver(args, precond, N, L, dev, seed):
+def poly_weights(k):
+    return ROOT / "fsd_b200" / "data" / f"learned_poly_k{k}.f32"
+
+
+def make_solver(args, precond, N, L, dev, seed, form=None):
+    """form (learned only): "poly" = the network's inner polynomial (a fitted
+    polynomial when no weights ship or with net=False), "gmres" = inner GMRES
+    steps on the approximate inverse; default from --poly."""
     from fsd_b200.core import FSD
 
+    form = form or ("poly" if args.poly >= 2 else "gmres")
+    poly = precond == "learned" and form == "poly"
     s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=seed, error=1e-3, solver_tol=1e-4,
             lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=precond, period=0, gmres_max_iter=3000,
-            gmres_restart=200 if precond == "ichol" else 100, learned_inner=args.inner if precond == "learned" else 0,
-            autotune=0 if args.no_autotune else 1)
+            gmres_restart=200 if precond == "ichol" else 100,
+            learned_inner=args.inner if (precond == "learned" and not poly) else 0,
+            learned_poly=args.poly if poly else 0, autotune=0 if args.no_autotune else 1)
     net = False
-    if precond == "learned" and WEIGHTS.exists() and not args.no_net:
-        s.learned_set_weights(np.fromfile(WEIGHTS, "<f4"))
+    wf = poly_weights(args.poly) if poly else WEIGHTS
+    if precond == "learned" and wf.exists() and not args.no_net:
+        s.learned_set_weights(np.fromfile(wf, "<f4"))
         net = True
     return s, net
 
@@ -347,6 +367,23 @@ def run_fsd(args, ws, rank, local):
         ichol = {"value": ws * args.ichol_steps / (r["total_ms"] / 1e3), "unit": "steps/s",
                  "ms_per_step": r["total_ms"] / args.ichol_steps, "steps": args.ichol_steps, "warmup": 1,
                  "iterations_per_step": r["iters"]}
+    # --- the preconditioner's forms without the network, on the same steps of
+    # the same trajectory: the approximate inverse with inner GMRES steps, and
+    # the polynomial fitted to probe vectors at every build
+    no_network = {}
+    if args.precond == "learned" and not args.no_compare:
+        forms = {"spai_inner_gmres": "gmres"}
+        if args.poly >= 2:
+            forms["fitted_polynomial"] = "poly"
+        for name, form in forms.items():
+            a2 = argparse.Namespace(**vars(args))
+            a2.no_net = True
+            sc, _ = make_solver(a2, "learned", N, L, dev, 1 + rank, form=form)
+            r = timed_steps(a2, sc, fresh_state(), args.steps, args.warmup, dev, ws)
+            sc.close()
+            no_network[name] = {"value": ws * args.steps / (r["total_ms"] / 1e3), "unit": "steps/s",
+                                "ms_per_step": r["total_ms"] / args.steps, "iterations_per_step": r["iters"],
+                                "precond_form": precond_form(a2, False, form)}
     # --- roofline of the dominant single-kernel region (profiled pass)
     regions = prof["regions"]
     prof_steps = prof["steps"]
@@ -371,7 +408,8 @@ def run_fsd(args, ws, rank, local):
         "data": "synthetic: seeded random sequential addition + overlap relaxation, min gap 1e-3",
         "config": {"workload": workload_name(N, phi), "N": N, "phi": phi,
                    "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
-                   "learned_inner": args.inner if args.precond == "learned" else None, "learned_network": net,
+                   "learned_inner": args.inner if (args.precond == "learned" and args.poly < 2) else None,
+                   "learned_poly": args.poly if args.precond == "learned" else None, "learned_network": net,
                    "precond_form": precond_form(args, net),
                    "autotune": not args.no_autotune,
                    "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
@@ -384,6 +422,10 @@ def run_fsd(args, ws, rank, local):
                                   "with it off"},
         "ichol": ichol,
         "speedup_vs_ichol": (value / ichol["value"]) if ichol else None,
+        "no_network": no_network,
+        "speedup_vs_ichol_no_network": {k: v["value"] / ichol["value"] for k, v in no_network.items()} if ichol
+        else None,
+        "speedup_vs_no_network": {k: value / v["value"] for k, v in no_network.items()},
         "clocks": main["clocks"],
     }
     if rank == 0:
@@ -553,9 +595,6 @@ def run_reference(args, ws, rank):
             "wall_s": time.time() - t_all}
 
 
-POLY_WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_poly_k8.f32"
-
-
 def run_config5(args, local):
     """Learned preconditioner on dense suspensions (N = 32768 at phi 0.45,
     0.5, 0.55, shear rate 1, kT = 1) on held-out seeds: one velocity
@@ -573,19 +612,20 @@ def run_config5(args, local):
     forms = {
         "ichol": dict(precond="ichol", gmres_restart=200, learned_inner=0),
         "spai_gmres6": dict(precond="learned", gmres_restart=100, learned_inner=6),
-        "learned_poly8": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=8),
+        "fitted_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10),
+        "learned_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10),
     }
-    w = np.fromfile(POLY_WEIGHTS, "<f4") if POLY_WEIGHTS.exists() else None
+    w = np.fromfile(poly_weights(10), "<f4") if poly_weights(10).exists() else None
     results = {}
     for phi in args.config5_phis:
         pos, L = suspension(N, phi, seed=1000 + int(round(phi * 100)))  # seeds the training never used
         res = {}
         for name, kw in forms.items():
-            if name == "learned_poly8" and w is None:
+            if name == "learned_poly10" and w is None:
                 continue
             s = FSD(N, (L, L, L, 0.0), device=dev, T=1.0, dt=1e-4, seed=7, solver_tol=1e-4, lanczos_tol=1e-3,
                     rfd_epsilon=1e-3, period=0, gmres_max_iter=4000, **kw)
-            if name == "learned_poly8":
+            if name == "learned_poly10":
                 s.learned_set_weights(w)
             times, iters, resid = [], [], []
             for rep in range(2):  # the first call also captures graphs and tunes
@@ -609,6 +649,9 @@ def run_config5(args, local):
                 resid.append(si["gmres_resid"])
             s.close()
             res[name] = {"outer_iterations": iters[-1], "residuals": resid[-1], "ms": times[-1]}
+            if "poly" in name:
+                res[name].update(poly_source=si["poly_source"], poly_loss_net=si["poly_loss_net"],
+                                 poly_loss_fit=si["poly_loss_fit"])
         results[str(phi)] = res
     return {"metric": "config 5: learned preconditioner on held-out dense suspensions, one velocity computation "
                       "(three saddle solves to 1e-4)", "unit": "ms", "N": N, "higher_is_better": False,

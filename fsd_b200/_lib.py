@@ -63,6 +63,7 @@ class fsd_solve_info(C.Structure):
         ("ichol_attempts", C.c_int), ("ichol_relaxer", C.c_float),
         ("nlist_max", C.c_int), ("status", C.c_int), ("ichol_shifted", C.c_int),
         ("ichol_gain", C.c_float),
+        ("poly_source", C.c_int), ("poly_loss_net", C.c_float), ("poly_loss_fit", C.c_float),
     ]
 
 
@@ -115,7 +116,7 @@ _SIGS = {
     "fsd_learned_train_step": (C.c_int, [H, P, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float), P]),
     "fsd_learned_set_poly": (C.c_int, [H, P, C.c_int]),
     "fsd_learned_get_poly": (C.c_int, [H, P, C.c_int]),
-    "fsd_learned_poly_train_step": (C.c_int, [H, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float),
+    "fsd_learned_poly_train_step": (C.c_int, [H, P, C.c_int, C.c_uint, C.c_float, C.c_int, C.POINTER(C.c_float),
                                               C.POINTER(C.c_float), P, P, P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),
     "fsd_saddle_solve": (C.c_int, [H, P, P, P, C.POINTER(C.c_int), C.POINTER(C.c_float)]),

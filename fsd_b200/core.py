@@ -246,7 +246,7 @@ class FSD:
         k = self.params.learned_poly
         return buf[:k].copy(), float(buf[16])
 
-    def learned_poly_train_step(self, pos, n_probes=4, step=0, lr=0.0, want_grad=False):
+    def learned_poly_train_step(self, pos, n_probes=4, step=0, lr=0.0, want_grad=False, natural=False):
         """Inner-polynomial loss of this configuration with the network's
         coefficients, its least-squares optimum, both coefficient sets, the
         weight gradient (when want_grad) and, for lr > 0, one Adam step."""
@@ -256,7 +256,7 @@ class FSD:
         coef, copt = np.zeros(k, np.float32), np.zeros(k, np.float32)
         g = np.zeros(lib().fsd_learned_num_weights(), np.float32) if want_grad else None
         check(lib().fsd_learned_poly_train_step(self._h, _ptr(pos), int(n_probes), int(step), float(lr),
-                                                C.byref(loss), C.byref(loss_opt),
+                                                int(bool(natural)), C.byref(loss), C.byref(loss_opt),
                                                 g.ctypes.data_as(C.c_void_p) if want_grad else None,
                                                 coef.ctypes.data_as(C.c_void_p), copt.ctypes.data_as(C.c_void_p)),
               "fsd_learned_poly_train_step")

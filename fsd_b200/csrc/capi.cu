@@ -401,6 +401,10 @@ int fsd_get_pse_info(const fsd_handle* h, fsd_pse_info* info) {
 int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info) {
     if (!h || !info) return FSD_ERR_BAD_PARAMS;
     *info = h->info;
+    const LearnedState* ls = (const LearnedState*)h->learned;
+    info->poly_source = ls ? ls->poly_source : 0;
+    info->poly_loss_net = ls ? ls->poly_loss_net : -1.f;
+    info->poly_loss_fit = ls ? ls->poly_loss_fit : -1.f;
     return FSD_OK;
 }
 
@@ -537,13 +541,13 @@ int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n) {
 }
 
 int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
-                                float* loss, float* loss_opt, float* host_grad, float* host_coef,
+                                int natural, float* loss, float* loss_opt, float* host_grad, float* host_coef,
                                 float* host_coef_opt) {
     if (!h || !d_pos || !h->nlist_valid || n_probes < 1 || n_probes > 64) return FSD_ERR_BAD_PARAMS;
     const int k = h->p.learned_poly;
     if (k < 2) return FSD_ERR_BAD_PARAMS;
-    return mpnn_poly_train_step(h, (const float4*)d_pos, n_probes, step, lr, k, loss, loss_opt, host_grad, host_coef,
-                                host_coef_opt);
+    return mpnn_poly_train_step(h, (const float4*)d_pos, n_probes, step, lr, k, natural, loss, loss_opt, host_grad,
+                                host_coef, host_coef_opt);
 }
 
 int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_probes, int n_probes,

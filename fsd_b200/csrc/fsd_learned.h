@@ -50,6 +50,9 @@ struct LearnedState {
     double* pnrm = nullptr;
     unsigned* pticket = nullptr;
     bool poly_user = false;   // coefficients set through fsd_learned_set_poly (else the network's)
+    int poly_source = 0;      // coefficients in use: 1 network, 2 least-squares fit, 3 caller's
+    float poly_loss_net = -1.f, poly_loss_fit = -1.f;  // held-out probe losses of the last build's check
+    unsigned poly_builds = 0; // builds so far (the check's probe draws)
     cudaGraph_t pgraph = nullptr;
     cudaGraphExec_t pexec = nullptr;
     cudaGraphNode_t pnode_first = nullptr, pnode_last = nullptr;
@@ -90,7 +93,9 @@ int mpnn_train_step(fsd_handle* h, const float4* pos, const float* host_probes, 
 // Polynomial coefficients for this configuration from the network (mean over
 // particles of the node head's first k outputs) into pc[0:k].
 int mpnn_poly_coeffs(fsd_handle* h, const float4* pos, float* pc, int k);
-int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, float* loss_out,
-                         float* loss_opt_out, float* host_grad, float* host_coef, float* host_coef_opt);
+int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, int natural,
+                         float* loss_out, float* loss_opt_out, float* host_grad, float* host_coef,
+                         float* host_coef_opt);
+int mpnn_poly_calibrate(fsd_handle* h, int k, uint32_t step);
 
 }  // namespace fsd

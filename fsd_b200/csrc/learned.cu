@@ -522,7 +522,6 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
     ProfRegion pr(h, R_PRECOND_BUILD);
     int e = FSD_OK;
     const bool poly = h->p.learned_poly >= 2;
-    if (poly && !s->poly_user && !mpnn_loaded(h)) return FSD_ERR_BAD_PARAMS;  // no coefficients to use
     if (poly) e = poly_alloc(h);
     else if (h->p.learned_inner > 0) e = inner_alloc(h);
     if (e != FSD_OK) return e;
@@ -539,12 +538,21 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
         }
     }
     if (poly) {
-        if (!s->poly_user) {
-            e = mpnn_poly_coeffs(h, pos, s->pc, h->p.learned_poly);
-            if (e != FSD_OK) return e;
-        }
         e = poly_lambda(h);
         if (e != FSD_OK) return e;
+        if (s->poly_user) {
+            s->poly_source = 3;
+        } else {
+            // the network's coefficients for this configuration, checked
+            // against a least-squares fit on held-out probes (or the fit alone
+            // without a network)
+            if (mpnn_loaded(h)) {
+                e = mpnn_poly_coeffs(h, pos, s->pc, h->p.learned_poly);
+                if (e != FSD_OK) return e;
+            }
+            e = mpnn_poly_calibrate(h, h->p.learned_poly, ++s->poly_builds);
+            if (e != FSD_OK) return e;
+        }
     }
     h->pc_valid = true;
     return FSD_OK;

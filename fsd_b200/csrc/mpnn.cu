@@ -1253,17 +1253,19 @@ static bool solve_small(std::vector<double> M, std::vector<double> g, int k, std
     return true;
 }
 
-int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, float* loss_out,
-                         float* loss_opt_out, float* host_grad, float* host_coef, float* host_coef_opt) {
+// Gram entries of P probe vectors t_p drawn from (seed, step) for the
+// current G, A and spectral bound: tt = t.t, g_m = W_m . t, M_ml = W_m . W_l
+// with W_m = AG T_m(S) t (S = (2/lambda) AG - I), m, l < k.
+struct PolyGram {
+    double tt = 0.0;
+    std::vector<double> g, M;
+};
+
+static int poly_gram(fsd_handle* h, int P, uint32_t step, int k, std::vector<PolyGram>& out) {
     LearnedState* ls = learned(h);
-    if (!mpnn_loaded(h) || P < 1 || k < 2 || k > kMaxPoly) return FSD_ERR_BAD_PARAMS;
     MpState* s = mp(h);
     cudaStream_t st = h->stream;
-    MP_TRY(poly_alloc(h));
-    MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
-    MP_TRY(spai_build(h));
-    MP_TRY(poly_lambda(h));
-    MP_TRY(mpnn_poly_coeffs(h, pos, ls->pc, k));
+    MP_TRY(mp_alloc_static(h));
     MP_TRY(mp_probes(h, P));
     const int N = s->N;
     const size_t n6 = 6 * (size_t)N, nP = (size_t)P * n6;
@@ -1281,7 +1283,6 @@ int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step,
         MP_TRY(grow(&s->gpart, ngp));
         s->gpart_cap = ngp;
     }
-    // probes t and the images W_m = AG B_m of the Chebyshev vectors B_m = T_m(S) t
     gaussian(h, s->Zp, nP, step, kStreamLearned, 1.0f);
     const int rows = (8 * N + 255) / 256;
     const float* Bprev = nullptr;
@@ -1293,31 +1294,24 @@ int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step,
         count_launch();
         k_pruned_multi<<<rows, 256, 0, st>>>(ls->a_pn, ls->a_plist, ls->a_blocks, s->Up, Wm, N, P);
         if (m + 1 < k) {
-            float* out = s->pb + (size_t)(m % 3) * nP;
+            float* o = s->pb + (size_t)(m % 3) * nP;
             count_launch();
-            k_cheb_next<<<nblk(nP), kThreads, 0, st>>>(Wm, Bm, Bprev, nP, ls->pc, m == 0 ? 1.0f : 2.0f, out);
+            k_cheb_next<<<nblk(nP), kThreads, 0, st>>>(Wm, Bm, Bprev, nP, ls->pc, m == 0 ? 1.0f : 2.0f, o);
             Bprev = Bm;
-            Bm = out;
+            Bm = o;
         }
     }
     count_launch();
     k_poly_gram<<<dim3(kGramBlocks, P), 256, 0, st>>>(s->Zp, s->pw, k, P, n6, s->gpart);
     FSD_CHECK_CUDA(cudaGetLastError());
     std::vector<double> part(ngp);
-    std::vector<float> c32(kMaxPoly + 1);
     FSD_CHECK_CUDA(cudaMemcpyAsync(part.data(), s->gpart, sizeof(double) * ngp, cudaMemcpyDeviceToHost, st));
-    FSD_CHECK_CUDA(cudaMemcpyAsync(c32.data(), ls->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaStreamSynchronize(st));
-    // Gram entries per probe, loss, gradient and the least-squares optimum
     auto pair_index = [&](int a, int b) {
         if (a > b) std::swap(a, b);
         return a * nvec - a * (a - 1) / 2 + (b - a);
     };
-    std::vector<double> c(k), grad(k, 0.0), Ms(k * k, 0.0), gs(k, 0.0);
-    for (int m = 0; m < k; ++m) c[m] = c32[m];
-    double loss = 0.0;
-    std::vector<std::vector<double>> Mp(P, std::vector<double>(k * k)), gp(P, std::vector<double>(k));
-    std::vector<double> ttp(P);
+    out.assign(P, PolyGram());
     for (int p = 0; p < P; ++p) {
         auto entry = [&](int a, int b) {
             const double* q = part.data() + ((size_t)p * npairs + pair_index(a, b)) * kGramBlocks;
@@ -1325,38 +1319,119 @@ int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step,
             for (int blk = 0; blk < kGramBlocks; ++blk) v += q[blk];
             return v;
         };
-        const double tt = entry(0, 0);
-        ttp[p] = tt;
+        PolyGram& G = out[p];
+        G.tt = entry(0, 0);
+        G.g.resize(k);
+        G.M.resize((size_t)k * k);
         for (int m = 0; m < k; ++m) {
-            gp[p][m] = entry(0, 1 + m);
-            for (int l = 0; l < k; ++l) Mp[p][m * k + l] = entry(1 + m, 1 + l);
+            G.g[m] = entry(0, 1 + m);
+            for (int l = 0; l < k; ++l) G.M[(size_t)m * k + l] = entry(1 + m, 1 + l);
         }
+    }
+    return FSD_OK;
+}
+
+// Mean relative residual E ||t - W c||^2 / ||t||^2 over probes [p0, p1).
+static double poly_loss(const std::vector<PolyGram>& gr, int p0, int p1, const std::vector<double>& c) {
+    const int k = (int)c.size();
+    double loss = 0.0;
+    for (int p = p0; p < p1; ++p) {
         double cMc = 0.0, cg = 0.0;
         for (int m = 0; m < k; ++m) {
-            cg += c[m] * gp[p][m];
-            double Mc = 0.0;
-            for (int l = 0; l < k; ++l) Mc += Mp[p][m * k + l] * c[l];
-            cMc += c[m] * Mc;
-            grad[m] += 2.0 * (Mc - gp[p][m]) / (tt * P);
-            gs[m] += gp[p][m] / tt;
-            for (int l = 0; l < k; ++l) Ms[m * k + l] += Mp[p][m * k + l] / tt;
+            cg += c[m] * gr[p].g[m];
+            for (int l = 0; l < k; ++l) cMc += c[m] * gr[p].M[(size_t)m * k + l] * c[l];
         }
-        loss += (tt - 2.0 * cg + cMc) / (tt * P);
+        loss += (gr[p].tt - 2.0 * cg + cMc) / gr[p].tt;
     }
+    return loss / (p1 - p0);
+}
+
+// Least-squares coefficients over probes [p0, p1); false if singular.
+static bool poly_fit(const std::vector<PolyGram>& gr, int p0, int p1, int k, std::vector<double>& c) {
+    std::vector<double> Ms((size_t)k * k, 0.0), gs(k, 0.0);
+    for (int p = p0; p < p1; ++p)
+        for (int m = 0; m < k; ++m) {
+            gs[m] += gr[p].g[m] / gr[p].tt;
+            for (int l = 0; l < k; ++l) Ms[(size_t)m * k + l] += gr[p].M[(size_t)m * k + l] / gr[p].tt;
+        }
+    return solve_small(Ms, gs, k, c);
+}
+
+// Check of the polynomial at every build.  With a network, its coefficients
+// are scored on one probe vector and kept when the relative residual they
+// leave, ||t - AG q(AG) t||^2 / ||t||^2, is at most kPolyAccept (a residual
+// reduction of about 0.22); otherwise, and without a network, four probe
+// vectors give a least-squares fit of the coefficients, which is used.  The
+// choice and the losses are recorded in the learned state.
+constexpr double kPolyAccept = 0.05;
+
+int mpnn_poly_calibrate(fsd_handle* h, int k, uint32_t step) {
+    LearnedState* ls = learned(h);
+    const bool net = mpnn_loaded(h);
+    ls->poly_loss_net = -1.f;
+    ls->poly_loss_fit = -1.f;
+    std::vector<PolyGram> gr;
+    if (net) {
+        float c32[kMaxPoly + 1];
+        FSD_CHECK_CUDA(cudaMemcpyAsync(c32, ls->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, h->stream));
+        MP_TRY(poly_gram(h, 1, 2 * step, k, gr));  // synchronises the stream
+        std::vector<double> cnet(k);
+        for (int m = 0; m < k; ++m) cnet[m] = c32[m];
+        const double lnet = poly_loss(gr, 0, 1, cnet);
+        ls->poly_loss_net = (float)lnet;
+        if (lnet <= kPolyAccept) {
+            ls->poly_source = 1;
+            return FSD_OK;
+        }
+    }
+    MP_TRY(poly_gram(h, 4, 2 * step + 1, k, gr));
+    std::vector<double> cfit;
+    if (!poly_fit(gr, 0, 4, k, cfit)) return FSD_ERR_BREAKDOWN;
+    ls->poly_loss_fit = (float)poly_loss(gr, 0, 4, cfit);
+    float c[kMaxPoly] = {};
+    for (int m = 0; m < k; ++m) c[m] = (float)cfit[m];
+    FSD_CHECK_CUDA(cudaMemcpyAsync(ls->pc, c, sizeof(float) * kMaxPoly, cudaMemcpyHostToDevice, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    ls->poly_source = 2;
+    return FSD_OK;
+}
+
+int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step, float lr, int k, int natural,
+                         float* loss_out, float* loss_opt_out, float* host_grad, float* host_coef,
+                         float* host_coef_opt) {
+    LearnedState* ls = learned(h);
+    if (!mpnn_loaded(h) || P < 1 || k < 2 || k > kMaxPoly) return FSD_ERR_BAD_PARAMS;
+    MpState* s = mp(h);
+    cudaStream_t st = h->stream;
+    MP_TRY(poly_alloc(h));
+    MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
+    MP_TRY(spai_build(h));
+    MP_TRY(poly_lambda(h));
+    MP_TRY(mpnn_poly_coeffs(h, pos, ls->pc, k));
+    std::vector<float> c32(kMaxPoly + 1);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(c32.data(), ls->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, st));
+    std::vector<PolyGram> gr;
+    MP_TRY(poly_gram(h, P, step, k, gr));
+    const int N = s->N;
+    std::vector<double> c(k), grad(k, 0.0);
+    for (int m = 0; m < k; ++m) c[m] = c32[m];
+    const double loss = poly_loss(gr, 0, P, c);
+    for (int p = 0; p < P; ++p)
+        for (int m = 0; m < k; ++m) {
+            double Mc = 0.0;
+            for (int l = 0; l < k; ++l) Mc += gr[p].M[(size_t)m * k + l] * c[l];
+            grad[m] += 2.0 * (Mc - gr[p].g[m]) / (gr[p].tt * P);
+        }
     std::vector<double> copt;
     double loss_opt = -1.0;
-    if (solve_small(Ms, gs, k, copt)) {
-        loss_opt = 0.0;
-        for (int p = 0; p < P; ++p) {
-            double cMc = 0.0, cg = 0.0;
-            for (int m = 0; m < k; ++m) {
-                cg += copt[m] * gp[p][m];
-                for (int l = 0; l < k; ++l) cMc += copt[m] * Mp[p][m * k + l] * copt[l];
-            }
-            loss_opt += (ttp[p] - 2.0 * cg + cMc) / (ttp[p] * P);
-        }
-    }
-    // backward: the node head's outputs each carry dL/dc / N
+    if (poly_fit(gr, 0, P, k, copt)) loss_opt = poly_loss(gr, 0, P, copt);
+    // The loss is quadratic in c with Hessian 2 Mbar (Mbar = mean_p M_p / tt_p),
+    // badly conditioned in the Chebyshev coefficients.  With `natural` the
+    // network is fed the Gauss-Newton direction Mbar^-1 dL/dc = 2 (c - c_opt)
+    // instead of dL/dc.
+    if (natural && !copt.empty())
+        for (int m = 0; m < k; ++m) grad[m] = 2.0 * (c[m] - copt[m]);
+    // backward: the node head's outputs each carry the gradient / N
     MP_TRY(mp_alloc_backward(h));
     PolyGrad pg{};
     for (int m = 0; m < k; ++m) pg.g[m] = (float)(grad[m] / N);

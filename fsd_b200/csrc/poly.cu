@@ -241,9 +241,7 @@ int poly_alloc(fsd_handle* h) {
 }
 
 bool poly_active(const fsd_handle* h) {
-    const LearnedState* s = (const LearnedState*)h->learned;
-    return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_poly >= 2 && s &&
-           (s->poly_user || (s->mp && mpnn_loaded(const_cast<fsd_handle*>(h))));
+    return h->p.precond == FSD_PRECOND_LEARNED && h->p.learned_poly >= 2;
 }
 
 // Upper bound of the spectrum of AG into pc[kMaxPoly]: kPowerIters power

@@ -137,6 +137,11 @@ typedef struct fsd_solve_info {
     int status;                  /* fsd_status of that call */
     int ichol_shifted;           /* pivot blocks that needed a local shift */
     float ichol_gain;            /* power-iteration estimate of lambda_max(G) of the accepted factor */
+    int poly_source;             /* learned_poly: coefficients of the last build, 1 the network's, 2 a
+                                    least-squares fit on probe vectors, 3 the caller's (0: not in use) */
+    float poly_loss_net;         /* probe loss ||t - AG q(AG) t||^2/||t||^2 of the network's coefficients at
+                                    the last build (-1: none) */
+    float poly_loss_fit;         /* loss of the least-squares fit on its four probes (-1: not fitted) */
 } fsd_solve_info;
 
 /* Arguments of one time step (Stokes_StepOne, Stokes.cuh:81-108). */
@@ -311,11 +316,19 @@ int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_
  * from the network; its least-squares optimum over all coefficients
  * (loss_opt, host_coef_opt, both optional); the network's coefficients
  * (host_coef, optional, k floats); the weight gradient (host_grad,
- * optional); and, when lr > 0, one Adam step. */
+ * optional); and, when lr > 0, one Adam step.  With natural != 0 the
+ * network is fed the Gauss-Newton direction 2 (c - c_opt) in place of the
+ * loss gradient (the loss is quadratic in c with a badly conditioned
+ * Hessian); host_grad then holds that direction's weight gradient.
+ * At every build in learned_poly mode without caller's coefficients, the
+ * network's coefficients are scored on one probe vector and kept when the
+ * relative residual they leave, ||t - AG q(AG) t||^2 / ||t||^2, is at most
+ * 0.05; otherwise, and without a network, a least-squares fit on four probe
+ * vectors is used (fsd_solve_info poly_source and the losses). */
 int fsd_learned_set_poly(fsd_handle* h, const float* host_c, int k);
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n);
 int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
-                                float* loss, float* loss_opt, float* host_grad, float* host_coef,
+                                int natural, float* loss, float* loss_opt, float* host_grad, float* host_coef,
                                 float* host_coef_opt);
 /* x = P^-1 b (Saddle_Preconditioner, Saddle.cu:171).  x and b may alias. */
 int fsd_precond_apply(fsd_handle* h, const float* d_b, float* d_x);
