@@ -463,7 +463,11 @@ int rfd_drift(fsd_handle* h, const float4* pos, uint32_t step, float* drift6) {
     int st = saddle_solve(h, w.pos_prime, w.rfd_rhs, w.rfd_sol, h->p.solver_tol, &it, &res);
     h->info.gmres_iters[0] = it;
     h->info.gmres_resid[0] = res;
-    if (st != FSD_OK) return st;
+    // A solve that stops above its tolerance keeps its best solution, as the
+    // reference continues after its non-convergence message (Solvers.cu:121).
+    int status = FSD_OK;
+    if (st == FSD_ERR_GMRES_MAXIT) status = st;
+    else if (st != FSD_OK) return st;
     FSD_CHECK_CUDA(cudaMemcpyAsync(w.vel, w.rfd_sol + 11 * N, sizeof(float) * 6 * N, cudaMemcpyDeviceToDevice,
                                    h->stream));
     count_launch();
@@ -471,12 +475,13 @@ int rfd_drift(fsd_handle* h, const float4* pos, uint32_t step, float* drift6) {
     st = saddle_solve(h, w.pos_prime, w.rfd_rhs, w.rfd_sol, h->p.solver_tol, &it, &res);
     h->info.gmres_iters[1] = it;
     h->info.gmres_resid[1] = res;
-    if (st != FSD_OK) return st;
+    if (st == FSD_ERR_GMRES_MAXIT) status = st;
+    else if (st != FSD_OK) return st;
     count_launch();
     k_rfd_finish<<<(6 * N + 255) / 256, 256, 0, h->stream>>>(drift6, w.vel, w.rfd_sol + 11 * N, N, h->p.T / eps);
     // Positions used by the mobility bins must be rebinned for x on the next matvec.
     FSD_CHECK_CUDA(cudaGetLastError());
-    return FSD_OK;
+    return status;
 }
 
 }  // namespace fsd

@@ -285,6 +285,7 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
     }
     const uint32_t step = a->timestep;
     int lanczos_status = FSD_OK;
+    int solve_status = FSD_OK;  // a solve that stopped above its tolerance (kept, reported)
     if (h->p.T > 0.f) {
         e = brownian_farfield(h, pos, step, rhs);
         if (e == FSD_ERR_LANCZOS_MAXIT) lanczos_status = e;
@@ -293,7 +294,8 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
         if (e == FSD_ERR_LANCZOS_MAXIT) lanczos_status = e;
         else if (e != FSD_OK) return e;
         e = rfd_drift(h, pos, step, vel);
-        if (e != FSD_OK) return e;
+        if (e == FSD_ERR_GMRES_MAXIT) solve_status = e;
+        else if (e != FSD_OK) return e;
     }
     count_launch();
     k_rhs_terms<<<(N + 127) / 128, 128, 0, st>>>(rhs, a->d_force, N, a->shear_rate, h->p.sqm_B2, a->d_b2_mask,
@@ -304,7 +306,8 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
     e = saddle_solve(h, pos, rhs, w.sol, h->p.solver_tol, &it, &res);
     h->info.gmres_iters[2] = it;
     h->info.gmres_resid[2] = res;
-    if (e != FSD_OK) return e;
+    if (e == FSD_ERR_GMRES_MAXIT) solve_status = e;
+    else if (e != FSD_OK) return e;
     count_launch();
     k_add<<<vb(6 * N), 256, 0, st>>>(vel, w.sol + 11 * N, 6 * (size_t)N);
     if (h->p.period > 0 && ((int)(a->timestep + 1) % h->p.period) == 0) {
@@ -314,8 +317,13 @@ int compute_velocity(fsd_handle* h, const fsd_step_args* a) {
         lub_rse(h, pos, a->shear_rate, (const float3*)a->d_ori, a->d_b2_mask, h->p.sqm_B2, vel + 6 * N);
     }
     FSD_CHECK_CUDA(cudaGetLastError());
-    return lanczos_status;
+    return solve_status != FSD_OK ? solve_status : lanczos_status;
 }
+
+// Outcomes after which a step still moves the particles: the solver and
+// Lanczos limits, reported to the caller (the reference prints a warning and
+// continues, Solvers.cu:121-125, Brownian_FarField.cu:787-794).
+static bool step_continues(int e) { return e == FSD_OK || e == FSD_ERR_LANCZOS_MAXIT || e == FSD_ERR_GMRES_MAXIT; }
 
 // Euler + shear from the velocity in a->d_velocity (Integrator.cu:126-228).
 int integrate_euler(fsd_handle* h, const fsd_step_args* a) {
@@ -344,7 +352,7 @@ static int step_rk2(fsd_handle* h, const fsd_step_args* a) {
     const int N = h->p.N;
     cudaStream_t st = h->stream;
     int e = compute_velocity(h, a);
-    if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+    if (!step_continues(e)) return e;
     int status = e;
     const float3* noise = (const float3*)a->d_noise_ang;
     if (!noise && h->p.rot_diff > 0.f) {
@@ -367,8 +375,8 @@ static int step_rk2(fsd_handle* h, const fsd_step_args* a) {
     a2.d_pos_gb = nullptr;
     a2.d_velocity = w.rk_vel;
     e = compute_velocity(h, &a2);
-    if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
-    if (e != FSD_OK) status = e;
+    if (!step_continues(e)) return e;
+    if (e == FSD_ERR_GMRES_MAXIT || status == FSD_OK) status = e;
     ProfRegion pr(h, R_INTEGRATE);
     count_launch();
     k_rk_stage2<<<(N + 127) / 128, 128, 0, st>>>((float4*)a->d_pos, (float3*)a->d_ori, w.rk_pos,
@@ -385,10 +393,10 @@ int step(fsd_handle* h, const fsd_step_args* a) {
     int e;
     if (h->p.integrator == 1) {
         e = step_rk2(h, a);
-        if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+        if (!step_continues(e)) return e;
     } else {
         e = compute_velocity(h, a);
-        if (e != FSD_OK && e != FSD_ERR_LANCZOS_MAXIT) return e;
+        if (!step_continues(e)) return e;
         const int ee = integrate_euler(h, a);
         if (ee != FSD_OK) return ee;
     }

@@ -364,7 +364,12 @@ int fsd_integrate_euler(fsd_handle* h, const fsd_step_args* a);
 /* Velocities and stresslets for the current configuration without moving
  * particles (Integrator_ComputeVelocity, Integrator.cu:744). */
 int fsd_compute_velocity(fsd_handle* h, const fsd_step_args* a);
-/* One full time step (Stokes_StepOne, Stokes.cu:119). */
+/* One full time step (Stokes_StepOne, Stokes.cu:119).  FSD_ERR_GMRES_MAXIT
+ * and FSD_ERR_LANCZOS_MAXIT from fsd_step and fsd_compute_velocity mean the
+ * step completed with the best solution or sample reached (fsd_solve_info
+ * has the residuals), as the reference prints a warning and continues
+ * (Solvers.cu:121-125, Brownian_FarField.cu:787-794); other errors stop the
+ * step before the particles move. */
 int fsd_step(fsd_handle* h, const fsd_step_args* a);
 /* One step of each of n independent suspensions (no counterpart in the
  * reference, which steps one system per process).  Handle i takes args[i];

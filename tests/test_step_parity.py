@@ -162,7 +162,7 @@ def test_full_brownian_step_matches_oracle(cuda, active):
     st = s.step(0, rate, p, o, img, F, V, pos_gb=gb, b1_mask=None if b1m is None else dev(b1m),
                 b2_mask=None if b2m is None else dev(b2m), raise_on_error=False)
     info = s.solve_info()
-    assert st in (0, 3) and max(info["gmres_resid"][:2]) < 1e-5 and info["gmres_resid"][2] <= 3e-6
+    assert st in (0, 3) and max(info["gmres_resid"]) < 1e-5
     v = V.cpu().numpy().astype(np.float64)
     # oracle: right-hand side, solve, stresslet, Euler
     pr = O.Problem(pos, L, xy, table=ewald_golden())
