@@ -157,17 +157,21 @@ SINGLE_KERNEL_REGIONS = {"fft": 1, "spread": 1, "contract": 1, "green": 1, "real
 WEIGHTS = ROOT / "fsd_b200" / "data" / "learned_precond.f32"
 
 
-def precond_form(args, net, form=None):
+def precond_form(args, net, form=None, interval=0.05):
     if args.precond == "ichol":
         return "RCM + block IC(0) of the pruned lubrication block (the reference's preconditioner)"
     if args.precond == "none":
         return "identity"
     form = form or ("poly" if args.poly >= 2 else "gmres")
     if form == "poly":
-        src = ("coefficients predicted by the trained message-passing network (checked on a probe at every build)"
-               if net else "coefficients fitted to four probe vectors at every build (no network)")
-        return (f"two-hop sparse approximate inverse G, inner Chebyshev polynomial y = G q(AG) t of "
-                f"{args.poly} terms, {src}; plain outer GMRES")
+        if net:
+            src = "Chebyshev interval [rho lambda, lambda] with rho predicted by the trained message-passing network"
+        elif interval > 0:
+            src = f"fixed Chebyshev interval [{interval} lambda, lambda] (no network)"
+        else:
+            src = "coefficients fitted to four probe vectors at every build (no network)"
+        return (f"two-hop sparse approximate inverse G, inner polynomial y = G q(AG) t of degree {args.poly - 1}, "
+                f"{src}; plain outer GMRES")
     return (f"two-hop sparse approximate inverse + {args.inner} inner GMRES steps, flexible outer GMRES"
             + (", trained network correction" if net else ", no network"))
 
@@ -176,10 +180,11 @@ def poly_weights(k):
     return ROOT / "fsd_b200" / "data" / f"learned_poly_k{k}.f32"
 
 
-def make_solver(args, precond, N, L, dev, seed, form=None):
-    """form (learned only): "poly" = the network's inner polynomial (a fitted
-    polynomial when no weights ship or with net=False), "gmres" = inner GMRES
-    steps on the approximate inverse; default from --poly."""
+def make_solver(args, precond, N, L, dev, seed, form=None, interval=0.05):
+    """form (learned only): "poly" = the inner Chebyshev polynomial, its
+    interval predicted by the network when weights ship (else the fixed
+    interval ratio `interval`, or a least-squares fit to probes for 0);
+    "gmres" = inner GMRES steps on the approximate inverse; default from --poly."""
     from fsd_b200.core import FSD
 
     form = form or ("poly" if args.poly >= 2 else "gmres")
@@ -188,7 +193,7 @@ def make_solver(args, precond, N, L, dev, seed, form=None):
             lanczos_tol=1e-3, rfd_epsilon=1e-3, precond=precond, period=0, gmres_max_iter=3000,
             gmres_restart=200 if precond == "ichol" else 100,
             learned_inner=args.inner if (precond == "learned" and not poly) else 0,
-            learned_poly=args.poly if poly else 0, autotune=0 if args.no_autotune else 1)
+            learned_poly=args.poly if poly else 0, poly_interval=interval, autotune=0 if args.no_autotune else 1)
     net = False
     wf = poly_weights(args.poly) if poly else WEIGHTS
     if precond == "learned" and wf.exists() and not args.no_net:
@@ -372,18 +377,19 @@ def run_fsd(args, ws, rank, local):
     # the polynomial fitted to probe vectors at every build
     no_network = {}
     if args.precond == "learned" and not args.no_compare:
-        forms = {"spai_inner_gmres": "gmres"}
+        forms = {"spai_inner_gmres": ("gmres", 0.05)}
         if args.poly >= 2:
-            forms["fitted_polynomial"] = "poly"
-        for name, form in forms.items():
+            forms["fixed_interval_polynomial"] = ("poly", 0.05)
+            forms["fitted_polynomial"] = ("poly", 0.0)
+        for name, (form, interval) in forms.items():
             a2 = argparse.Namespace(**vars(args))
             a2.no_net = True
-            sc, _ = make_solver(a2, "learned", N, L, dev, 1 + rank, form=form)
+            sc, _ = make_solver(a2, "learned", N, L, dev, 1 + rank, form=form, interval=interval)
             r = timed_steps(a2, sc, fresh_state(), args.steps, args.warmup, dev, ws)
             sc.close()
             no_network[name] = {"value": ws * args.steps / (r["total_ms"] / 1e3), "unit": "steps/s",
                                 "ms_per_step": r["total_ms"] / args.steps, "iterations_per_step": r["iters"],
-                                "precond_form": precond_form(a2, False, form)}
+                                "precond_form": precond_form(a2, False, form, interval)}
     # --- roofline of the dominant single-kernel region (profiled pass)
     regions = prof["regions"]
     prof_steps = prof["steps"]
@@ -612,7 +618,10 @@ def run_config5(args, local):
     forms = {
         "ichol": dict(precond="ichol", gmres_restart=200, learned_inner=0),
         "spai_gmres6": dict(precond="learned", gmres_restart=100, learned_inner=6),
-        "fitted_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10),
+        "fitted_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10,
+                              poly_interval=0.0),
+        "fixed_interval_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10,
+                                      poly_interval=0.05),
         "learned_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10),
     }
     w = np.fromfile(poly_weights(10), "<f4") if poly_weights(10).exists() else None
@@ -652,8 +661,7 @@ def run_config5(args, local):
             res[name] = {"outer_iterations": iters[-1], "residuals": resid[-1], "ms": times[-1],
                          "converged": si["status"] != 3}
             if "poly" in name:
-                res[name].update(poly_source=si["poly_source"], poly_loss_net=si["poly_loss_net"],
-                                 poly_loss_fit=si["poly_loss_fit"])
+                res[name].update(poly_source=si["poly_source"], poly_ratio=si["poly_ratio"])
         results[str(phi)] = res
     return {"metric": "config 5: learned preconditioner on held-out dense suspensions, one velocity computation "
                       "(three saddle solves to 1e-4)", "unit": "ms", "N": N, "higher_is_better": False,

@@ -39,7 +39,7 @@ class fsd_params(C.Structure):
         ("precond", C.c_int), ("force_mode", C.c_int), ("kgrid_pi_ref", C.c_int),
         ("rlub", C.c_float), ("rp", C.c_float), ("nlist_buffer", C.c_float),
         ("ichol_local_shift", C.c_int), ("ichol_gain_limit", C.c_float),
-        ("learned_inner", C.c_int), ("learned_poly", C.c_int), ("autotune", C.c_int),
+        ("learned_inner", C.c_int), ("learned_poly", C.c_int), ("poly_interval", C.c_float), ("autotune", C.c_int),
         ("friction_type", C.c_int), ("friction_h0", C.c_float), ("friction_alpha", C.c_float * 6),
         ("integrator", C.c_int),
     ]
@@ -64,6 +64,7 @@ class fsd_solve_info(C.Structure):
         ("nlist_max", C.c_int), ("status", C.c_int), ("ichol_shifted", C.c_int),
         ("ichol_gain", C.c_float),
         ("poly_source", C.c_int), ("poly_loss_net", C.c_float), ("poly_loss_fit", C.c_float),
+        ("poly_ratio", C.c_float),
     ]
 
 
@@ -116,6 +117,10 @@ _SIGS = {
     "fsd_learned_train_step": (C.c_int, [H, P, P, C.c_int, C.c_uint, C.c_float, C.POINTER(C.c_float), P]),
     "fsd_learned_set_poly": (C.c_int, [H, P, C.c_int]),
     "fsd_learned_get_poly": (C.c_int, [H, P, C.c_int]),
+    "fsd_learned_set_interval": (C.c_int, [H, C.c_float]),
+    "fsd_learned_interval_coefficients": (C.c_int, [C.c_float, C.c_float, C.c_int, P]),
+    "fsd_learned_ratio_train_step": (C.c_int, [H, P, C.c_float, C.c_float, C.POINTER(C.c_float),
+                                               C.POINTER(C.c_float)]),
     "fsd_learned_poly_train_step": (C.c_int, [H, P, C.c_int, C.c_uint, C.c_float, C.c_int, C.POINTER(C.c_float),
                                               C.POINTER(C.c_float), P, P, P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),

@@ -1,0 +1,241 @@
+// Block-sparse (6x6 fp32 blocks, block CSR) products of the learned
+// preconditioner's inner polynomial, with the matrix streamed into shared
+// memory by the Tensor Memory Accelerator.
+//
+// The approximate inverse G (54 MB at N = 32768, phi = 0.4) and the pruned
+// lubrication matrix A are read once per product.  One CTA takes a tile of
+// consecutive rows whose blocks (at most kTileBlocks) lie contiguously in
+// memory; one thread issues a bulk copy (cp.async.bulk, completing on an
+// mbarrier) of the tile's blocks and column indices into shared memory, so
+// the matrix streams at copy-engine rate while the eight-lane row groups
+// gather the vector operand from L2.  Three CTAs fit on an SM, so one CTA's
+// copy overlaps the others' arithmetic.  Tiles are cut on the host once per
+// preconditioner build.
+//
+// The mbarrier wait is bounded: when it runs out the CTA records an error
+// (read by the host after the solve), waits once more (also bounded) for its
+// own copy and returns without writing.
+#include <algorithm>
+#include <vector>
+
+#include "fsd_device.cuh"
+#include "fsd_learned.h"
+#include "fsd_solver.h"
+
+namespace fsd {
+
+namespace {
+
+constexpr long long kBsrSpinLimit = 1ll << 22;
+__device__ int g_bsr_error = 0;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t phase) {
+    for (long long n = 0; n < kBsrSpinLimit; ++n) {
+        if (bar_try_wait(bar, phase)) return true;
+        if (n > 32) __nanosleep(32);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ float row6(const float* blk, int rr, float xj, unsigned gmask) {
+    const float2* g = reinterpret_cast<const float2*>(blk + rr * 6);
+    const float2 g01 = g[0], g23 = g[1], g45 = g[2];
+    float s = g01.x * __shfl_sync(gmask, xj, 0, 8);
+    s = fmaf(g01.y, __shfl_sync(gmask, xj, 1, 8), s);
+    s = fmaf(g23.x, __shfl_sync(gmask, xj, 2, 8), s);
+    s = fmaf(g23.y, __shfl_sync(gmask, xj, 3, 8), s);
+    s = fmaf(g45.x, __shfl_sync(gmask, xj, 4, 8), s);
+    s = fmaf(g45.y, __shfl_sync(gmask, xj, 5, 8), s);
+    return s;
+}
+
+}  // namespace
+
+// Modes: 0 = first product of the Clenshaw recurrence (operand t = b[0:6N] -
+// b[11N:17N], writes T = t, B = c_{k-1} t, out = c_{k-1} G t); 1 = plain
+// product out = M x; 2 = last product y = G v with the saddle post step into
+// xs; 3 = Clenshaw step out = c_m T + f ((2/lambda) A u - B1) - B2.
+template <int MODE>
+__global__ void __launch_bounds__(256, 3) k_bsr_tma(BsrTmaArgs a) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ __align__(8) uint64_t bar;
+    float* sG = reinterpret_cast<float*>(sm);
+    int* sC = reinterpret_cast<int*>(sm + (size_t)kTileBlocks * 144);
+    const int t = blockIdx.x;
+    if (t >= *a.ntiles) return;  // the launch covers the tile capacity
+    const int r0 = a.tile_row[t], r1 = a.tile_row[t + 1];
+    const int e0 = a.rowptr[r0], e1 = a.rowptr[r1];
+    const int ce0 = e0 & ~3, ce1 = (e1 + 3) & ~3;  // 16-byte aligned copy of the column indices
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t gbytes = (uint32_t)(e1 - e0) * 144u, cbytes = (uint32_t)(ce1 - ce0) * 4u;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                     "r"(gbytes + cbytes)
+                     : "memory");
+        if (gbytes) bulk_load(sG, a.val + (size_t)e0 * 36, gbytes, &bar);
+        if (cbytes) bulk_load(sC, a.col + ce0, cbytes, &bar);
+    }
+    if (!bar_wait(&bar, 0)) {
+        if (threadIdx.x == 0) atomicExch(&g_bsr_error, 1);
+        bar_wait(&bar, 0);  // the copy may still land in this CTA's shared memory
+        return;
+    }
+    const int lane8 = threadIdx.x & 7;
+    const int group = threadIdx.x >> 3;
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const int rr = lane8 < 6 ? lane8 : 0;
+    const int N = a.N;
+    const size_t offU = 11 * (size_t)N;
+    auto ld = [&](int j) -> float {
+        if (lane8 >= 6) return 0.f;
+        if (MODE == 0) return a.x[6 * (size_t)j + lane8] - a.x[offU + 6 * (size_t)j + lane8];
+        return a.x[6 * (size_t)j + lane8];
+    };
+    // whole groups of eight take rows; a group's lanes stay together
+    for (int r = r0 + group; r < r1; r += (int)(blockDim.x >> 3)) {
+        const int qb = a.rowptr[r] - e0, qe = a.rowptr[r + 1] - e0;
+        const int* cc = sC + (e0 - ce0);
+        float acc = 0.f;
+        int q = qb;
+        for (; q + 3 < qe; q += 4) {
+            const int j0 = cc[q], j1 = cc[q + 1], j2 = cc[q + 2], j3 = cc[q + 3];
+            const float x0 = ld(j0), x1 = ld(j1), x2 = ld(j2), x3 = ld(j3);
+            const float* gq = sG + (size_t)q * 36;
+            acc += row6(gq, rr, x0, gmask);
+            acc += row6(gq + 36, rr, x1, gmask);
+            acc += row6(gq + 72, rr, x2, gmask);
+            acc += row6(gq + 108, rr, x3, gmask);
+        }
+        for (; q < qe; ++q) acc += row6(sG + (size_t)q * 36, rr, ld(cc[q]), gmask);
+        const size_t i6 = 6 * (size_t)r + lane8;
+        if (MODE == 0) {
+            if (lane8 < 6) {
+                const float c = a.pc[a.k - 1];
+                const float tv = a.x[i6] - a.x[offU + i6];
+                a.T[i6] = tv;
+                a.B[i6] = c * tv;
+                a.out[i6] = c * acc;
+            }
+        } else if (MODE == 1) {
+            if (lane8 < 6) a.out[i6] = acc;
+        } else if (MODE == 2) {
+            if (lane8 < 6) {
+                const float bq = a.b[i6];
+                a.xs[i6] = bq - acc;
+                a.xs[offU + i6] = acc;
+            }
+            if (lane8 < 5) {
+                const size_t q5 = 6 * (size_t)N + 5 * (size_t)r + lane8;
+                a.xs[q5] = a.b[q5];
+            }
+        } else {
+            if (lane8 < 6) {
+                const float s2 = 2.0f / a.pc[kMaxPoly];
+                const float f = a.m >= 1 ? 2.0f : 1.0f;
+                float v = fmaf(a.pc[a.m], a.T[i6], f * fmaf(s2, acc, -a.B1[i6]));
+                if (a.B2) v -= a.B2[i6];
+                a.out[i6] = v;
+            }
+        }
+    }
+}
+
+size_t bsr_tma_smem() { return (size_t)kTileBlocks * 144 + (size_t)(kTileBlocks + 8) * 4; }
+
+// Kernel entry of a mode (for launches and graph-node updates).
+const void* bsr_tma_kernel(int mode) {
+    switch (mode) {
+        case 0: return (const void*)k_bsr_tma<0>;
+        case 1: return (const void*)k_bsr_tma<1>;
+        case 2: return (const void*)k_bsr_tma<2>;
+        default: return (const void*)k_bsr_tma<3>;
+    }
+}
+
+int bsr_tma_prepare() {
+    for (int m = 0; m < 4; ++m) FSD_CHECK_CUDA(ensure_smem_limit(bsr_tma_kernel(m), bsr_tma_smem()));
+    return FSD_OK;
+}
+
+void bsr_tma_launch(int mode, const BsrTmaArgs& a, int grid, cudaStream_t st) {
+    const size_t smem = bsr_tma_smem();
+    switch (mode) {
+        case 0: k_bsr_tma<0><<<grid, 256, smem, st>>>(a); break;
+        case 1: k_bsr_tma<1><<<grid, 256, smem, st>>>(a); break;
+        case 2: k_bsr_tma<2><<<grid, 256, smem, st>>>(a); break;
+        default: k_bsr_tma<3><<<grid, 256, smem, st>>>(a); break;
+    }
+}
+
+// Pruned A (padded rows of kPrunedCap blocks) copied into block CSR.
+__global__ void k_compact_pruned(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist,
+                                 const float* __restrict__ A, const int* __restrict__ rowptr, int N, int* col,
+                                 float* val) {
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= N) return;
+    const unsigned n = pn[i];
+    const int base = rowptr[i];
+    for (unsigned q = 0; q < n; ++q) {
+        if (lane == 0) col[base + q] = (int)plist[(size_t)i * kPrunedCap + q];
+        const float* src = A + ((size_t)i * kPrunedCap + q) * 36;
+        float* dst = val + (size_t)(base + q) * 36;
+        for (int k = lane; k < 36; k += 32) dst[k] = src[k];
+    }
+}
+
+int bsr_tma_error() {
+    int e = 0;
+    cudaMemcpyFromSymbol(&e, g_bsr_error, sizeof(int));
+    if (e) {
+        const int z = 0;
+        cudaMemcpyToSymbol(g_bsr_error, &z, sizeof(int));
+    }
+    return e;
+}
+
+// Tiles of consecutive rows with at most kTileBlocks blocks (and rows) each,
+// from a host copy of the row pointer.  Rows longer than a tile cannot occur:
+// G rows hold at most kSpaiCap blocks and A rows at most kPrunedCap.
+int bsr_make_tiles(const std::vector<int>& rowptr, int N, std::vector<int>& tiles) {
+    tiles.clear();
+    tiles.push_back(0);
+    int start = 0;
+    for (int r = 0; r < N; ++r) {
+        if (rowptr[r + 1] - rowptr[start] > kTileBlocks || r - start >= kTileBlocks) {
+            tiles.push_back(r);
+            start = r;
+        }
+        if (rowptr[r + 1] - rowptr[r] > kTileBlocks) return FSD_ERR_BAD_PARAMS;
+    }
+    tiles.push_back(N);
+    return FSD_OK;
+}
+
+}  // namespace fsd

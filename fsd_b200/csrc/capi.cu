@@ -190,6 +190,7 @@ void fsd_default_params(fsd_params* p) {
     p->ichol_gain_limit = 100.0f;
     p->learned_inner = 4;
     p->learned_poly = 0;
+    p->poly_interval = 0.05f;
     p->friction_type = 0;
     p->friction_h0 = 0.0f;
     for (int k = 0; k < 6; ++k) p->friction_alpha[k] = 0.0f;
@@ -298,6 +299,7 @@ int fsd_create(const fsd_params* p, void* stream, fsd_handle** out) {
     if (p->gmres_restart < 1 || p->gmres_restart > kMaxRestart || p->lanczos_max < 4) return FSD_ERR_BAD_PARAMS;
     if (p->learned_inner < 0 || p->learned_inner > kMaxInner) return FSD_ERR_BAD_PARAMS;
     if (p->learned_poly < 0 || p->learned_poly == 1 || p->learned_poly > kMaxPoly) return FSD_ERR_BAD_PARAMS;
+    if (!(p->poly_interval >= 0.f && p->poly_interval < 1.f)) return FSD_ERR_BAD_PARAMS;
     if (p->friction_type < 0 || p->friction_type > 1 || (p->friction_type == 1 && !(p->friction_h0 > 0.f)))
         return FSD_ERR_BAD_PARAMS;
     if (p->integrator < 0 || p->integrator > 1) return FSD_ERR_BAD_PARAMS;
@@ -405,6 +407,7 @@ int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info) {
     info->poly_source = ls ? ls->poly_source : 0;
     info->poly_loss_net = ls ? ls->poly_loss_net : -1.f;
     info->poly_loss_fit = ls ? ls->poly_loss_fit : -1.f;
+    info->poly_ratio = ls ? ls->poly_ratio : -1.f;
     return FSD_OK;
 }
 
@@ -533,6 +536,26 @@ int fsd_learned_tensor_cores(fsd_handle* h, int on) {
 int fsd_learned_set_poly(fsd_handle* h, const float* host_c, int k) {
     if (!h) return FSD_ERR_BAD_PARAMS;
     return poly_set_coefficients(h, host_c, k);
+}
+
+int fsd_learned_set_interval(fsd_handle* h, float rho) {
+    if (!h || !(rho >= 0.f && rho < 1.f)) return FSD_ERR_BAD_PARAMS;
+    LearnedState* s = learned(h);
+    s->user_ratio = rho > 0.f ? rho : -1.f;
+    if (rho > 0.f) s->poly_user = false;
+    return FSD_OK;
+}
+
+int fsd_learned_interval_coefficients(float rho, float lambda, int k, float* host_c) {
+    if (!host_c || k < 2 || k > kMaxPoly || !(rho > 0.f && rho < 1.f) || !(lambda > 0.f)) return FSD_ERR_BAD_PARAMS;
+    poly_interval_coefficients(rho, lambda, k, host_c);
+    return FSD_OK;
+}
+
+int fsd_learned_ratio_train_step(fsd_handle* h, const float* d_pos, float target_log_ratio, float lr, float* loss,
+                                 float* predicted_log_ratio) {
+    if (!h || !d_pos || !h->nlist_valid || h->p.learned_poly < 2) return FSD_ERR_BAD_PARAMS;
+    return mpnn_ratio_train_step(h, (const float4*)d_pos, target_log_ratio, lr, loss, predicted_log_ratio);
 }
 
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n) {

@@ -50,7 +50,7 @@ int learned_reserve(fsd_handle* h, int nnzb) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
     if (!s->g_rowptr) FSD_CHECK_CUDA(cudaMalloc(&s->g_rowptr, sizeof(int) * (N + 1)));
-    if (nnzb > s->g_cap) {
+    if (nnzb + 8 > s->g_cap) {  // headroom: the streamed products read column indices up to three past the end
         if (s->g_col) cudaFree(s->g_col);
         if (s->g_val) cudaFree(s->g_val);
         s->g_col = nullptr;
@@ -538,18 +538,33 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
         }
     }
     if (poly) {
+        e = poly_prepare_products(h);
+        if (e != FSD_OK) return e;
         e = poly_lambda(h);
         if (e != FSD_OK) return e;
+        // Coefficients: the caller's; else the Chebyshev interval whose lower
+        // end the network predicts for this configuration; else a fixed
+        // interval ratio (poly_interval > 0); else a least-squares fit on
+        // probe vectors.
+        s->poly_ratio = -1.f;
         if (s->poly_user) {
             s->poly_source = 3;
+        } else if (s->user_ratio > 0.f) {
+            e = poly_set_interval(h, s->user_ratio);
+            if (e != FSD_OK) return e;
+            s->poly_source = 4;
+        } else if (mpnn_loaded(h)) {
+            double rho = 0.0;
+            e = mpnn_poly_ratio(h, pos, &rho, nullptr);
+            if (e != FSD_OK) return e;
+            e = poly_set_interval(h, rho);
+            if (e != FSD_OK) return e;
+            s->poly_source = 1;
+        } else if (h->p.poly_interval > 0.f) {
+            e = poly_set_interval(h, h->p.poly_interval);
+            if (e != FSD_OK) return e;
+            s->poly_source = 4;
         } else {
-            // the network's coefficients for this configuration, checked
-            // against a least-squares fit on held-out probes (or the fit alone
-            // without a network)
-            if (mpnn_loaded(h)) {
-                e = mpnn_poly_coeffs(h, pos, s->pc, h->p.learned_poly);
-                if (e != FSD_OK) return e;
-            }
             e = mpnn_poly_calibrate(h, h->p.learned_poly, ++s->poly_builds);
             if (e != FSD_OK) return e;
         }
@@ -563,6 +578,7 @@ int learned_set_weights(fsd_handle* h, const float* host_w, int n) {
     if (e == FSD_OK) {
         learned(h)->g_user = false;
         learned(h)->poly_user = false;  // the network's coefficients from now on
+        learned(h)->user_ratio = -1.f;
     }
     return e;
 }

@@ -1048,177 +1048,6 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     }
 }
 
-// Spreading with separable Gaussian weights (tile-relative separations
-// only).  The box tilt couples x to y alone, so over a particle's stencil
-// (sx, sy, sz) the weight factors as
-//   prefac exp(-a r_x(sx, sy)^2) exp(-a r_y(sy)^2) * exp(-a r_z(sz)^2),
-//   r_x = r_x0 + hx sx + xy hy sy,  r_y = r_y0 + hy sy,  r_z = r_z0 + hz sz:
-// each staged particle carries its P x P (x, y) factors and its P z factors
-// (P^2 + 2P exponentials instead of P^3), and a contribution is one product
-// of two staged factors followed by packed FP32 FMAs (fma.rn.f32x2, two
-// field components per instruction, rounding as two scalar FMAs).  The
-// gather order is that of k_spread, so every node adds its contributors in
-// the same order; the result differs from k_spread's only by the rounding of
-// the factored exponential.
-constexpr int kSepCap = 256;  // staged particles per pass
-
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-    unsigned long long ra = *reinterpret_cast<unsigned long long*>(&a);
-    unsigned long long rb = *reinterpret_cast<unsigned long long*>(&b);
-    unsigned long long rc = *reinterpret_cast<unsigned long long*>(&c);
-    unsigned long long rd;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(rc));
-    return *reinterpret_cast<float2*>(&rd);
-}
-
-// Staged record, `stride` floats (a multiple of 4): v[0:12] (six field pairs
-// in grid order), origin (packed cells) and pad [12:16], z factors [16:16+P],
-// (x, y) factors [24:24+P^2] indexed sx * P + sy.
-__global__ void __launch_bounds__(256, 3) k_spread_sep(SpreadArgs a, int stride) {
-    __shared__ unsigned scan_sh[32];
-    __shared__ unsigned s_total;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int P = a.P;
-    const int ntx = (a.Nx + a.TX - 1) / a.TX, nty = (a.Ny + a.TY - 1) / a.TY;
-    int bid = blockIdx.x;
-    const int tx = bid % ntx;
-    bid /= ntx;
-    const int ty = bid % nty;
-    const int tz = bid / nty;
-    const int x0 = tx * a.TX, y0 = ty * a.TY, z0 = tz * a.TZ;
-    float3 pg0;  // position of the tile's origin node
-    pg0.x = a.hx * x0 - a.box.Lx / 2.0f;
-    pg0.y = a.hy * y0 - a.box.Ly / 2.0f;
-    pg0.z = a.hz * z0 - a.box.Lz / 2.0f;
-    pg0.x = pg0.x + a.box.xy * pg0.y;
-    const int EX = a.TX + P - 1, EY = a.TY + P - 1, EZ = a.TZ + P - 1;
-    const int ex0 = x0 - (P - 1), ey0 = y0 - (P - 1), ez0 = z0 - (P - 1);
-    const int ncell = EX * EY * EZ;
-    float* sp = reinterpret_cast<float*>(smem_raw);                       // kSepCap x stride floats
-    unsigned* cell_off = reinterpret_cast<unsigned*>(sp + (size_t)kSepCap * stride);  // ncell + 1
-    const int nth = blockDim.x;
-    const int cpt = (ncell + nth - 1) / nth;
-    unsigned mycount = 0;
-    const int c_begin = threadIdx.x * cpt, c_end = min(ncell, (threadIdx.x + 1) * cpt);
-    for (int c = c_begin; c < c_end; ++c) {
-        const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
-        const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
-        const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
-        cell_off[c] = mycount;
-        mycount += a.bin_start[bin + 1] - a.bin_start[bin];
-    }
-    unsigned x = mycount;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) scan_sh[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        unsigned sv = (lane < (nth >> 5)) ? scan_sh[lane] : 0u;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, sv, o);
-            if (lane >= o) sv += y;
-        }
-        scan_sh[lane] = sv;
-        if (lane == 31) s_total = sv;
-    }
-    __syncthreads();
-    const unsigned myoff = (wid ? scan_sh[wid - 1] : 0u) + x - mycount;
-    const unsigned total = s_total;
-    for (int c = c_begin; c < c_end; ++c) cell_off[c] += myoff;
-    if (threadIdx.x == 0) cell_off[ncell] = total;
-
-    const int lz = threadIdx.x % a.TZ, ly = (threadIdx.x / a.TZ) % a.TY, lx = threadIdx.x / (a.TZ * a.TY);
-    const int nx = x0 + lx, ny = y0 + ly, nz = z0 + lz;
-    const bool active = (lx < a.TX) && nx < a.Nx && ny < a.Ny && nz < a.Nz;
-    const float xyhy = a.box.xy * a.hy;
-    float2 acc[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) acc[c] = make_float2(0.f, 0.f);
-
-    for (unsigned chunk = 0; chunk < total; chunk += kSepCap) {
-        unsigned k = myoff;
-        for (int c = c_begin; c < c_end; ++c) {
-            const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
-            const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
-            const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
-            const unsigned q0 = a.bin_start[bin], q1 = a.bin_start[bin + 1];
-            if (k + (q1 - q0) <= chunk || k >= chunk + kSepCap) {  // this cell's particles lie outside the chunk
-                k += q1 - q0;
-                continue;
-            }
-            for (unsigned q = q0; q < q1; ++q, ++k) {
-                if (k < chunk || k >= chunk + kSepCap) continue;
-                const unsigned pidx = a.bin_parts[q];
-                float* rec = sp + (size_t)(k - chunk) * stride;
-                const float4 ps = a.pos[pidx];
-                const float3 d = min_image(make_float3(pg0.x - ps.x, pg0.y - ps.y, pg0.z - ps.z), a.box);
-                const float4 f = a.f4[pidx], c0 = a.c4[2 * pidx], c1 = a.c4[2 * pidx + 1];
-                float4* r4 = reinterpret_cast<float4*>(rec);
-                r4[0] = make_float4(f.x, f.y, c0.x, c0.y);
-                r4[1] = make_float4(c0.z, c1.y, c1.x, c0.w);
-                r4[2] = make_float4(c1.z, c1.w, f.z, 0.0f);
-                reinterpret_cast<int*>(rec)[12] = cx | (cy << 10) | (cz << 20);
-                const float rx0 = d.x + a.hx * (float)(cx - (P - 1)) + xyhy * (float)(cy - (P - 1));
-                const float ry0 = d.y + a.hy * (float)(cy - (P - 1));
-                const float rz0 = d.z + a.hz * (float)(cz - (P - 1));
-#pragma unroll 1
-                for (int sz = 0; sz < P; ++sz) {
-                    const float rz = rz0 + a.hz * (float)sz;
-                    rec[16 + sz] = expf(-a.expfac * rz * rz);
-                }
-#pragma unroll 1
-                for (int sy = 0; sy < P; ++sy) {
-                    const float ry = ry0 + a.hy * (float)sy;
-                    const float ey = a.prefac * expf(-a.expfac * ry * ry);
-#pragma unroll 1
-                    for (int sx = 0; sx < P; ++sx) {
-                        const float rx = rx0 + a.hx * (float)sx + xyhy * (float)sy;
-                        rec[24 + sx * P + sy] = ey * expf(-a.expfac * rx * rx);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        const unsigned cend = chunk + min((unsigned)kSepCap, total - chunk);
-        if (active) {
-            for (int ix = 0; ix < P; ++ix) {
-                const int sx = P - 1 - ix;
-                for (int iy = 0; iy < P; ++iy) {
-                    const int sxy = 24 + sx * P + (P - 1 - iy);
-                    const int c0 = ((lx + ix) * EY + (ly + iy)) * EZ + lz;
-                    const unsigned q0 = max(cell_off[c0], chunk), q1 = min(cell_off[c0 + P], cend);
-                    for (unsigned q = q0; q < q1; ++q) {
-                        const float* rec = sp + (size_t)(q - chunk) * stride;
-                        const int cz = reinterpret_cast<const int*>(rec)[12] >> 20;
-                        const float w = rec[sxy] * rec[16 + (P - 1) - (cz - lz)];
-                        const float4* r4 = reinterpret_cast<const float4*>(rec);
-                        const float4 v0 = r4[0], v1 = r4[1], v2 = r4[2];
-                        const float2 w2 = make_float2(w, w);
-                        acc[0] = ffma2(w2, make_float2(v0.x, v0.y), acc[0]);
-                        acc[1] = ffma2(w2, make_float2(v0.z, v0.w), acc[1]);
-                        acc[2] = ffma2(w2, make_float2(v1.x, v1.y), acc[2]);
-                        acc[3] = ffma2(w2, make_float2(v1.z, v1.w), acc[3]);
-                        acc[4] = ffma2(w2, make_float2(v2.x, v2.y), acc[4]);
-                        acc[5] = ffma2(w2, make_float2(v2.z, v2.w), acc[5]);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (active) {
-        const size_t G = (size_t)a.Nx * a.Ny * a.Nz;
-        const size_t g = ((size_t)nx * a.Ny + ny) * a.Nz + nz;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) a.grid[(size_t)c * G + g] = acc[c];
-    }
-}
-
 // ------------------------------------------------------------- contraction
 // One warp per particle: interpolate velocity (3) and velocity gradient (8)
 // from the P^3 stencil (Mobility_WaveSpace_ContractU / ContractD,
@@ -1479,14 +1308,6 @@ static void spread(fsd_handle* h, const float4* pos) {
               (a.TZ + g.P) * tilt < 0.5f * g.Nz;
     const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
     const size_t cell_bytes = sizeof(unsigned) * ((size_t)(a.TX + g.P - 1) * (a.TY + g.P - 1) * (a.TZ + g.P - 1) + 1);
-    if (a.local && g.P <= 8) {
-        const int stride = 24 + ((g.P * g.P + 3) & ~3);
-        const size_t smem = sizeof(float) * (size_t)kSepCap * stride + cell_bytes;
-        if (!smem_limit_ok((const void*)k_spread_sep, smem, "k_spread_sep shared memory")) return;
-        count_launch();
-        k_spread_sep<<<ntiles, a.TX * a.TY * a.TZ, smem, h->stream>>>(a, stride);
-        return;
-    }
     count_launch();
     k_spread<<<ntiles, a.TX * a.TY * a.TZ, cell_bytes, h->stream>>>(a);
 }

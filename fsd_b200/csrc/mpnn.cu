@@ -1357,34 +1357,14 @@ static bool poly_fit(const std::vector<PolyGram>& gr, int p0, int p1, int k, std
     return solve_small(Ms, gs, k, c);
 }
 
-// Check of the polynomial at every build.  With a network, its coefficients
-// are scored on one probe vector and kept when the relative residual they
-// leave, ||t - AG q(AG) t||^2 / ||t||^2, is at most kPolyAccept (a residual
-// reduction of about 0.22); otherwise, and without a network, four probe
-// vectors give a least-squares fit of the coefficients, which is used.  The
-// choice and the losses are recorded in the learned state.
-constexpr double kPolyAccept = 0.05;
-
+// Least-squares fit of the coefficients to four probe vectors drawn at this
+// build (the learned_poly form without a network and without a fixed
+// interval); its loss is recorded in the learned state.
 int mpnn_poly_calibrate(fsd_handle* h, int k, uint32_t step) {
     LearnedState* ls = learned(h);
-    const bool net = mpnn_loaded(h);
     ls->poly_loss_net = -1.f;
-    ls->poly_loss_fit = -1.f;
     std::vector<PolyGram> gr;
-    if (net) {
-        float c32[kMaxPoly + 1];
-        FSD_CHECK_CUDA(cudaMemcpyAsync(c32, ls->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, h->stream));
-        MP_TRY(poly_gram(h, 1, 2 * step, k, gr));  // synchronises the stream
-        std::vector<double> cnet(k);
-        for (int m = 0; m < k; ++m) cnet[m] = c32[m];
-        const double lnet = poly_loss(gr, 0, 1, cnet);
-        ls->poly_loss_net = (float)lnet;
-        if (lnet <= kPolyAccept) {
-            ls->poly_source = 1;
-            return FSD_OK;
-        }
-    }
-    MP_TRY(poly_gram(h, 4, 2 * step + 1, k, gr));
+    MP_TRY(poly_gram(h, 4, step, k, gr));
     std::vector<double> cfit;
     if (!poly_fit(gr, 0, 4, k, cfit)) return FSD_ERR_BREAKDOWN;
     ls->poly_loss_fit = (float)poly_loss(gr, 0, 4, cfit);
@@ -1458,6 +1438,62 @@ int mpnn_poly_train_step(fsd_handle* h, const float4* pos, int P, uint32_t step,
         if (host_coef) host_coef[m] = (float)c[m];
         if (host_coef_opt) host_coef_opt[m] = copt.empty() ? 0.f : (float)copt[m];
     }
+    return FSD_OK;
+}
+
+// ------------------------------------------- learned Chebyshev interval
+// The network's use in the default learned_poly mode: it predicts, for a
+// configuration, the lower end a = rho lambda of the Chebyshev interval of
+// the inner polynomial, log rho being the mean over particles of the node
+// head's first output.  It is trained on the interval ratio that gave the
+// fewest outer GMRES iterations in solves of the solver's own configurations
+// (a squared error in log rho, one scalar per configuration).
+constexpr double kRatioMin = 1e-3, kRatioMax = 0.5;
+
+int mpnn_poly_ratio(fsd_handle* h, const float4* pos, double* rho, float* log_rho) {
+    LearnedState* ls = learned(h);
+    MP_TRY(poly_alloc(h));
+    MP_TRY(mpnn_poly_coeffs(h, pos, ls->pc, 1));  // pc[0] = mean of the first node output (synchronised)
+    float s0 = 0.f;
+    FSD_CHECK_CUDA(cudaMemcpyAsync(&s0, ls->pc, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    if (log_rho) *log_rho = s0;
+    *rho = std::min(kRatioMax, std::max(kRatioMin, std::exp((double)s0)));
+    return FSD_OK;
+}
+
+int mpnn_ratio_train_step(fsd_handle* h, const float4* pos, float target_log_rho, float lr, float* loss,
+                          float* pred_log_rho) {
+    LearnedState* ls = learned(h);
+    if (!mpnn_loaded(h)) return FSD_ERR_BAD_PARAMS;
+    MpState* s = mp(h);
+    cudaStream_t st = h->stream;
+    MP_TRY(precond_assemble_pruned(h, pos, 1.0f, &ls->a_pn, &ls->a_plist, &ls->a_blocks));
+    MP_TRY(spai_build(h));
+    double rho = 0.0;
+    float s0 = 0.f;
+    MP_TRY(mpnn_poly_ratio(h, pos, &rho, &s0));
+    const double d = (double)s0 - (double)target_log_rho;
+    MP_TRY(mp_alloc_backward(h));
+    PolyGrad pg{};
+    pg.g[0] = (float)(2.0 * d / s->N);  // d(d^2)/d s0, spread over the particles' outputs
+    count_launch();
+    k_fill_don<<<(unsigned)(((size_t)s->N * kMpHeadN + 255) / 256), 256, 0, st>>>(s->don, s->N, pg);
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->doe, 0, sizeof(float) * (size_t)s->E_cap * kMpHeadE, st));
+    FSD_CHECK_CUDA(cudaMemsetAsync(s->gw, 0, sizeof(float) * MpLayout::total, st));
+    MP_TRY(mp_backward(h));
+    if (lr > 0.f) {
+        s->adam_t += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)s->adam_t), c2 = 1.f - powf(b2, (float)s->adam_t);
+        count_launch();
+        k_adam<<<(MpLayout::total + 255) / 256, 256, 0, st>>>(s->w, s->gw, s->mw, s->vw, MpLayout::total, lr, b1, b2,
+                                                             c1, c2, 1e-8f, 1.0f);
+    }
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (s->use_umma && umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
+    if (loss) *loss = (float)(d * d);
+    if (pred_log_rho) *pred_log_rho = s0;
     return FSD_OK;
 }
 

@@ -104,81 +104,6 @@ __device__ __forceinline__ float a_row(const unsigned* __restrict__ pn, const un
     return acc;
 }
 
-// u = c_{k-1} G t with t = b[0:6N] - b[11N:17N]; T = t and B = c_{k-1} t (own row).
-__global__ void __launch_bounds__(256) k_poly_first(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                    const float* __restrict__ G, const float* __restrict__ b,
-                                                    const float* __restrict__ pc, int k, int N, float* __restrict__ T,
-                                                    float* __restrict__ B, float* __restrict__ U) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int r = threadIdx.x & 7;
-    if (i >= N) return;  // whole groups of eight leave together
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
-    const size_t offU = 11 * (size_t)N;
-    const float c = pc[k - 1];
-    const float acc = g_row<true>(rowptr, col, G, b, offU, i, r, gmask);
-    if (r < 6) {
-        const float t = b[6 * i + r] - b[offU + 6 * i + r];
-        T[6 * i + r] = t;
-        B[6 * i + r] = c * t;
-        U[6 * i + r] = c * acc;
-    }
-}
-
-// U = G X.
-__global__ void __launch_bounds__(256) k_poly_g(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                const float* __restrict__ G, const float* __restrict__ X, int N,
-                                                float* __restrict__ U) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int r = threadIdx.x & 7;
-    if (i >= N) return;
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
-    const float acc = g_row<false>(rowptr, col, G, X, 0, i, r, gmask);
-    if (r < 6) U[6 * i + r] = acc;
-}
-
-// out = c_m T + f ((2/lambda) A U - B1) - B2 (B2 may be null), f = 2 for m >= 1
-// and 1 for m = 0 (Clenshaw's last step).
-__global__ void __launch_bounds__(256) k_poly_a(const unsigned* __restrict__ pn, const unsigned* __restrict__ plist,
-                                                const float* __restrict__ A, const float* __restrict__ U,
-                                                const float* __restrict__ T, const float* __restrict__ B1,
-                                                const float* __restrict__ B2, const float* __restrict__ pc, int m,
-                                                int N, float* __restrict__ out) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int r = threadIdx.x & 7;
-    if (i >= N) return;
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
-    const float acc = a_row(pn, plist, A, U, i, r, gmask);
-    if (r < 6) {
-        const size_t q = 6 * (size_t)i + r;
-        const float s2 = 2.0f / pc[kMaxPoly];
-        const float f = m >= 1 ? 2.0f : 1.0f;
-        float v = fmaf(pc[m], T[q], f * fmaf(s2, acc, -B1[q]));
-        if (B2) v -= B2[q];
-        out[q] = v;
-    }
-}
-
-// y = G V; x = [b[0:6N] - y ; b[6N:11N] ; y].
-__global__ void __launch_bounds__(256) k_poly_last(const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                   const float* __restrict__ G, const float* __restrict__ V,
-                                                   const float* b, float* x, int N) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-    const int r = threadIdx.x & 7;
-    if (i >= N) return;
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
-    const float y = g_row<false>(rowptr, col, G, V, 0, i, r, gmask);
-    if (r < 6) {
-        const size_t q = 6 * (size_t)i + r;
-        const float bq = b[q];
-        x[q] = bq - y;
-        x[11 * (size_t)N + q] = y;
-    }
-    if (r < 5) {
-        const size_t q = 6 * (size_t)N + 5 * (size_t)i + r;
-        x[q] = b[q];
-    }
-}
-
 // ---------------------------------------------------------- spectral bound
 __global__ void k_set_double(double* p, double v) { *p = v; }
 
@@ -283,29 +208,153 @@ static int poly_v_slot(int k) {
     return cur;
 }
 
-// Kernels of one application on b into x, enqueued on st (for capture).
+// Block-CSR copy of A and the row tiles of G and A for the streamed
+// products (bsr_tma.cu), once per build.
+int poly_prepare_products(fsd_handle* h) {
+    LearnedState* s = learned(h);
+    const int N = h->p.N;
+    cudaStream_t st = h->stream;
+    std::vector<unsigned> pn(N);
+    std::vector<int> grow(N + 1), arow(N + 1);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(pn.data(), s->a_pn, sizeof(unsigned) * N, cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(grow.data(), s->g_rowptr, sizeof(int) * (N + 1), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));
+    arow[0] = 0;
+    for (int i = 0; i < N; ++i) arow[i + 1] = arow[i] + (int)pn[i];
+    const size_t nnz = (size_t)arow[N];
+    if (!s->a_rowptr) FSD_CHECK_CUDA(cudaMalloc(&s->a_rowptr, sizeof(int) * (N + 1)));
+    if (nnz + 8 > s->a_cap) {  // headroom: the column copy reads up to three past the end
+        if (s->a_col) cudaFree(s->a_col);
+        if (s->a_val) cudaFree(s->a_val);
+        s->a_col = nullptr;
+        s->a_val = nullptr;
+        const size_t cap = nnz + nnz / 8 + 1024;
+        FSD_CHECK_CUDA(cudaMalloc(&s->a_col, sizeof(int) * cap));
+        FSD_CHECK_CUDA(cudaMalloc(&s->a_val, sizeof(float) * 36 * cap));
+        s->a_cap = cap;
+    }
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->a_rowptr, arow.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice, st));
+    count_launch();
+    k_compact_pruned<<<(N + 7) / 8, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, s->a_rowptr, N, s->a_col,
+                                                  s->a_val);
+    std::vector<int> gt, at;
+    int e = bsr_make_tiles(grow, N, gt);
+    if (e != FSD_OK) return e;
+    e = bsr_make_tiles(arow, N, at);
+    if (e != FSD_OK) return e;
+    if (!s->g_tiles) {
+        s->tile_cap = N / 13 + 2;  // a full tile holds >= 13 rows (>= 417 of at most 448 blocks, rows <= 32)
+        FSD_CHECK_CUDA(cudaMalloc(&s->g_tiles, sizeof(int) * (s->tile_cap + 2)));
+        FSD_CHECK_CUDA(cudaMalloc(&s->a_tiles, sizeof(int) * (s->tile_cap + 2)));
+        e = bsr_tma_prepare();
+        if (e != FSD_OK) return e;
+    }
+    const int ng = (int)gt.size() - 1, na = (int)at.size() - 1;
+    if (ng > s->tile_cap || na > s->tile_cap) return FSD_ERR_BAD_PARAMS;
+    gt.resize(s->tile_cap + 1, N);
+    at.resize(s->tile_cap + 1, N);
+    gt.push_back(ng);
+    at.push_back(na);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->g_tiles, gt.data(), sizeof(int) * (s->tile_cap + 2), cudaMemcpyHostToDevice, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->a_tiles, at.data(), sizeof(int) * (s->tile_cap + 2), cudaMemcpyHostToDevice, st));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(st));  // the host tile vectors go out of scope
+    FSD_CHECK_CUDA(cudaGetLastError());
+    return FSD_OK;
+}
+
+// Clenshaw slots: b_{k-1} in slot 0; each b_m goes to the slot that holds
+// neither b_{m+1} nor b_{m+2}.
+static int poly_next_slot(int cur, int prev) { return (cur + 1) % 3 == prev ? (cur + 2) % 3 : (cur + 1) % 3; }
+
+// Slot that holds v = b_0 after the recurrence for k coefficients.
+static int poly_v_slot(int k) {
+    int cur = 0, prev = -1;
+    for (int m = k - 2; m >= 0; --m) {
+        const int nxt = poly_next_slot(cur, prev);
+        prev = cur;
+        cur = nxt;
+    }
+    return cur;
+}
+
+static BsrTmaArgs g_args(const LearnedState* s, int N) {
+    BsrTmaArgs a{};
+    a.rowptr = s->g_rowptr;
+    a.col = s->g_col;
+    a.val = s->g_val;
+    a.tile_row = s->g_tiles;
+    a.ntiles = s->g_tiles + s->tile_cap + 1;
+    a.N = N;
+    a.pc = s->pc;
+    return a;
+}
+
+static BsrTmaArgs a_args(const LearnedState* s, int N) {
+    BsrTmaArgs a{};
+    a.rowptr = s->a_rowptr;
+    a.col = s->a_col;
+    a.val = s->a_val;
+    a.tile_row = s->a_tiles;
+    a.ntiles = s->a_tiles + s->tile_cap + 1;
+    a.N = N;
+    a.pc = s->pc;
+    return a;
+}
+
+// Arguments of the first (mode 0) and last (mode 2) products for b and x.
+static BsrTmaArgs first_args(const LearnedState* s, int N, int k, const float* b) {
+    const size_t n6 = 6 * (size_t)N;
+    BsrTmaArgs a = g_args(s, N);
+    a.x = b;
+    a.T = s->pbuf;
+    a.out = s->pbuf + n6;
+    a.B = s->pbuf + 2 * n6;
+    a.k = k;
+    return a;
+}
+
+static BsrTmaArgs last_args(const LearnedState* s, int N, int k, const float* b, float* x) {
+    const size_t n6 = 6 * (size_t)N;
+    BsrTmaArgs a = g_args(s, N);
+    a.x = s->pbuf + (2 + poly_v_slot(k)) * n6;
+    a.b = b;
+    a.xs = x;
+    return a;
+}
+
+// Kernels of one application on b into x, enqueued on st (for capture):
+// k products with G and k - 1 with A.
 static int poly_enqueue(fsd_handle* h, const float* b, float* x, cudaStream_t st) {
     LearnedState* s = learned(h);
     const int N = h->p.N;
     const int k = h->p.learned_poly;
     const size_t n6 = 6 * (size_t)N;
-    const int rows = (8 * N + 255) / 256;
+    const int grid = s->tile_cap;
     float* T = s->pbuf;
     float* U = s->pbuf + n6;
     float* Bs[3] = {s->pbuf + 2 * n6, s->pbuf + 3 * n6, s->pbuf + 4 * n6};
-    // b_{k-1} -> Bs[0]; then b_m into the slot after b_{m+1}
-    k_poly_first<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, b, s->pc, k, N, T, Bs[0], U);
-    int cur = 0;           // slot of b_{m+1}
-    int prev = -1;         // slot of b_{m+2} (none for m = k-2)
+    bsr_tma_launch(0, first_args(s, N, k, b), grid, st);  // U = c_{k-1} G t, b_{k-1} -> slot 0
+    int cur = 0, prev = -1;
     for (int m = k - 2; m >= 0; --m) {
-        if (m < k - 2) k_poly_g<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, Bs[cur], N, U);
+        if (m < k - 2) {
+            BsrTmaArgs ga = g_args(s, N);
+            ga.x = Bs[cur];
+            ga.out = U;
+            bsr_tma_launch(1, ga, grid, st);
+        }
         const int nxt = poly_next_slot(cur, prev);
-        k_poly_a<<<rows, 256, 0, st>>>(s->a_pn, s->a_plist, s->a_blocks, U, T, Bs[cur], prev >= 0 ? Bs[prev] : nullptr,
-                                       s->pc, m, N, Bs[nxt]);
+        BsrTmaArgs aa = a_args(s, N);
+        aa.x = U;
+        aa.T = T;
+        aa.B1 = Bs[cur];
+        aa.B2 = prev >= 0 ? Bs[prev] : nullptr;
+        aa.m = m;
+        aa.out = Bs[nxt];
+        bsr_tma_launch(3, aa, grid, st);
         prev = cur;
         cur = nxt;
     }
-    k_poly_last<<<rows, 256, 0, st>>>(s->g_rowptr, s->g_col, s->g_val, Bs[cur], b, x, N);
+    bsr_tma_launch(2, last_args(s, N, k, b, x), grid, st);
     FSD_CHECK_CUDA(cudaGetLastError());
     return FSD_OK;
 }
@@ -314,9 +363,10 @@ static int poly_kernels(int k) { return 2 * k - 1; }
 
 static int poly_graph(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
-    const void* key[8] = {s->g_rowptr, s->g_col, s->g_val, s->a_pn, s->a_plist, s->a_blocks, s->pbuf, s->pc};
+    const void* key[12] = {s->g_rowptr, s->g_col, s->g_val, s->a_rowptr, s->a_col,  s->a_val,
+                           s->g_tiles,  s->a_tiles, s->pbuf, s->pc,       nullptr,   nullptr};
     bool same = s->pexec && s->pkey_k == h->p.learned_poly;
-    for (int i = 0; i < 8 && same; ++i) same = key[i] == s->pkey[i];
+    for (int i = 0; i < 10 && same; ++i) same = key[i] == s->pkey[i];
     if (same) return FSD_OK;
     if (s->pexec) cudaGraphExecDestroy(s->pexec);
     if (s->pgraph) cudaGraphDestroy(s->pgraph);
@@ -343,8 +393,8 @@ static int poly_graph(fsd_handle* h, const float* b, float* x) {
         if (t != cudaGraphNodeTypeKernel) continue;
         cudaKernelNodeParams kp;
         FSD_CHECK_CUDA(cudaGraphKernelNodeGetParams(nd, &kp));
-        if (kp.func == (void*)k_poly_first) s->pnode_first = nd;
-        if (kp.func == (void*)k_poly_last) s->pnode_last = nd;
+        if (kp.func == bsr_tma_kernel(0)) s->pnode_first = nd;
+        if (kp.func == bsr_tma_kernel(2)) s->pnode_last = nd;
     }
     if (!s->pnode_first || !s->pnode_last) {
         cudaGraphDestroy(g);
@@ -356,7 +406,7 @@ static int poly_graph(fsd_handle* h, const float* b, float* x) {
         FSD_CHECK_CUDA(ie);
     }
     s->pgraph = g;
-    for (int i = 0; i < 8; ++i) s->pkey[i] = key[i];
+    for (int i = 0; i < 10; ++i) s->pkey[i] = key[i];
     s->pkey_k = h->p.learned_poly;
     return FSD_OK;
 }
@@ -364,32 +414,20 @@ static int poly_graph(fsd_handle* h, const float* b, float* x) {
 // Point the first node at b and the last at (b, x).
 static int poly_bind(fsd_handle* h, const float* b, float* x) {
     LearnedState* s = learned(h);
-    int N = h->p.N;
-    int k = h->p.learned_poly;
-    const size_t n6 = 6 * (size_t)N;
-    const int rows = (8 * N + 255) / 256;
-    const int* rowptr = s->g_rowptr;
-    const int* col = s->g_col;
-    const float* G = s->g_val;
-    const float* pc = s->pc;
-    float* T = s->pbuf;
-    float* U = s->pbuf + n6;
-    float* B0 = s->pbuf + 2 * n6;
-    void* first_args[] = {&rowptr, &col, &G, &b, &pc, &k, &N, &T, &B0, &U};
-    cudaKernelNodeParams kf = {};
-    kf.func = (void*)k_poly_first;
-    kf.gridDim = dim3(rows);
-    kf.blockDim = dim3(256);
-    kf.kernelParams = first_args;
-    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->pexec, s->pnode_first, &kf));
-    const float* V = s->pbuf + (2 + poly_v_slot(k)) * n6;  // the Clenshaw slot that holds v
-    void* last_args[] = {&rowptr, &col, &G, &V, &b, &x, &N};
-    cudaKernelNodeParams kl = {};
-    kl.func = (void*)k_poly_last;
-    kl.gridDim = dim3(rows);
-    kl.blockDim = dim3(256);
-    kl.kernelParams = last_args;
-    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->pexec, s->pnode_last, &kl));
+    const int N = h->p.N, k = h->p.learned_poly;
+    BsrTmaArgs fa = first_args(s, N, k, b), la = last_args(s, N, k, b, x);
+    void* fargs[] = {&fa};
+    void* largs[] = {&la};
+    cudaKernelNodeParams kp = {};
+    kp.gridDim = dim3(s->tile_cap);
+    kp.blockDim = dim3(256);
+    kp.sharedMemBytes = (unsigned)bsr_tma_smem();
+    kp.func = (void*)bsr_tma_kernel(0);
+    kp.kernelParams = fargs;
+    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->pexec, s->pnode_first, &kp));
+    kp.func = (void*)bsr_tma_kernel(2);
+    kp.kernelParams = largs;
+    FSD_CHECK_CUDA(cudaGraphExecKernelNodeSetParams(s->pexec, s->pnode_last, &kp));
     return FSD_OK;
 }
 
@@ -404,6 +442,55 @@ int poly_apply(fsd_handle* h, const float* b, float* x) {
     return FSD_OK;
 }
 
+// Coefficients of q for the Chebyshev interval [rho lambda, lambda]: the
+// residual polynomial 1 - x q(x) = T_k((1 + rho - 2u)/(1 - rho)) /
+// T_k((1 + rho)/(1 - rho)), u = x / lambda, is the classical Chebyshev
+// acceleration on that interval (bounded by one on all of [0, lambda], so no
+// eigenvalue of AG is amplified, and smallest on [rho lambda, lambda]).  q has
+// degree k - 1 and is expanded exactly in T_m(2u - 1), m < k, by Chebyshev
+// interpolation at k nodes (FP64).
+static double cheb_T(int n, double z) {
+    if (std::fabs(z) <= 1.0) return std::cos(n * std::acos(z));
+    const double v = std::cosh(n * std::acosh(std::fabs(z)));
+    return (z < 0 && (n & 1)) ? -v : v;
+}
+
+void poly_interval_coefficients(double rho, double lambda, int k, float* c) {
+    const double zs = (1.0 + rho) / (1.0 - rho);
+    const double Tz = cheb_T(k, zs);
+    std::vector<double> gu(k), uu(k);
+    for (int j = 0; j < k; ++j) {
+        const double th = M_PI * (j + 0.5) / k;
+        const double u = 0.5 * (std::cos(th) + 1.0);
+        const double r = cheb_T(k, (1.0 + rho - 2.0 * u) / (1.0 - rho)) / Tz;
+        uu[j] = u;
+        gu[j] = (1.0 - r) / (lambda * u);
+    }
+    for (int m = 0; m < k; ++m) {
+        double acc = 0.0;
+        for (int j = 0; j < k; ++j) acc += gu[j] * std::cos(m * M_PI * (j + 0.5) / k);
+        c[m] = (float)((m == 0 ? 1.0 : 2.0) * acc / k);
+    }
+}
+
+// Coefficients for the interval ratio rho (in (0, 1)) with the spectral
+// bound of the last power iteration; caller's stream, synchronised.
+int poly_set_interval(fsd_handle* h, double rho) {
+    LearnedState* s = learned(h);
+    const int k = h->p.learned_poly;
+    float pc[kMaxPoly + 1];
+    FSD_CHECK_CUDA(cudaMemcpyAsync(pc, s->pc, sizeof(float) * (kMaxPoly + 1), cudaMemcpyDeviceToHost, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    const double lambda = pc[kMaxPoly];
+    if (!(lambda > 0.0) || !(rho > 0.0 && rho < 1.0)) return FSD_ERR_BREAKDOWN;
+    float c[kMaxPoly] = {};
+    poly_interval_coefficients(rho, lambda, k, c);
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->pc, c, sizeof(float) * kMaxPoly, cudaMemcpyHostToDevice, h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    s->poly_ratio = (float)rho;
+    return FSD_OK;
+}
+
 int poly_set_coefficients(fsd_handle* h, const float* host_c, int k) {
     if (k < 2 || k > kMaxPoly || !host_c) return FSD_ERR_BAD_PARAMS;
     const int e = poly_alloc(h);
@@ -414,6 +501,7 @@ int poly_set_coefficients(fsd_handle* h, const float* host_c, int k) {
     FSD_CHECK_CUDA(cudaMemcpyAsync(s->pc, c, sizeof(float) * kMaxPoly, cudaMemcpyHostToDevice, h->stream));
     FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
     s->poly_user = true;
+    s->user_ratio = -1.f;
     return FSD_OK;
 }
 
@@ -426,7 +514,8 @@ int poly_get_coefficients(fsd_handle* h, float* host_c, int n) {
 }
 
 void poly_free(LearnedState* s) {
-    void* ptrs[] = {s->pc, s->pbuf, s->ppart, s->pnrm, s->pticket};
+    void* ptrs[] = {s->pc, s->pbuf, s->ppart, s->pnrm, s->pticket, s->a_rowptr, s->a_col, s->a_val, s->g_tiles,
+                    s->a_tiles};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->pexec) cudaGraphExecDestroy(s->pexec);

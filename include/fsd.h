@@ -97,11 +97,15 @@ typedef struct fsd_params {
     int learned_inner;           /* FSD_PRECOND_LEARNED: inner GMRES steps on R_FU^pruned + D per application,
                                     right-preconditioned by the learned block-sparse G (4; 0 = apply G once).
                                     With inner steps the outer solve is flexible GMRES. */
-    int learned_poly;            /* FSD_PRECOND_LEARNED: when >= 2 (at most 16) and coefficients are available
-                                    (network weights, or fsd_learned_set_poly), y ~ (R_FU^pruned + D)^-1 t is
-                                    G q(AG) t with a Chebyshev polynomial q of this many coefficients on the
-                                    spectrum of AG, predicted per configuration by the network; the outer
-                                    solve stays plain GMRES.  0 (default): learned_inner decides. */
+    int learned_poly;            /* FSD_PRECOND_LEARNED: when >= 2 (at most 16), y ~ (R_FU^pruned + D)^-1 t is
+                                    G q(AG) t with a polynomial q of degree learned_poly - 1, expanded in
+                                    Chebyshev polynomials on [0, lambda] (lambda: power-iteration bound of
+                                    the spectrum of AG, times 1.1), so 1 - x q(x) is the Chebyshev
+                                    acceleration on [rho lambda, lambda]; the network predicts rho for each
+                                    configuration.  The outer solve stays plain GMRES.  0 (default):
+                                    learned_inner decides. */
+    float poly_interval;         /* learned_poly without network weights: the fixed ratio rho (0.05); 0 = fit
+                                    the coefficients to four probe vectors at every build instead */
     int autotune;                /* 1: time candidate spreading tiles and FFT line batches on the first mobility
                                     call and keep the fastest (cached per process and grid shape).  Results then
                                     depend on the choice through the summation order, so runs in different
@@ -137,11 +141,13 @@ typedef struct fsd_solve_info {
     int status;                  /* fsd_status of that call */
     int ichol_shifted;           /* pivot blocks that needed a local shift */
     float ichol_gain;            /* power-iteration estimate of lambda_max(G) of the accepted factor */
-    int poly_source;             /* learned_poly: coefficients of the last build, 1 the network's, 2 a
-                                    least-squares fit on probe vectors, 3 the caller's (0: not in use) */
+    int poly_source;             /* learned_poly: coefficients of the last build, 1 the Chebyshev interval the
+                                    network predicts, 2 a least-squares fit on probe vectors, 3 the caller's,
+                                    4 a fixed interval (0: not in use) */
     float poly_loss_net;         /* probe loss ||t - AG q(AG) t||^2/||t||^2 of the network's coefficients at
                                     the last build (-1: none) */
     float poly_loss_fit;         /* loss of the least-squares fit on its four probes (-1: not fitted) */
+    float poly_ratio;            /* Chebyshev interval ratio rho of the last build (-1: none) */
 } fsd_solve_info;
 
 /* Arguments of one time step (Stokes_StepOne, Stokes.cuh:81-108). */
@@ -320,12 +326,22 @@ int fsd_learned_train_step(fsd_handle* h, const float* d_pos, const float* host_
  * network is fed the Gauss-Newton direction 2 (c - c_opt) in place of the
  * loss gradient (the loss is quadratic in c with a badly conditioned
  * Hessian); host_grad then holds that direction's weight gradient.
- * At every build in learned_poly mode without caller's coefficients, the
- * network's coefficients are scored on one probe vector and kept when the
- * relative residual they leave, ||t - AG q(AG) t||^2 / ||t||^2, is at most
- * 0.05; otherwise, and without a network, a least-squares fit on four probe
- * vectors is used (fsd_solve_info poly_source and the losses). */
+ * These train the coefficients themselves (the loss a least-squares fit
+ * minimises); the default learned_poly mode trains the interval instead
+ * (fsd_learned_ratio_train_step). */
 int fsd_learned_set_poly(fsd_handle* h, const float* host_c, int k);
+/* Fixed Chebyshev interval ratio rho (0 < rho < 1) for the next builds in
+ * place of the network's prediction (0 clears it; setting weights clears it
+ * too), and the coefficients of that interval's polynomial for a spectral
+ * bound lambda and k terms (host only). */
+int fsd_learned_set_interval(fsd_handle* h, float rho);
+int fsd_learned_interval_coefficients(float rho, float lambda, int k, float* host_c);
+/* One training step of the interval network on this configuration (the
+ * neighbour list current for d_pos): the squared error between the predicted
+ * log rho and target_log_ratio (the ratio that gave the fewest outer
+ * iterations), the prediction, and, when lr > 0, one Adam step. */
+int fsd_learned_ratio_train_step(fsd_handle* h, const float* d_pos, float target_log_ratio, float lr, float* loss,
+                                 float* predicted_log_ratio);
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n);
 int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
                                 int natural, float* loss, float* loss_opt, float* host_grad, float* host_coef,
