@@ -120,7 +120,7 @@ _SIGS = {
     "fsd_learned_set_interval": (C.c_int, [H, C.c_float]),
     "fsd_learned_interval_coefficients": (C.c_int, [C.c_float, C.c_float, C.c_int, P]),
     "fsd_learned_ratio_train_step": (C.c_int, [H, P, C.c_float, C.c_float, C.POINTER(C.c_float),
-                                               C.POINTER(C.c_float)]),
+                                               C.POINTER(C.c_float), P]),
     "fsd_learned_poly_train_step": (C.c_int, [H, P, C.c_int, C.c_uint, C.c_float, C.c_int, C.POINTER(C.c_float),
                                               C.POINTER(C.c_float), P, P, P]),
     "fsd_precond_apply": (C.c_int, [H, P, P]),

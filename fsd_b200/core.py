@@ -269,13 +269,16 @@ class FSD:
         """Fixed Chebyshev interval ratio for the next builds (0 clears it)."""
         check(lib().fsd_learned_set_interval(self._h, float(rho)), "fsd_learned_set_interval")
 
-    def learned_ratio_train_step(self, pos, target_log_ratio: float, lr: float = 0.0):
-        """(squared error, predicted log ratio) of the interval network on this configuration."""
+    def learned_ratio_train_step(self, pos, target_log_ratio: float, lr: float = 0.0, want_grad: bool = False):
+        """(squared error, predicted log ratio[, weight gradient]) of the interval network on this configuration."""
         self._sync_stream()
         loss, pred = C.c_float(0.0), C.c_float(0.0)
+        g = np.zeros(lib().fsd_learned_num_weights(), np.float32) if want_grad else None
         check(lib().fsd_learned_ratio_train_step(self._h, _ptr(pos), float(target_log_ratio), float(lr),
-                                                 C.byref(loss), C.byref(pred)), "fsd_learned_ratio_train_step")
-        return loss.value, pred.value
+                                                 C.byref(loss), C.byref(pred),
+                                                 g.ctypes.data_as(C.c_void_p) if want_grad else None),
+              "fsd_learned_ratio_train_step")
+        return (loss.value, pred.value, g) if want_grad else (loss.value, pred.value)
 
     def learned_tensor_cores(self, on: bool):
         check(lib().fsd_learned_tensor_cores(self._h, int(bool(on))), "fsd_learned_tensor_cores")

@@ -553,9 +553,10 @@ int fsd_learned_interval_coefficients(float rho, float lambda, int k, float* hos
 }
 
 int fsd_learned_ratio_train_step(fsd_handle* h, const float* d_pos, float target_log_ratio, float lr, float* loss,
-                                 float* predicted_log_ratio) {
+                                 float* predicted_log_ratio, float* host_grad) {
     if (!h || !d_pos || !h->nlist_valid || h->p.learned_poly < 2) return FSD_ERR_BAD_PARAMS;
-    return mpnn_ratio_train_step(h, (const float4*)d_pos, target_log_ratio, lr, loss, predicted_log_ratio);
+    return mpnn_ratio_train_step(h, (const float4*)d_pos, target_log_ratio, lr, loss, predicted_log_ratio,
+                                 host_grad);
 }
 
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n) {

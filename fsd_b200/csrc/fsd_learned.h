@@ -148,6 +148,6 @@ int mpnn_poly_calibrate(fsd_handle* h, int k, uint32_t step);
 // first output, clamped to [kRatioMin, kRatioMax]).
 int mpnn_poly_ratio(fsd_handle* h, const float4* pos, double* rho, float* log_rho);
 int mpnn_ratio_train_step(fsd_handle* h, const float4* pos, float target_log_rho, float lr, float* loss,
-                          float* pred_log_rho);
+                          float* pred_log_rho, float* host_grad);
 
 }  // namespace fsd

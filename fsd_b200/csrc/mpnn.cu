@@ -1463,7 +1463,7 @@ int mpnn_poly_ratio(fsd_handle* h, const float4* pos, double* rho, float* log_rh
 }
 
 int mpnn_ratio_train_step(fsd_handle* h, const float4* pos, float target_log_rho, float lr, float* loss,
-                          float* pred_log_rho) {
+                          float* pred_log_rho, float* host_grad) {
     LearnedState* ls = learned(h);
     if (!mpnn_loaded(h)) return FSD_ERR_BAD_PARAMS;
     MpState* s = mp(h);
@@ -1490,6 +1490,8 @@ int mpnn_ratio_train_step(fsd_handle* h, const float4* pos, float target_log_rho
         k_adam<<<(MpLayout::total + 255) / 256, 256, 0, st>>>(s->w, s->gw, s->mw, s->vw, MpLayout::total, lr, b1, b2,
                                                              c1, c2, 1e-8f, 1.0f);
     }
+    if (host_grad)
+        FSD_CHECK_CUDA(cudaMemcpyAsync(host_grad, s->gw, sizeof(float) * MpLayout::total, cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaStreamSynchronize(st));
     if (s->use_umma && umma_error() != 0) return FSD_ERR_DEVICE_WAIT;
     if (loss) *loss = (float)(d * d);

@@ -339,9 +339,10 @@ int fsd_learned_interval_coefficients(float rho, float lambda, int k, float* hos
 /* One training step of the interval network on this configuration (the
  * neighbour list current for d_pos): the squared error between the predicted
  * log rho and target_log_ratio (the ratio that gave the fewest outer
- * iterations), the prediction, and, when lr > 0, one Adam step. */
+ * iterations), the prediction, the weight gradient (host_grad, optional,
+ * fsd_learned_num_weights() floats) and, when lr > 0, one Adam step. */
 int fsd_learned_ratio_train_step(fsd_handle* h, const float* d_pos, float target_log_ratio, float lr, float* loss,
-                                 float* predicted_log_ratio);
+                                 float* predicted_log_ratio, float* host_grad);
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n);
 int fsd_learned_poly_train_step(fsd_handle* h, const float* d_pos, int n_probes, unsigned int step, float lr,
                                 int natural, float* loss, float* loss_opt, float* host_grad, float* host_coef,

@@ -236,3 +236,30 @@ def poly_apply(b, c, lam, A, G, N):
     x[: 6 * N] = b[: 6 * N] - y
     x[11 * N:] = y
     return x
+
+
+def interval_coefficients(rho, k):
+    """Coefficients c_m (m < k, lambda = 1) of q in T_m(2u - 1) with
+    1 - u q(u) = T_k((1 + rho - 2u)/(1 - rho)) / T_k((1 + rho)/(1 - rho)):
+    FP64 least squares on 64 points, an independent route to the library's
+    interpolation."""
+    def T(n, z):
+        z = np.asarray(z, np.float64)
+        out = np.empty_like(z)
+        m = np.abs(z) <= 1
+        out[m] = np.cos(n * np.arccos(z[m]))
+        zz = z[~m]
+        out[~m] = np.cosh(n * np.arccosh(np.abs(zz))) * np.where((zz < 0) & (n % 2 == 1), -1.0, 1.0)
+        return out
+    u = np.linspace(0.01, 1.0, 64)
+    r = T(k, (1 + rho - 2 * u) / (1 - rho)) / T(k, np.array([(1 + rho) / (1 - rho)]))[0]
+    q = (1 - r) / u
+    B = np.stack([T(m, 2 * u - 1) for m in range(k)], 1)
+    c, *_ = np.linalg.lstsq(B, q, rcond=None)
+    return c
+
+
+def ratio_loss(wv, pr, target):
+    """(log rho prediction - target)^2 with log rho = mean of the node head's first output."""
+    _, on = forward(wv, pr["x"], pr["i"], pr["j"], pr["N"])
+    return float((on[:, 0].mean() - target) ** 2)
