@@ -193,21 +193,6 @@ int poly_lambda(fsd_handle* h) {
     return FSD_OK;
 }
 
-// Clenshaw slots: b_{k-1} in slot 0; each b_m goes to the slot that holds
-// neither b_{m+1} nor b_{m+2}.  Returns the slot of b_m and updates (cur, prev).
-static int poly_next_slot(int cur, int prev) { return (cur + 1) % 3 == prev ? (cur + 2) % 3 : (cur + 1) % 3; }
-
-// Slot that holds v = b_0 after the recurrence for k coefficients.
-static int poly_v_slot(int k) {
-    int cur = 0, prev = -1;
-    for (int m = k - 2; m >= 0; --m) {
-        const int nxt = poly_next_slot(cur, prev);
-        prev = cur;
-        cur = nxt;
-    }
-    return cur;
-}
-
 // Block-CSR copy of A and the row tiles of G and A for the streamed
 // products (bsr_tma.cu), once per build.
 int poly_prepare_products(fsd_handle* h) {
