@@ -12,7 +12,10 @@ learned_poly mode).
   along random directions 5e-3 (the FP32 backward through three
   message-passing layers measured 4e-3).
 * A build with a fixed interval uses it (solve info) and its application
-  matches the oracle's FP64 Clenshaw evaluation of the same coefficients: 1e-5.
+  matches the oracle's FP64 Clenshaw evaluation of the same coefficients:
+  1e-4.  The interval polynomial's Chebyshev coefficients alternate in sign
+  with sum of magnitudes near 45 (rho = 0.05, ten terms), so the recurrence
+  amplifies FP32 rounding about 45-fold (2.5e-5 measured).
 """
 from __future__ import annotations
 
@@ -95,5 +98,5 @@ def test_fixed_interval_application_matches_oracle(cuda):
     got = s.precond_apply(torch.as_tensor(b, dtype=torch.float32).cuda()).cpu().numpy()
     ref = M.poly_apply(b.astype(np.float32).astype(np.float64), c.astype(np.float64), np.float64(np.float32(lam)),
                        pr["A"], pr["G0"], N)
-    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-4
     s.close()
