@@ -56,21 +56,24 @@ def rsa(N: int, L: float, rng: np.random.Generator, min_gap: float = 1e-3, max_r
     return pos
 
 
-def relax_overlaps(pos: np.ndarray, L: float, min_gap: float = 1e-3, sweeps: int = 200) -> np.ndarray:
-    """Separate overlapping pairs along their line of centres until the minimum
-    gap holds or the sweep budget runs out."""
+def relax_overlaps(pos: np.ndarray, L: float, min_gap: float = 1e-3, sweeps: int = 200, target_gap: float | None = None,
+                   factor: float = 1.02) -> np.ndarray:
+    """Separate pairs closer than the minimum gap along their line of centres
+    (each by `factor` times half the shortfall to `target_gap`, default the
+    minimum gap) until the minimum gap holds or the sweep budget runs out."""
     dmin = 2.0 + min_gap
+    dpush = 2.0 + (min_gap if target_gap is None else target_gap)
     pos = pos.copy()
     for _ in range(sweeps):
         tree = cKDTree(_wrap(pos, L), boxsize=L)
-        pairs = tree.query_pairs(dmin, output_type="ndarray")
-        if len(pairs) == 0:
+        if len(tree.query_pairs(dmin, output_type="ndarray")) == 0:
             break
+        pairs = tree.query_pairs(dpush, output_type="ndarray")
         d = pos[pairs[:, 1]] - pos[pairs[:, 0]]
         d -= L * np.rint(d / L)
         r = np.linalg.norm(d, axis=1)
         r = np.maximum(r, 1e-9)
-        push = 0.5 * (dmin - r)[:, None] * d / r[:, None] * 1.02
+        push = 0.5 * (dpush - r)[:, None] * d / r[:, None] * factor
         disp = np.zeros_like(pos)
         np.add.at(disp, pairs[:, 0], -push)
         np.add.at(disp, pairs[:, 1], push)
@@ -86,6 +89,10 @@ def suspension(N: int, phi: float, seed: int, min_gap: float = 1e-3, relax_sweep
     if len(pos) < N:
         pos = np.concatenate([pos, rng.random((N - len(pos), 3)) * L])
     pos = relax_overlaps(pos, L, min_gap, relax_sweeps)
+    if min_gap_f64(pos, L) < 0.0:
+        # overlaps left (phi above about 0.5): push pairs toward three times
+        # the gap, one and a half times the shortfall per sweep, until it holds
+        pos = relax_overlaps(pos, L, min_gap, 1000, target_gap=3 * min_gap, factor=1.5)
     pos = _wrap(pos, L) - L / 2.0
     out = np.zeros((N, 4), np.float32)
     out[:, :3] = pos
@@ -93,6 +100,13 @@ def suspension(N: int, phi: float, seed: int, min_gap: float = 1e-3, relax_sweep
     x = out[:, :3]
     x[x >= np.float32(L / 2.0)] -= np.float32(L)
     return out, L
+
+
+def min_gap_f64(pos: np.ndarray, L: float) -> float:
+    """Smallest surface gap of positions in [0, L)^3 (or any periodic image)."""
+    p = _wrap(np.asarray(pos, np.float64)[:, :3], L)
+    d, _ = cKDTree(p, boxsize=L).query(p, k=2)
+    return float(d[:, 1].min() - 2.0)
 
 
 def min_gap(pos: np.ndarray, L: float) -> float:

@@ -175,6 +175,7 @@ struct TuneChoice {
     int TX = 0, TY = 0, TZ = 0;  // spreading tile
     int Bxy = 0, Bz = 0;         // FFT lines per block (x/y passes, z pass)
     int Bg = 0;                  // z-run length of the fused x-pass + Green kernel
+    int spread_rows = 0;         // 1: one node per thread walking stencil rows; 0: warp node blocks
     bool set = false;
 };
 

@@ -898,10 +898,20 @@ struct __align__(16) StagedParticle {  // read as four float4: (x, y, z, o), v[0
 // cell order; cell_off[c] is the first staged index of extended cell c (the
 // launch's dynamic shared memory, ncell + 1 entries).  The particles that
 // reach a node are those whose stencil origin lies in the P^3 cells below
-// it: for each of its P x P (x, y) rows a contiguous range of P cells, so a
-// node visits exactly its contributors, in staged order.
+// it.  Two ways of visiting them, both adding each node's contributions in
+// staged order (so both give the same sums):
+//  ROWS = true   one node per thread; for each of its P x P (x, y) rows a
+//                contiguous range of P cells, so a node visits exactly its
+//                contributors (lanes diverge on uneven row lengths);
+//  ROWS = false  a warp owns a 2 x 4 x 4 block of nodes; it ballots which
+//                staged particles reach the block and takes them one at a
+//                time, every lane reading the same particle (a shared-memory
+//                broadcast) and adding it when its node lies in the stencil.
+//                Needs TX % 2 == 0, TY % 4 == 0, TZ % 4 == 0.
+template <bool ROWS>
 __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     __shared__ StagedParticle sp[kSpreadCap];
+    __shared__ int so[ROWS ? 1 : kSpreadCap];  // packed origins, contiguous for the ballot
     __shared__ unsigned scan_sh[32];
     __shared__ unsigned s_total;
     extern __shared__ unsigned cell_off[];
@@ -925,14 +935,32 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     const int nth = blockDim.x;
     const int cpt = (ncell + nth - 1) / nth;  // extended cells per thread, contiguous
     // Count staged particles per thread (deterministic order: cell order, then bin order).
+    // The extended cells are walked with running coordinates (one division per
+    // thread); ex0 + cx lies in [-(P - 1), 2 Nx) because TX <= Nx - P + 1, so
+    // one conditional add or subtract wraps it.  Each cell's bin goes to
+    // cell_bin for the staging pass.
+    unsigned* cell_bin = cell_off + ncell + 1;
     unsigned mycount = 0;
     const int c_begin = threadIdx.x * cpt, c_end = min(ncell, (threadIdx.x + 1) * cpt);
-    for (int c = c_begin; c < c_end; ++c) {
-        const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
-        const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
-        const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
-        cell_off[c] = mycount;  // offset within this thread's cells; the block offset is added below
-        mycount += a.bin_start[bin + 1] - a.bin_start[bin];
+    {
+        int cz = c_begin % EZ, cy = (c_begin / EZ) % EY, cx = c_begin / (EZ * EY);
+        for (int c = c_begin; c < c_end; ++c) {
+            int gx = ex0 + cx, gy = ey0 + cy, gz = ez0 + cz;
+            gx += gx < 0 ? a.Nx : (gx >= a.Nx ? -a.Nx : 0);
+            gy += gy < 0 ? a.Ny : (gy >= a.Ny ? -a.Ny : 0);
+            gz += gz < 0 ? a.Nz : (gz >= a.Nz ? -a.Nz : 0);
+            const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
+            cell_bin[c] = bin;
+            cell_off[c] = mycount;  // offset within this thread's cells; the block offset is added below
+            mycount += a.bin_start[bin + 1] - a.bin_start[bin];
+            if (++cz == EZ) {
+                cz = 0;
+                if (++cy == EY) {
+                    cy = 0;
+                    ++cx;
+                }
+            }
+        }
     }
     // Block exclusive scan of counts.
     unsigned x = mycount;
@@ -961,7 +989,21 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     if (threadIdx.x == 0) cell_off[ncell] = total;
 
     // This thread's node.
-    const int lz = threadIdx.x % a.TZ, ly = (threadIdx.x / a.TZ) % a.TY, lx = threadIdx.x / (a.TZ * a.TY);
+    int lx, ly, lz;
+    int bx = 0, by = 0, bz = 0;  // the warp's node block (ROWS = false)
+    if (ROWS) {
+        lz = threadIdx.x % a.TZ;
+        ly = (threadIdx.x / a.TZ) % a.TY;
+        lx = threadIdx.x / (a.TZ * a.TY);
+    } else {
+        const int WZ = a.TZ >> 2, WY = a.TY >> 2;
+        bz = 4 * (wid % WZ);
+        by = 4 * ((wid / WZ) % WY);
+        bx = 2 * (wid / (WZ * WY));
+        lz = bz + (lane & 3);
+        ly = by + ((lane >> 2) & 3);
+        lx = bx + (lane >> 4);
+    }
     const int nx = x0 + lx, ny = y0 + ly, nz = z0 + lz;
     const bool active = (lx < a.TX) && nx < a.Nx && ny < a.Ny && nz < a.Nz;
     const float Ld2x = a.box.Lx / 2.0f, Ld2y = a.box.Ly / 2.0f, Ld2z = a.box.Lz / 2.0f;
@@ -979,11 +1021,11 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
     for (unsigned chunk = 0; chunk < total; chunk += kSpreadCap) {
         // Stage this thread's particles that fall in [chunk, chunk + cap).
         unsigned k = myoff;
-        for (int c = threadIdx.x * cpt; c < min(ncell, (threadIdx.x + 1) * cpt); ++c) {
-            const int cz = c % EZ, cy = (c / EZ) % EY, cx = c / (EZ * EY);
-            const int gx = (ex0 + cx + a.Nx) % a.Nx, gy = (ey0 + cy + a.Ny) % a.Ny, gz = (ez0 + cz + a.Nz) % a.Nz;
-            const unsigned bin = (unsigned)((gx * a.Ny + gy) * a.Nz + gz);
-            for (unsigned q = a.bin_start[bin]; q < a.bin_start[bin + 1]; ++q, ++k) {
+        int cz = c_begin % EZ, cy = (c_begin / EZ) % EY, cx = c_begin / (EZ * EY);
+        for (int c = c_begin; c < c_end; ++c) {
+            const unsigned bin = cell_bin[c];
+            const unsigned q1 = a.bin_start[bin + 1];
+            for (unsigned q = a.bin_start[bin]; q < q1; ++q, ++k) {
                 if (k < chunk || k >= chunk + kSpreadCap) continue;
                 const unsigned p = a.bin_parts[q];
                 StagedParticle& s = sp[k - chunk];
@@ -999,15 +1041,72 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
                     s.z = ps.z;
                 }
                 s.o = cx | (cy << 10) | (cz << 20);
+                if (!ROWS) so[k - chunk] = s.o;
                 const float4 f = a.f4[p], c0 = a.c4[2 * p], c1 = a.c4[2 * p + 1];
                 // pairs: (Fx,Fy) (Cxx,Cxy) (Cxz,Cyx) (Cyy,Cyz) (Czx,Czy) (Fz,0)
                 s.v[0] = f.x; s.v[1] = f.y; s.v[2] = c0.x; s.v[3] = c0.y; s.v[4] = c0.z; s.v[5] = c1.y;
                 s.v[6] = c1.x; s.v[7] = c0.w; s.v[8] = c1.z; s.v[9] = c1.w; s.v[10] = f.z; s.v[11] = 0.0f;
             }
+            if (++cz == EZ) {
+                cz = 0;
+                if (++cy == EY) {
+                    cy = 0;
+                    ++cx;
+                }
+            }
         }
         __syncthreads();
         const unsigned cend = chunk + min((unsigned)kSpreadCap, total - chunk);
-        if (active) {
+        if (!ROWS) {
+            // Lane (i, j, k) of the warp holds node (bx + i, by + j, bz + k),
+            // lane = 16 i + 4 j + k.  For the particle it examines, each lane
+            // builds the mask of the warp's lanes inside that particle's
+            // stencil (i in [dx - P + 1, dx], dx = cx - bx, and so on); the
+            // warp then takes the particles whose mask is not empty in staged
+            // order and reads the mask from the examining lane.
+            const unsigned cnt = cend - chunk;
+            const unsigned live = __ballot_sync(0xffffffffu, active);
+            for (unsigned base = 0; base < cnt; base += 32) {
+                unsigned lm = 0;
+                if (base + lane < cnt) {
+                    const int o = so[base + lane];
+                    const int dx = (o & 1023) - bx, dy = ((o >> 10) & 1023) - by, dz = (o >> 20) - bz;
+                    // bits [max(0, d - P + 1), min(w - 1, d)] of a w-bit row
+                    auto span = [P](int d, int w) -> unsigned {
+                        const int lo = max(0, d - P + 1), hi = min(w - 1, d);
+                        return lo <= hi ? ((2u << hi) - (1u << lo)) : 0u;
+                    };
+                    const unsigned mx = span(dx, 2), my = span(dy, 4), mz = span(dz, 4);
+                    const unsigned yz = mz * ((my & 1u) | ((my & 2u) << 3) | ((my & 4u) << 6) | ((my & 8u) << 9));
+                    lm = yz * ((mx & 1u) | ((mx & 2u) << 15)) & live;
+                }
+                unsigned m = __ballot_sync(0xffffffffu, lm != 0);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    const unsigned mask = __shfl_sync(0xffffffffu, lm, b);
+                    if ((mask >> lane) & 1u) {
+                        const float4* s4 = reinterpret_cast<const float4*>(&sp[base + b]);
+                        const float4 sx = s4[0], v0 = s4[1], v1 = s4[2], v2 = s4[3];
+                        const float3 r = a.local ? make_float3(sx.x + dn.x, sx.y + dn.y, sx.z + dn.z)
+                                                 : min_image(make_float3(pg.x - sx.x, pg.y - sx.y, pg.z - sx.z), a.box);
+                        const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
+                        const float wgt = a.prefac * expf(-a.expfac * rsq);
+                        acc[0] += wgt * v0.x;
+                        acc[1] += wgt * v0.y;
+                        acc[2] += wgt * v0.z;
+                        acc[3] += wgt * v0.w;
+                        acc[4] += wgt * v1.x;
+                        acc[5] += wgt * v1.y;
+                        acc[6] += wgt * v1.z;
+                        acc[7] += wgt * v1.w;
+                        acc[8] += wgt * v2.x;
+                        acc[9] += wgt * v2.y;
+                        acc[10] += wgt * v2.z;
+                    }
+                }
+            }
+        } else if (active) {
             for (int ix = 0; ix < P; ++ix) {
                 for (int iy = 0; iy < P; ++iy) {
                     const int c0 = ((lx + ix) * EY + (ly + iy)) * EZ + lz;
@@ -1307,9 +1406,13 @@ static void spread(fsd_handle* h, const float4* pos) {
     a.local = (a.TX + g.P) * tilt < 0.5f * g.Nx && (a.TY + g.P) * tilt < 0.5f * g.Ny &&
               (a.TZ + g.P) * tilt < 0.5f * g.Nz;
     const int ntiles = ((g.Nx + a.TX - 1) / a.TX) * ((g.Ny + a.TY - 1) / a.TY) * ((g.Nz + a.TZ - 1) / a.TZ);
-    const size_t cell_bytes = sizeof(unsigned) * ((size_t)(a.TX + g.P - 1) * (a.TY + g.P - 1) * (a.TZ + g.P - 1) + 1);
+    const size_t cell_bytes = sizeof(unsigned) * (2 * (size_t)(a.TX + g.P - 1) * (a.TY + g.P - 1) * (a.TZ + g.P - 1) + 1);
+    const bool blocks = a.TX % 2 == 0 && a.TY % 4 == 0 && a.TZ % 4 == 0 && a.TX * a.TY * a.TZ == 256;
     count_launch();
-    k_spread<<<ntiles, a.TX * a.TY * a.TZ, cell_bytes, h->stream>>>(a);
+    if (blocks && !(h->tune.set && h->tune.spread_rows))
+        k_spread<false><<<ntiles, a.TX * a.TY * a.TZ, cell_bytes, h->stream>>>(a);
+    else
+        k_spread<true><<<ntiles, a.TX * a.TY * a.TZ, cell_bytes, h->stream>>>(a);
 }
 
 static void contract(fsd_handle* h, const float4* pos) {
@@ -1409,18 +1512,22 @@ static int autotune(fsd_handle* h, const float4* pos) {
     const int tx_c[] = {1, 2, 4, 8}, ty_c[] = {2, 4, 8}, tz_c[] = {4, 8, 16, 32};
     for (int TX : tx_c)
         for (int TY : ty_c)
-            for (int TZ : tz_c) {
-                const int T = TX * TY * TZ;
-                if (T < 64 || T > 256 || TX > g.Nx - g.P + 1 || TY > g.Ny - g.P + 1 || TZ > g.Nz - g.P + 1) continue;
-                h->tune = TuneChoice{TX, TY, TZ, 0, 0, 0, true};
-                const float ms = time_ms(h, [&] { spread(h, pos); });
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best.TX = TX;
-                    best.TY = TY;
-                    best.TZ = TZ;
+            for (int TZ : tz_c)
+                for (int rows = 0; rows < 2; ++rows) {
+                    const int T = TX * TY * TZ;
+                    if (T < 64 || T > 256 || TX > g.Nx - g.P + 1 || TY > g.Ny - g.P + 1 || TZ > g.Nz - g.P + 1)
+                        continue;
+                    if (!rows && !(TX % 2 == 0 && TY % 4 == 0 && TZ % 4 == 0 && T == 256)) continue;
+                    h->tune = TuneChoice{TX, TY, TZ, 0, 0, 0, rows, true};
+                    const float ms = time_ms(h, [&] { spread(h, pos); });
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best.TX = TX;
+                        best.TY = TY;
+                        best.TZ = TZ;
+                        best.spread_rows = rows;
+                    }
                 }
-            }
     std::vector<int> bxy, bz;
     for (int d = 8; d <= 32; ++d)
         if (g.Nz % d == 0) bxy.push_back(d);
@@ -1433,7 +1540,7 @@ static int autotune(fsd_handle* h, const float4* pos) {
     best_ms = 1e30f;
     for (int a : bxy)
         for (int b : bz) {
-            h->tune = TuneChoice{best.TX, best.TY, best.TZ, a, b, 0, true};
+            h->tune = TuneChoice{best.TX, best.TY, best.TZ, a, b, 0, best.spread_rows, true};
             const float ms = time_ms(h, [&] {
                 fft3d(h, false, 6);
                 fft3d(h, true, 6);
