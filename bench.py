@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--config5-phis", type=float, nargs="+", default=[0.45, 0.5, 0.55])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core timing (profiling runs)")
+    ap.add_argument("--case", choices=["mobility", "poly_apply", "gmres_apply", "precond_build"], default=None,
+                    help="one operator on the benchmarked suspension, --steps times after one untimed call "
+                         "(the small cases the kernel profiles are captured on; prints its own JSON line)")
     return ap.parse_args()
 
 
@@ -669,10 +672,62 @@ def run_config5(args, local):
             "results": results}
 
 
+def run_case(args, local):
+    """One operator of the path on the benchmarked suspension (N, phi, seed 1):
+    the mobility (wave + real space), one application of the learned inner
+    polynomial (k = --poly, fixed interval 0.05) or of the inner-GMRES form
+    (--inner steps), or one build of the learned preconditioner with the
+    shipped network; CUDA-event time per call."""
+    import torch
+
+    from fsd_b200.configs import suspension
+    from fsd_b200.core import FSD
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N = args.N
+    pos, L = suspension(N, args.phi, seed=1)
+    p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
+    kw = {}
+    if args.case == "poly_apply":
+        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly, poly_interval=0.05)
+    elif args.case == "gmres_apply":
+        kw = dict(precond="learned", learned_inner=args.inner)
+    elif args.case == "precond_build":
+        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly)
+    s = FSD(N, (L, L, L, 0.0), device=dev, **kw)
+    if args.case == "precond_build" and poly_weights(args.poly).exists():
+        s.learned_set_weights(np.fromfile(poly_weights(args.poly), "<f4"))
+    s.build_neighbor_list(p)
+    rng = np.random.default_rng(0)
+    if args.case == "mobility":
+        x = torch.as_tensor(rng.standard_normal(11 * N), dtype=torch.float32, device=dev)
+        op = lambda: s.mobility(p, x)  # noqa: E731
+    elif args.case in ("poly_apply", "gmres_apply"):
+        s.precond_build(p)
+        x = torch.as_tensor(rng.standard_normal(17 * N), dtype=torch.float32, device=dev)
+        op = lambda: s.precond_apply(x)  # noqa: E731
+    else:
+        op = lambda: s.precond_build(p)  # noqa: E731
+    op()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        op()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / max(1, args.steps)
+    s.close()
+    return {"case": args.case, "N": N, "phi": args.phi, "calls": args.steps, "us_per_call": 1e3 * ms}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
-    if args.impl == "reference":
+    if args.case:
+        out = run_case(args, local) if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, ws, rank)
     elif args.config5:
         out = run_config5(args, local) if rank == 0 else None

@@ -3,14 +3,18 @@
 // memory by the Tensor Memory Accelerator.
 //
 // The approximate inverse G (54 MB at N = 32768, phi = 0.4) and the pruned
-// lubrication matrix A are read once per product.  One CTA takes a tile of
-// consecutive rows whose blocks (at most kTileBlocks) lie contiguously in
-// memory; one thread issues a bulk copy (cp.async.bulk, completing on an
-// mbarrier) of the tile's blocks and column indices into shared memory, so
-// the matrix streams at copy-engine rate while the eight-lane row groups
-// gather the vector operand from L2.  Three CTAs fit on an SM, so one CTA's
-// copy overlaps the others' arithmetic.  Tiles are cut on the host once per
-// preconditioner build.
+// lubrication matrix A are read once per product.  One CTA of 128 threads
+// takes a tile of consecutive rows whose blocks (at most kTileBlocks) lie
+// contiguously in memory; one thread issues a bulk copy (cp.async.bulk,
+// completing on an mbarrier) of the tile's blocks into shared memory, and
+// while it is in flight the threads gather the tile's row pointers and the
+// operand's 6-vectors for its column indices into shared memory (every load
+// issued before any is waited on).  The rows are then multiplied from shared
+// memory alone, eight lanes per row.  Tiles are small so that many CTAs (up
+// to ten) share an SM: the kernel is bound by the chain of L2 round trips
+// per tile, which the resident tiles overlap.  The copies carry an L2
+// evict-last policy, so G and A stay in L2 across the 2k - 1 products of one
+// application.  Tiles are cut on the host once per preconditioner build.
 //
 // The mbarrier wait is bounded: when it runs out the CTA records an error
 // (read by the host after the solve), waits once more (also bounded) for its
@@ -51,11 +55,17 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t phase) {
     return false;
 }
 
+// Bulk copy global -> this CTA's shared memory, completing on bar, with an L2
+// policy: the matrices of the inner polynomial (G and A, about 75 MB at
+// N = 32768, phi = 0.4) are read 2k - 1 times per application, back to back,
+// and fit in the 126 MB L2 together, so their lines are marked evict-last.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    uint64_t policy;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(policy));
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
             smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
         : "memory");
 }
 
@@ -78,61 +88,98 @@ __device__ __forceinline__ float row6(const float* blk, int rr, float xj, unsign
 // product out = M x; 2 = last product y = G v with the saddle post step into
 // xs; 3 = Clenshaw step out = c_m T + f ((2/lambda) A u - B1) - B2.
 template <int MODE>
-__global__ void __launch_bounds__(256, 3) k_bsr_tma(BsrTmaArgs a) {
+__global__ void __launch_bounds__(kBsrThreads, 8) k_bsr_tma(BsrTmaArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
+    __shared__ int sR[kTileBlocks + 1];  // the tile's row pointers, relative to its first block
     float* sG = reinterpret_cast<float*>(sm);
-    int* sC = reinterpret_cast<int*>(sm + (size_t)kTileBlocks * 144);
+    float* sX = reinterpret_cast<float*>(sm + (size_t)kTileBlocks * 144);
     const int t = blockIdx.x;
     if (t >= *a.ntiles) return;  // the launch covers the tile capacity
     const int r0 = a.tile_row[t], r1 = a.tile_row[t + 1];
     const int e0 = a.rowptr[r0], e1 = a.rowptr[r1];
-    const int ce0 = e0 & ~3, ce1 = (e1 + 3) & ~3;  // 16-byte aligned copy of the column indices
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const uint32_t gbytes = (uint32_t)(e1 - e0) * 144u, cbytes = (uint32_t)(ce1 - ce0) * 4u;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
-                     "r"(gbytes + cbytes)
+        const uint32_t gbytes = (uint32_t)(e1 - e0) * 144u;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)), "r"(gbytes)
                      : "memory");
         if (gbytes) bulk_load(sG, a.val + (size_t)e0 * 36, gbytes, &bar);
-        if (cbytes) bulk_load(sC, a.col + ce0, cbytes, &bar);
     }
-    if (!bar_wait(&bar, 0)) {
+    const int N = a.N;
+    const size_t offU = 11 * (size_t)N;
+    // Row pointers and operand 6-vectors of the tile's columns: each thread
+    // takes whole blocks, issuing every load before it waits on any.  MODE 0
+    // reads the caller's saddle vector (only 4-byte alignment assumed: scalar
+    // loads); the other modes read the handle's own 6N-float slots, which are
+    // 8-byte aligned (float2 loads).
+    {
+        constexpr int kGather = (kTileBlocks + kBsrThreads - 1) / kBsrThreads;
+        int rp[kGather], cj[kGather];
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            const int q = threadIdx.x + kBsrThreads * k;
+            rp[k] = q <= r1 - r0 ? a.rowptr[r0 + q] : 0;
+            cj[k] = q < e1 - e0 ? a.col[e0 + q] : -1;
+        }
+        float2 xv[kGather][3];
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            if (cj[k] < 0) continue;
+            if (MODE == 0) {
+                const float* x1 = a.x + 6 * (size_t)cj[k];
+                const float* u1 = x1 + offU;
+                xv[k][0] = make_float2(x1[0] - u1[0], x1[1] - u1[1]);
+                xv[k][1] = make_float2(x1[2] - u1[2], x1[3] - u1[3]);
+                xv[k][2] = make_float2(x1[4] - u1[4], x1[5] - u1[5]);
+            } else {
+                const float2* x2 = reinterpret_cast<const float2*>(a.x + 6 * (size_t)cj[k]);
+                xv[k][0] = x2[0];
+                xv[k][1] = x2[1];
+                xv[k][2] = x2[2];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kGather; ++k) {
+            const int q = threadIdx.x + kBsrThreads * k;
+            if (q <= r1 - r0) sR[q] = rp[k] - e0;
+            if (cj[k] < 0) continue;
+            float2* d2 = reinterpret_cast<float2*>(sX + 6 * (size_t)q);
+            d2[0] = xv[k][0];
+            d2[1] = xv[k][1];
+            d2[2] = xv[k][2];
+        }
+    }
+    const bool ok = bar_wait(&bar, 0);
+    __syncthreads();  // sX and sR complete
+    if (!ok) {
         if (threadIdx.x == 0) atomicExch(&g_bsr_error, 1);
         bar_wait(&bar, 0);  // the copy may still land in this CTA's shared memory
         return;
     }
     const int lane8 = threadIdx.x & 7;
     const int group = threadIdx.x >> 3;
-    const unsigned gmask = 0xffu << (threadIdx.x & 24);
     const int rr = lane8 < 6 ? lane8 : 0;
-    const int N = a.N;
-    const size_t offU = 11 * (size_t)N;
-    auto ld = [&](int j) -> float {
-        if (lane8 >= 6) return 0.f;
-        if (MODE == 0) return a.x[6 * (size_t)j + lane8] - a.x[offU + 6 * (size_t)j + lane8];
-        return a.x[6 * (size_t)j + lane8];
-    };
-    // whole groups of eight take rows; a group's lanes stay together
-    for (int r = r0 + group; r < r1; r += (int)(blockDim.x >> 3)) {
-        const int qb = a.rowptr[r] - e0, qe = a.rowptr[r + 1] - e0;
-        const int* cc = sC + (e0 - ce0);
+    // whole groups of eight take rows; lanes 0-5 each produce one row of the 6-vector
+    for (int rl = group; rl < r1 - r0; rl += kBsrThreads / 8) {
+        const int r = r0 + rl;
+        const int qb = sR[rl], qe = sR[rl + 1];
         float acc = 0.f;
-        int q = qb;
-        for (; q + 3 < qe; q += 4) {
-            const int j0 = cc[q], j1 = cc[q + 1], j2 = cc[q + 2], j3 = cc[q + 3];
-            const float x0 = ld(j0), x1 = ld(j1), x2 = ld(j2), x3 = ld(j3);
-            const float* gq = sG + (size_t)q * 36;
-            acc += row6(gq, rr, x0, gmask);
-            acc += row6(gq + 36, rr, x1, gmask);
-            acc += row6(gq + 72, rr, x2, gmask);
-            acc += row6(gq + 108, rr, x3, gmask);
+        for (int q = qb; q < qe; ++q) {
+            const float2* g2 = reinterpret_cast<const float2*>(sG + (size_t)q * 36 + rr * 6);
+            const float2* x2 = reinterpret_cast<const float2*>(sX + (size_t)q * 6);
+            const float2 g01 = g2[0], g23 = g2[1], g45 = g2[2];
+            const float2 x01 = x2[0], x23 = x2[1], x45 = x2[2];
+            acc = fmaf(g01.x, x01.x, acc);
+            acc = fmaf(g01.y, x01.y, acc);
+            acc = fmaf(g23.x, x23.x, acc);
+            acc = fmaf(g23.y, x23.y, acc);
+            acc = fmaf(g45.x, x45.x, acc);
+            acc = fmaf(g45.y, x45.y, acc);
         }
-        for (; q < qe; ++q) acc += row6(sG + (size_t)q * 36, rr, ld(cc[q]), gmask);
         const size_t i6 = 6 * (size_t)r + lane8;
         if (MODE == 0) {
             if (lane8 < 6) {
@@ -166,7 +213,7 @@ __global__ void __launch_bounds__(256, 3) k_bsr_tma(BsrTmaArgs a) {
     }
 }
 
-size_t bsr_tma_smem() { return (size_t)kTileBlocks * 144 + (size_t)(kTileBlocks + 8) * 4; }
+size_t bsr_tma_smem() { return (size_t)kTileBlocks * (144 + 24); }
 
 // Kernel entry of a mode (for launches and graph-node updates).
 const void* bsr_tma_kernel(int mode) {
@@ -186,10 +233,10 @@ int bsr_tma_prepare() {
 void bsr_tma_launch(int mode, const BsrTmaArgs& a, int grid, cudaStream_t st) {
     const size_t smem = bsr_tma_smem();
     switch (mode) {
-        case 0: k_bsr_tma<0><<<grid, 256, smem, st>>>(a); break;
-        case 1: k_bsr_tma<1><<<grid, 256, smem, st>>>(a); break;
-        case 2: k_bsr_tma<2><<<grid, 256, smem, st>>>(a); break;
-        default: k_bsr_tma<3><<<grid, 256, smem, st>>>(a); break;
+        case 0: k_bsr_tma<0><<<grid, kBsrThreads, smem, st>>>(a); break;
+        case 1: k_bsr_tma<1><<<grid, kBsrThreads, smem, st>>>(a); break;
+        case 2: k_bsr_tma<2><<<grid, kBsrThreads, smem, st>>>(a); break;
+        default: k_bsr_tma<3><<<grid, kBsrThreads, smem, st>>>(a); break;
     }
 }
 

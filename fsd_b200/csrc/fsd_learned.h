@@ -8,7 +8,8 @@
 namespace fsd {
 
 // Block-CSR products with the matrix tile streamed by bulk copies (bsr_tma.cu).
-constexpr int kTileBlocks = 448;  // blocks (and rows) of a tile
+constexpr int kTileBlocks = 104;  // blocks (and rows) of a tile of the block-sparse products
+constexpr int kBsrThreads = 128;  // threads per tile
 struct BsrTmaArgs {
     const int* rowptr;
     const int* col;

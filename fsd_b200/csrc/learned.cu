@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -555,11 +556,13 @@ int precond_build_learned(fsd_handle* h, const float4* pos) {
             s->poly_source = 4;
         } else if (mpnn_loaded(h)) {
             double rho = 0.0;
-            e = mpnn_poly_ratio(h, pos, &rho, nullptr);
+            float log_rho = 0.f;
+            e = mpnn_poly_ratio(h, pos, &rho, &log_rho);
             if (e != FSD_OK) return e;
-            e = poly_set_interval(h, rho);
+            const bool finite = std::isfinite(log_rho);  // else the fixed interval (or 0.05)
+            e = poly_set_interval(h, finite ? rho : (h->p.poly_interval > 0.f ? h->p.poly_interval : 0.05));
             if (e != FSD_OK) return e;
-            s->poly_source = 1;
+            s->poly_source = finite ? 1 : 4;
         } else if (h->p.poly_interval > 0.f) {
             e = poly_set_interval(h, h->p.poly_interval);
             if (e != FSD_OK) return e;

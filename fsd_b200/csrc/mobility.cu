@@ -1153,16 +1153,35 @@ __global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
 // Mobility.cu:503-841).  Output per particle, 11 floats: u then the velocity
 // gradient in the reference's transposed storage
 // {XX, YX, ZX, ZY, YY, XY, XZ, YZ}.
-__global__ void __launch_bounds__(256) k_contract(const float4* __restrict__ pos, const float2* __restrict__ grid, int N,
-                                                  Box b, int Nx, int Ny, int Nz, int P, float hx, float hy, float hz,
-                                                  float prefac, float expfac, float* __restrict__ out) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// Warps take particles in the cell-list order (a permutation of 0..N-1), so
+// the warps of a block read overlapping stencils through L1.  KP > 0 fixes the
+// stencil width at compile time (the node index arithmetic then divides by a
+// constant); KP = 0 reads it at run time.  With `local` (the stencil spans
+// well under half the box) each node's separation is the stencil origin's
+// minimum image plus the node's fixed offset in the sheared grid.
+template <int KP>
+__global__ void __launch_bounds__(256) k_contract(const float4* __restrict__ pos, const unsigned* __restrict__ order,
+                                                  const float2* __restrict__ grid, int N, Box b, int Nx, int Ny,
+                                                  int Nz, int Prun, float hx, float hy, float hz, float prefac,
+                                                  float expfac, bool local, float* __restrict__ out) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (i >= N) return;
+    if (w >= N) return;
+    const int P = KP > 0 ? KP : Prun;
+    const int i = (int)order[w];
     const float4 p = pos[i];
     const int3 s = stencil_origin(p, b, Nx, Ny, Nz, P, nullptr);
     const size_t G = (size_t)Nx * Ny * Nz;
     const float Ld2x = b.Lx / 2.0f, Ld2y = b.Ly / 2.0f, Ld2z = b.Lz / 2.0f;
+    float3 r0;  // stencil origin node minus the particle, minimum image
+    {
+        float3 pg;
+        pg.x = hx * s.x - Ld2x;
+        pg.y = hy * s.y - Ld2y;
+        pg.z = hz * s.z - Ld2z;
+        pg.x = pg.x + b.xy * pg.y;
+        r0 = min_image(make_float3(pg.x - p.x, pg.y - p.y, pg.z - p.z), b);
+    }
     float acc[11];
 #pragma unroll
     for (int c = 0; c < 11; ++c) acc[c] = 0.0f;
@@ -1173,12 +1192,17 @@ __global__ void __launch_bounds__(256) k_contract(const float4* __restrict__ pos
         ix -= (ix >= Nx) ? Nx : 0;
         iy -= (iy >= Ny) ? Ny : 0;
         iz -= (iz >= Nz) ? Nz : 0;
-        float3 pg;
-        pg.x = hx * ix - Ld2x;
-        pg.y = hy * iy - Ld2y;
-        pg.z = hz * iz - Ld2z;
-        pg.x = pg.x + b.xy * pg.y;
-        const float3 r = min_image(make_float3(pg.x - p.x, pg.y - p.y, pg.z - p.z), b);
+        float3 r;
+        if (local) {
+            r = make_float3(r0.x + (hx * tx + b.xy * (hy * ty)), r0.y + hy * ty, r0.z + hz * tz);
+        } else {
+            float3 pg;
+            pg.x = hx * ix - Ld2x;
+            pg.y = hy * iy - Ld2y;
+            pg.z = hz * iz - Ld2z;
+            pg.x = pg.x + b.xy * pg.y;
+            r = min_image(make_float3(pg.x - p.x, pg.y - p.y, pg.z - p.z), b);
+        }
         const float rsq = r.x * r.x + r.y * r.y + r.z * r.z;
         const float wgt = prefac * expf(-expfac * rsq);
         const size_t g = ((size_t)ix * Ny + iy) * Nz + iz;
@@ -1422,9 +1446,19 @@ static void contract(fsd_handle* h, const float4* pos) {
     const float expfac = 2.0 * xisq / g.eta;
     const float quadW = g.hx * g.hy * g.hz;
     const int N = h->p.N;
+    // node separations from the stencil origin reach (P - 1) cells per axis
+    // plus the tilt's x shift; below half the box they are their own minimum image
+    const float tilt = 1.0f + fabsf(h->box.xy);
+    const bool local = (g.P + 1) * tilt < 0.5f * g.Nx && (g.P + 1) * tilt < 0.5f * g.Ny &&
+                       (g.P + 1) * tilt < 0.5f * g.Nz;
+    const unsigned grid = (unsigned)(((size_t)N * 32 + 255) / 256);
     count_launch();
-    k_contract<<<(N * 32 + 255) / 256, 256, 0, h->stream>>>(pos, h->w.grid, N, h->box, g.Nx, g.Ny, g.Nz, g.P, g.hx,
-                                                            g.hy, g.hz, quadW * prefac, expfac, h->w.uwave);
+    if (g.P == 6)
+        k_contract<6><<<grid, 256, 0, h->stream>>>(pos, h->w.order, h->w.grid, N, h->box, g.Nx, g.Ny, g.Nz, g.P, g.hx,
+                                                   g.hy, g.hz, quadW * prefac, expfac, local, h->w.uwave);
+    else
+        k_contract<0><<<grid, 256, 0, h->stream>>>(pos, h->w.order, h->w.grid, N, h->box, g.Nx, g.Ny, g.Nz, g.P, g.hx,
+                                                   g.hy, g.hz, quadW * prefac, expfac, local, h->w.uwave);
 }
 
 void mobility_wave_from_spectrum(fsd_handle* h, const float4* pos) {

@@ -1474,6 +1474,11 @@ int mpnn_ratio_train_step(fsd_handle* h, const float4* pos, float target_log_rho
     float s0 = 0.f;
     MP_TRY(mpnn_poly_ratio(h, pos, &rho, &s0));
     const double d = (double)s0 - (double)target_log_rho;
+    if (!std::isfinite(d)) {  // e.g. overlapping particles: no gradient, no update
+        if (loss) *loss = (float)d;
+        if (pred_log_rho) *pred_log_rho = s0;
+        return FSD_ERR_BREAKDOWN;
+    }
     MP_TRY(mp_alloc_backward(h));
     PolyGrad pg{};
     pg.g[0] = (float)(2.0 * d / s->N);  // d(d^2)/d s0, spread over the particles' outputs

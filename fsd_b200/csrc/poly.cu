@@ -228,7 +228,7 @@ int poly_prepare_products(fsd_handle* h) {
     e = bsr_make_tiles(arow, N, at);
     if (e != FSD_OK) return e;
     if (!s->g_tiles) {
-        s->tile_cap = N / 13 + 2;  // a full tile holds >= 13 rows (>= 417 of at most 448 blocks, rows <= 32)
+        s->tile_cap = N / 3 + 2;  // a full tile holds >= 3 rows (> 72 of at most 104 blocks, rows <= 32)
         FSD_CHECK_CUDA(cudaMalloc(&s->g_tiles, sizeof(int) * (s->tile_cap + 2)));
         FSD_CHECK_CUDA(cudaMalloc(&s->a_tiles, sizeof(int) * (s->tile_cap + 2)));
         e = bsr_tma_prepare();
@@ -405,7 +405,7 @@ static int poly_bind(fsd_handle* h, const float* b, float* x) {
     void* largs[] = {&la};
     cudaKernelNodeParams kp = {};
     kp.gridDim = dim3(s->tile_cap);
-    kp.blockDim = dim3(256);
+    kp.blockDim = dim3(kBsrThreads);
     kp.sharedMemBytes = (unsigned)bsr_tma_smem();
     kp.func = (void*)bsr_tma_kernel(0);
     kp.kernelParams = fargs;

@@ -24,14 +24,16 @@
 namespace fsd {
 
 namespace {
-constexpr int kBuckets = 3;
-constexpr int kBucketMax[kBuckets] = {12, 20, kSpaiCap};
-__host__ __device__ constexpr int bucket_of(int n) { return n <= 12 ? 0 : (n <= 20 ? 1 : 2); }
-constexpr int kSpaiThreads = 128;
+// Buckets of set sizes (particles per two-hop set), so that each launch sizes
+// its shared memory for its largest set; the larger sets get 256 threads.
+constexpr int kBuckets = 6;
+constexpr int kBucketMax[kBuckets] = {12, 16, 20, 24, 28, kSpaiCap};
+__host__ __device__ constexpr int bucket_of(int n) { return n <= 12 ? 0 : (n <= 28 ? (n - 9) / 4 : 5); }
+constexpr int bucket_threads(int b) { return kBucketMax[b] > 16 ? 256 : 128; }
 
-inline size_t spai_smem(int m) {  // packed FP64 lower triangle + 6 right-hand sides + the set
+inline size_t spai_smem(int m) {  // packed FP64 lower triangle + 6 right-hand sides + inverse pivots + the set
     const size_t n = 6 * (size_t)m;
-    return sizeof(double) * (n * (n + 1) / 2 + 6 * n) + sizeof(int) * kSpaiCap;
+    return sizeof(double) * (n * (n + 1) / 2 + 7 * n) + sizeof(int) * kSpaiCap;
 }
 }  // namespace
 
@@ -87,7 +89,8 @@ __device__ __forceinline__ const float* a_block(const unsigned* pn, const unsign
     return nullptr;
 }
 
-__global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* __restrict__ pn,
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_spai_solve(const unsigned* __restrict__ pn,
                                                              const unsigned* __restrict__ plist,
                                                              const float* __restrict__ A,
                                                              const int* __restrict__ sets,
@@ -103,7 +106,8 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
     const int n = 6 * m;
     double* H = sm;                               // packed lower triangle, n(n+1)/2
     double* R = sm + (size_t)n * (n + 1) / 2;     // n x 6, row-major
-    int* S = (int*)(R + 6 * (size_t)n);
+    double* dinv = R + 6 * (size_t)n;             // 1 / L_jj
+    int* S = (int*)(dinv + n);
     for (int a = threadIdx.x; a < m; a += blockDim.x) S[a] = sets[(size_t)c * kSpaiCap + a];
     __syncthreads();
     // Normal matrix: H[a][b] = sum_k A_{s_a k} A_{s_b k}^T over k in both pruned lists (b <= a).
@@ -117,25 +121,33 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
         const unsigned* ra = plist + (size_t)sa * kPrunedCap;
         const unsigned* rb = plist + (size_t)sb * kPrunedCap;
         const unsigned na = pn[sa], nb = pn[sb];
-        // one row of the 6x6 block at a time keeps the FP64 accumulators in registers
-        for (int r = 0; r < 6; ++r) {
-            double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        // three rows of the 6x6 block per pass (18 FP64 accumulators in registers)
+        for (int r0 = 0; r0 < 6; r0 += 3) {
+            double acc[3][6];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) acc[r][q] = 0.0;
             unsigned ia = 0, ib = 0;
             while (ia < na && ib < nb) {
                 const unsigned ka = ra[ia], kb = rb[ib];
                 if (ka == kb) {
-                    const float* Pa = A + ((size_t)sa * kPrunedCap + ia) * 36 + r * 6;
+                    const float* Pa = A + ((size_t)sa * kPrunedCap + ia) * 36 + r0 * 6;
                     const float* Pb = A + ((size_t)sb * kPrunedCap + ib) * 36;
-                    double pa[6];
+                    float pa[18], pb[36];
 #pragma unroll
-                    for (int u = 0; u < 6; ++u) pa[u] = (double)Pa[u];
+                    for (int u = 0; u < 18; ++u) pa[u] = Pa[u];
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) {
-                        double v = 0.0;
+                    for (int u = 0; u < 36; ++u) pb[u] = Pb[u];
 #pragma unroll
-                        for (int u = 0; u < 6; ++u) v += pa[u] * (double)Pb[q * 6 + u];
-                        acc[q] += v;
-                    }
+                    for (int r = 0; r < 3; ++r)
+#pragma unroll
+                        for (int q = 0; q < 6; ++q) {
+                            double v = 0.0;
+#pragma unroll
+                            for (int u = 0; u < 6; ++u) v += (double)pa[r * 6 + u] * (double)pb[q * 6 + u];
+                            acc[r][q] += v;
+                        }
                     ++ia;
                     ++ib;
                 } else if (ka < kb) {
@@ -144,11 +156,14 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
                     ++ib;
                 }
             }
-            const int i = 6 * a + r;
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const int j = 6 * b + q;
-                if (i >= j) H[tri(i, j)] = acc[q];
+            for (int r = 0; r < 3; ++r) {
+                const int i = 6 * a + r0 + r;
+#pragma unroll
+                for (int q = 0; q < 6; ++q) {
+                    const int j = 6 * b + q;
+                    if (i >= j) H[tri(i, j)] = acc[r][q];
+                }
             }
         }
     }
@@ -159,13 +174,15 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
     }
     __syncthreads();
     // Right-looking block Cholesky on the 6x6 blocks of the particles, in
-    // place, with the forward substitution L y = R carried along: per block
-    // column, one thread factors the diagonal block, the rows below take
-    // their panel entries (one row per thread), then the trailing rows and
-    // right-hand sides are updated (one row per thread).  Three barriers per
-    // block column instead of three per scalar column.
+    // place, with the forward substitution L y = R carried along.  Per block
+    // column: one thread factors the diagonal block (keeping 1 / L_jj, so
+    // the rest multiplies instead of dividing), the rows below take their
+    // panel entries (one row per thread) while six threads solve the block's
+    // right-hand sides, then the trailing lower triangle and right-hand sides
+    // are updated with the work spread evenly over the threads (one entry,
+    // or one right-hand-side row, per item).  Three barriers per block column.
     __shared__ int bad;
-    __shared__ double bsum[kSpaiThreads];
+    __shared__ double bsum[THREADS];
     if (threadIdx.x == 0) bad = 0;
     __syncthreads();
     for (int jb = 0; jb < m; ++jb) {
@@ -178,12 +195,13 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
                     bad = 1;
                     d = 1.0;
                 }
-                d = sqrt(d);
-                H[tri(j, j)] = d;
+                const double inv = rsqrt(d);
+                H[tri(j, j)] = d * inv;
+                dinv[j] = inv;
                 for (int i = j + 1; i < j0 + 6; ++i) {
                     double v = H[tri(i, j)];
                     for (int q = j0; q < j; ++q) v -= H[tri(i, q)] * H[tri(j, q)];
-                    H[tri(i, j)] = v / d;
+                    H[tri(i, j)] = v * inv;
                 }
             }
         }
@@ -195,7 +213,7 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
             for (int q = 0; q < 6; ++q) {
                 double v = H[tri(i, j0 + q)];
                 for (int p2 = 0; p2 < q; ++p2) v -= l[p2] * H[tri(j0 + q, j0 + p2)];
-                l[q] = v / H[tri(j0 + q, j0 + q)];
+                l[q] = v * dinv[j0 + q];
             }
 #pragma unroll
             for (int q = 0; q < 6; ++q) H[tri(i, j0 + q)] = l[q];
@@ -206,47 +224,60 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
             for (int q = 0; q < 6; ++q) {
                 double v = R[(size_t)(j0 + q) * 6 + c];
                 for (int p2 = 0; p2 < q; ++p2) v -= H[tri(j0 + q, j0 + p2)] * R[(size_t)(j0 + p2) * 6 + c];
-                R[(size_t)(j0 + q) * 6 + c] = v / H[tri(j0 + q, j0 + q)];
+                R[(size_t)(j0 + q) * 6 + c] = v * dinv[j0 + q];
             }
         }
         __syncthreads();
-        // trailing update of rows i >= j0 + 6 and their right-hand sides
-        for (int i = j0 + 6 + threadIdx.x; i < n; i += blockDim.x) {
-            double li[6];
+        // trailing update: items [0, T(T+1)/2) are the entries (i, k), k <= i,
+        // of the trailing lower triangle (i = j0 + 6 + i', k = j0 + 6 + k');
+        // items [T(T+1)/2, T(T+1)/2 + T) are its right-hand-side rows
+        const int T = n - j0 - 6;
+        const int ntri = T * (T + 1) / 2;
+        for (int t = threadIdx.x; t < ntri + T; t += blockDim.x) {
+            if (t < ntri) {
+                int ip = (int)((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
+                while ((ip + 1) * (ip + 2) / 2 <= t) ++ip;
+                while (ip * (ip + 1) / 2 > t) --ip;
+                const int kp = t - ip * (ip + 1) / 2;
+                const double* li = H + tri(j0 + 6 + ip, j0);
+                const double* lk = H + tri(j0 + 6 + kp, j0);
+                H[tri(j0 + 6 + ip, j0 + 6 + kp)] -= li[0] * lk[0] + li[1] * lk[1] + li[2] * lk[2] + li[3] * lk[3] +
+                                                    li[4] * lk[4] + li[5] * lk[5];
+            } else {
+                const int i = j0 + 6 + (t - ntri);
+                const double* li = H + tri(i, j0);
 #pragma unroll
-            for (int q = 0; q < 6; ++q) li[q] = H[tri(i, j0 + q)];
-            for (int k = j0 + 6; k <= i; ++k) {
-                const double* lk = H + tri(k, j0);
-                H[tri(i, k)] -= li[0] * lk[0] + li[1] * lk[1] + li[2] * lk[2] + li[3] * lk[3] + li[4] * lk[4] +
-                                li[5] * lk[5];
-            }
+                for (int c = 0; c < 6; ++c) {
+                    double v = 0.0;
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                double v = 0.0;
-#pragma unroll
-                for (int q = 0; q < 6; ++q) v += li[q] * R[(size_t)(j0 + q) * 6 + c];
-                R[(size_t)i * 6 + c] -= v;
+                    for (int q = 0; q < 6; ++q) v += li[q] * R[(size_t)(j0 + q) * 6 + c];
+                    R[(size_t)i * 6 + c] -= v;
+                }
             }
         }
         __syncthreads();
     }
     // Backward substitution L^T x = y by blocks: the coupling of block jb to
     // the solved blocks below is summed by all threads ((q, c) pairs times
-    // four row ranges), then the 6x6 triangular solve (one column per thread).
+    // kParts row ranges), then the 6x6 triangular solve (one column per thread).
+    constexpr int kParts = THREADS / 36;  // 3 with 128 threads, 7 with 256
     for (int jb = m - 1; jb >= 0; --jb) {
         const int j0 = 6 * jb;
         const int t = threadIdx.x;
-        const int pc = t % 36, part = t / 36;  // parts 0..2 with 128 threads (t >= 108 idle)
+        const int pc = t % 36, part = t / 36;
         double v = 0.0;
-        if (part < 3) {
+        if (part < kParts) {
             const int q = pc / 6, c = pc % 6;
-            for (int i = j0 + 6 + part; i < n; i += 3) v += H[tri(i, j0 + q)] * R[(size_t)i * 6 + c];
+            for (int i = j0 + 6 + part; i < n; i += kParts) v += H[tri(i, j0 + q)] * R[(size_t)i * 6 + c];
         }
         bsum[t] = v;
         __syncthreads();
         if (t < 36) {
             const int q = t / 6, c = t % 6;
-            R[(size_t)(j0 + q) * 6 + c] -= bsum[t] + bsum[t + 36] + bsum[t + 72];
+            double sum = 0.0;
+#pragma unroll
+            for (int k = 0; k < kParts; ++k) sum += bsum[t + 36 * k];
+            R[(size_t)(j0 + q) * 6 + c] -= sum;
         }
         __syncthreads();
         if (t < 6) {
@@ -254,7 +285,7 @@ __global__ void __launch_bounds__(kSpaiThreads, 4) k_spai_solve(const unsigned* 
             for (int q = 5; q >= 0; --q) {
                 double w = R[(size_t)(j0 + q) * 6 + c];
                 for (int p2 = q + 1; p2 < 6; ++p2) w -= H[tri(j0 + p2, j0 + q)] * R[(size_t)(j0 + p2) * 6 + c];
-                R[(size_t)(j0 + q) * 6 + c] = w / H[tri(j0 + q, j0 + q)];
+                R[(size_t)(j0 + q) * 6 + c] = w * dinv[j0 + q];
             }
         }
         __syncthreads();
@@ -318,8 +349,9 @@ int spai_build(fsd_handle* h) {
         FSD_CHECK_CUDA(cudaMalloc(&s->sp_scan, sizeof(unsigned) * scan_scratch_elems(N)));
         FSD_CHECK_CUDA(cudaMalloc(&s->sp_bucket, sizeof(int) * (size_t)kBuckets * N));
         FSD_CHECK_CUDA(cudaMalloc(&s->sp_cnt, sizeof(unsigned) * (kBuckets + 2)));
-        FSD_CHECK_CUDA(cudaMallocHost(&s->sp_host, sizeof(unsigned) * 4));
-        FSD_CHECK_CUDA(ensure_smem_limit((const void*)k_spai_solve, spai_smem(kBucketMax[kBuckets - 1])));
+        FSD_CHECK_CUDA(cudaMallocHost(&s->sp_host, sizeof(unsigned) * (kBuckets + 2)));
+        FSD_CHECK_CUDA(ensure_smem_limit((const void*)k_spai_solve<128>, spai_smem(16)));
+        FSD_CHECK_CUDA(ensure_smem_limit((const void*)k_spai_solve<256>, spai_smem(kSpaiCap)));
     }
     // counters: buckets [0, kBuckets), then truncated sets, then failed rows
     FSD_CHECK_CUDA(cudaMemsetAsync(s->sp_cnt, 0, sizeof(unsigned) * (kBuckets + 2), st));
@@ -329,11 +361,13 @@ int spai_build(fsd_handle* h) {
     k_spai_sets<<<(N + 127) / 128, 128, 0, st>>>(s->a_pn, s->a_plist, N, s->sp_sets, s->sp_size, s->sp_cnt,
                                                  s->sp_bucket, truncated);
     exclusive_scan(s->sp_size, s->sp_rowptr, N, s->sp_scan, st);
+    // block count, truncated sets and the bucket sizes (the launches below are sized by them)
     FSD_CHECK_CUDA(cudaMemcpyAsync(s->sp_host, s->sp_rowptr + N, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    FSD_CHECK_CUDA(cudaMemcpyAsync(s->sp_host + 1, truncated, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(s->sp_host + 1, s->sp_cnt, sizeof(unsigned) * (kBuckets + 1),
+                                   cudaMemcpyDeviceToHost, st));
     FSD_CHECK_CUDA(cudaStreamSynchronize(st));
     const int nnzb = (int)s->sp_host[0];
-    s->sp_truncated = (int)s->sp_host[1];
+    s->sp_truncated = (int)s->sp_host[1 + kBuckets];
     int e = learned_reserve(h, nnzb);
     if (e != FSD_OK) return e;
     FSD_CHECK_CUDA(cudaMemcpyAsync(s->g_rowptr, s->sp_rowptr, sizeof(int) * (N + 1), cudaMemcpyDeviceToDevice, st));
@@ -341,10 +375,17 @@ int spai_build(fsd_handle* h) {
     count_launch();
     k_spai_cols<<<(N + 127) / 128, 128, 0, st>>>(s->sp_sets, s->sp_size, s->g_rowptr, N, s->g_col);
     for (int b = 0; b < kBuckets; ++b) {
+        const unsigned cnt = s->sp_host[1 + b];
+        if (cnt == 0) continue;
         count_launch();
-        k_spai_solve<<<N, kSpaiThreads, spai_smem(kBucketMax[b]), st>>>(
-            s->a_pn, s->a_plist, s->a_blocks, s->sp_sets, s->sp_size, s->sp_cnt, s->sp_bucket, b, N, s->g_rowptr,
-            s->g_col, s->g_val, fail);
+        if (bucket_threads(b) == 128)
+            k_spai_solve<128><<<cnt, 128, spai_smem(kBucketMax[b]), st>>>(
+                s->a_pn, s->a_plist, s->a_blocks, s->sp_sets, s->sp_size, s->sp_cnt, s->sp_bucket, b, N,
+                s->g_rowptr, s->g_col, s->g_val, fail);
+        else
+            k_spai_solve<256><<<cnt, 256, spai_smem(kBucketMax[b]), st>>>(
+                s->a_pn, s->a_plist, s->a_blocks, s->sp_sets, s->sp_size, s->sp_cnt, s->sp_bucket, b, N,
+                s->g_rowptr, s->g_col, s->g_val, fail);
     }
     FSD_CHECK_CUDA(cudaGetLastError());
     s->g_nnzb = nnzb;

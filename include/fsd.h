@@ -340,7 +340,9 @@ int fsd_learned_interval_coefficients(float rho, float lambda, int k, float* hos
  * neighbour list current for d_pos): the squared error between the predicted
  * log rho and target_log_ratio (the ratio that gave the fewest outer
  * iterations), the prediction, the weight gradient (host_grad, optional,
- * fsd_learned_num_weights() floats) and, when lr > 0, one Adam step. */
+ * fsd_learned_num_weights() floats) and, when lr > 0, one Adam step.
+ * FSD_ERR_BREAKDOWN (weights untouched) when the prediction is not finite,
+ * as for overlapping particles. */
 int fsd_learned_ratio_train_step(fsd_handle* h, const float* d_pos, float target_log_ratio, float lr, float* loss,
                                  float* predicted_log_ratio, float* host_grad);
 int fsd_learned_get_poly(fsd_handle* h, float* host_c, int n);

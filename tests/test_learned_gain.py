@@ -1,0 +1,84 @@
+"""What the trained network gains, on held-out dense suspensions.
+
+N = 32768 unit spheres at phi = 0.45, 0.5 and 0.55 (seeds 2000 + 100 phi,
+which neither the training trajectories nor the benchmark use).  The same
+saddle system A(x) y = (0; -psi) -- the right-hand side of the random finite
+difference solves (Integrator.cu:549-718), two of the three solves of a
+Brownian step -- is solved to 1e-4 with the two-hop approximate inverse
+preconditioner in two forms:
+
+* six inner GMRES steps on G (flexible outer GMRES), no network;
+* the inner Chebyshev polynomial y = G q(AG) t of degree nine whose interval
+  [rho lambda, lambda] is predicted per configuration by the trained
+  message-passing network (fsd_b200/data/learned_poly_k10.f32) -- the
+  learned form.
+
+The learned form must take fewer outer iterations and less device time for
+the preconditioner build plus the solve (second run of each, after graphs are
+captured), and its solution must satisfy the FP64 oracle's saddle system to
+1.1e-4 (the solver's FP32 residual target 1e-4 plus the FP32 operator's
+rounding against FP64).
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import ewald_golden
+from fsd_b200.configs import suspension
+from fsd_b200.core import FSD
+from oracle import fsd_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N = 32768
+WEIGHTS = Path(__file__).resolve().parents[1] / "fsd_b200" / "data" / "learned_poly_k10.f32"
+
+
+def _solve(pos, Lc, rhs, **kw):
+    s = FSD(N, (Lc, Lc, Lc, 0.0), precond="learned", solver_tol=1e-4, gmres_restart=100, gmres_max_iter=3000,
+            **kw)
+    if kw.get("learned_poly", 0):
+        s.learned_set_weights(np.fromfile(WEIGHTS, "<f4"))
+    p = torch.as_tensor(pos).cuda().view(-1).contiguous()
+    s.build_neighbor_list(p)
+    best = None
+    for rep in range(3):  # the first run captures graphs and sizes workspaces
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        s.precond_build(p)
+        x, it, res, st = s.saddle_solve(p, rhs, raise_on_error=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if rep and (best is None or ms < best[0]):
+            best = (ms, it, res, st, x.cpu().numpy().astype(np.float64), s.solve_info())
+    s.close()
+    return best
+
+
+@pytest.mark.parametrize("phi", [0.45, 0.5, 0.55])
+def test_learned_interval_beats_inner_gmres(cuda, phi):
+    assert WEIGHTS.exists(), "the trained interval network ships with the package"
+    pos, Lc = suspension(N, phi, seed=2000 + int(round(phi * 100)))
+    psi = np.random.default_rng(int(round(phi * 100))).standard_normal(6 * N)
+    rhs_h = np.zeros(17 * N)
+    rhs_h[11 * N:] = -psi
+    rhs = torch.as_tensor(rhs_h, dtype=torch.float32).cuda()
+    ms_g, it_g, res_g, st_g, _, _ = _solve(pos, Lc, rhs, learned_inner=6)
+    ms_p, it_p, res_p, st_p, x, info = _solve(pos, Lc, rhs, learned_inner=0, learned_poly=10)
+    print(f"phi={phi}: inner GMRES {it_g} it {ms_g:.1f} ms | learned interval rho={info['poly_ratio']:.4f} "
+          f"{it_p} it {ms_p:.1f} ms")
+    assert st_g == 0 and st_p == 0 and res_p < 1e-4
+    assert info["poly_source"] == 1  # the interval came from the network
+    assert it_p < it_g
+    assert ms_p < ms_g
+    Lt = (Lc, Lc, Lc)
+    table = ewald_golden()
+    pr = O.Problem(pos, Lt, 0.0, table=table, rows=O.neighbor_list_kdtree(pos, Lt, table[3] + 0.4))
+    r = rhs.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(r - pr.saddle_multiply(x)) / np.linalg.norm(r) < 1.1e-4
