@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--phi", type=float, default=0.4)
     ap.add_argument("--precond", default="learned", choices=["ichol", "none", "learned"])
     ap.add_argument("--inner", type=int, default=6, help="inner GMRES steps of the learned preconditioner")
-    ap.add_argument("--poly", type=int, default=10,
-                    help="terms of the learned inner polynomial (0: inner GMRES steps instead)")
-    ap.add_argument("--no-compare", action="store_true", help="skip the no-network forms")
+    ap.add_argument("--poly", type=int, default=0,
+                    help="main arm: terms of the learned inner polynomial (0: inner GMRES steps)")
+    ap.add_argument("--poly-terms", type=int, default=10,
+                    help="terms of the inner polynomial in the comparison arms (and in --case / --config5)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the other forms of the preconditioner")
     ap.add_argument("--no-ichol", action="store_true", help="skip the IChol comparison run")
     ap.add_argument("--no-net", action="store_true", help="learned preconditioner without the network correction")
     ap.add_argument("--no-autotune", action="store_true", help="fixed spreading tiles and FFT batches")
@@ -375,24 +377,29 @@ def run_fsd(args, ws, rank, local):
         ichol = {"value": ws * args.ichol_steps / (r["total_ms"] / 1e3), "unit": "steps/s",
                  "ms_per_step": r["total_ms"] / args.ichol_steps, "steps": args.ichol_steps, "warmup": 1,
                  "iterations_per_step": r["iters"]}
-    # --- the preconditioner's forms without the network, on the same steps of
-    # the same trajectory: the approximate inverse with inner GMRES steps, and
-    # the polynomial fitted to probe vectors at every build
-    no_network = {}
+    # --- the preconditioner's other forms on the same steps of the same
+    # trajectory: inner GMRES steps on the approximate inverse, and the inner
+    # polynomial with the network's interval, a fixed interval, or
+    # coefficients fitted to probe vectors at every build
+    forms = {}
     if args.precond == "learned" and not args.no_compare:
-        forms = {"spai_inner_gmres": ("gmres", 0.05)}
-        if args.poly >= 2:
-            forms["fixed_interval_polynomial"] = ("poly", 0.05)
-            forms["fitted_polynomial"] = ("poly", 0.0)
-        for name, (form, interval) in forms.items():
+        main_poly = args.poly >= 2
+        cand = {"spai_inner_gmres": ("gmres", 0.05, False)} if main_poly else {}
+        if not main_poly:
+            cand["learned_interval_polynomial"] = ("poly", 0.05, True)
+        cand["fixed_interval_polynomial"] = ("poly", 0.05, False)
+        cand["fitted_polynomial"] = ("poly", 0.0, False)
+        for name, (form, interval, with_net) in cand.items():
             a2 = argparse.Namespace(**vars(args))
-            a2.no_net = True
-            sc, _ = make_solver(a2, "learned", N, L, dev, 1 + rank, form=form, interval=interval)
+            a2.no_net = not with_net
+            if form == "poly":
+                a2.poly = args.poly if main_poly else args.poly_terms
+            sc, net2 = make_solver(a2, "learned", N, L, dev, 1 + rank, form=form, interval=interval)
             r = timed_steps(a2, sc, fresh_state(), args.steps, args.warmup, dev, ws)
             sc.close()
-            no_network[name] = {"value": ws * args.steps / (r["total_ms"] / 1e3), "unit": "steps/s",
-                                "ms_per_step": r["total_ms"] / args.steps, "iterations_per_step": r["iters"],
-                                "precond_form": precond_form(a2, False, form, interval)}
+            forms[name] = {"value": ws * args.steps / (r["total_ms"] / 1e3), "unit": "steps/s",
+                           "ms_per_step": r["total_ms"] / args.steps, "iterations_per_step": r["iters"],
+                           "learned_network": net2, "precond_form": precond_form(a2, net2, form, interval)}
     # --- roofline of the dominant single-kernel region (profiled pass)
     regions = prof["regions"]
     prof_steps = prof["steps"]
@@ -418,7 +425,8 @@ def run_fsd(args, ws, rank, local):
         "config": {"workload": workload_name(N, phi), "N": N, "phi": phi,
                    "grid": [info.Nx, info.Ny, info.Nz], "P": info.P, "precond": args.precond,
                    "learned_inner": args.inner if (args.precond == "learned" and args.poly < 2) else None,
-                   "learned_poly": args.poly if args.precond == "learned" else None, "learned_network": net,
+                   "learned_poly": args.poly if (args.precond == "learned" and args.poly >= 2) else None,
+                   "learned_network": net,
                    "precond_form": precond_form(args, net),
                    "autotune": not args.no_autotune,
                    "gmres_tol": 1e-4, "ewald_error": 1e-3, "l2": "flushed before every timed step (256 MiB write)",
@@ -431,10 +439,10 @@ def run_fsd(args, ws, rank, local):
                                   "with it off"},
         "ichol": ichol,
         "speedup_vs_ichol": (value / ichol["value"]) if ichol else None,
-        "no_network": no_network,
-        "speedup_vs_ichol_no_network": {k: v["value"] / ichol["value"] for k, v in no_network.items()} if ichol
+        "other_forms": forms,
+        "speedup_vs_ichol_other_forms": {k: v["value"] / ichol["value"] for k, v in forms.items()} if ichol
         else None,
-        "speedup_vs_no_network": {k: value / v["value"] for k, v in no_network.items()},
+        "headline_over_other_forms": {k: value / v["value"] for k, v in forms.items()},
         "clocks": main["clocks"],
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -627,7 +635,7 @@ def run_config5(args, local):
                                       poly_interval=0.05),
         "learned_poly10": dict(precond="learned", gmres_restart=100, learned_inner=0, learned_poly=10),
     }
-    w = np.fromfile(poly_weights(10), "<f4") if poly_weights(10).exists() else None
+    w = np.fromfile(poly_weights(10), "<f4") if poly_weights(10).exists() else None  # the shipped k = 10 network
     results = {}
     for phi in args.config5_phis:
         pos, L = suspension(N, phi, seed=1000 + int(round(phi * 100)))  # seeds the training never used
@@ -640,7 +648,10 @@ def run_config5(args, local):
             if name == "learned_poly10":
                 s.learned_set_weights(w)
             times, iters, resid = [], [], []
-            for rep in range(2):  # the first call also captures graphs and tunes
+            # the first call also captures graphs and tunes; the second is timed
+            # at the next timestep (new Brownian draws; the main solve starts
+            # from the first call's solution, as in a trajectory)
+            for rep in range(2):
                 p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
                 ori = torch.as_tensor(np.tile([0.0, 0.0, 1.0], N).astype(np.float32), device=dev)
                 img = torch.zeros(3 * N, dtype=torch.int32, device=dev)
@@ -649,7 +660,7 @@ def run_config5(args, local):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize(dev)
                 e0.record()
-                a = s.step_args(0, 1.0, p, ori, img, F, V)
+                a = s.step_args(rep, 1.0, p, ori, img, F, V)
                 st = _lib.lib().fsd_compute_velocity(s._h, C.byref(a))
                 e1.record()
                 torch.cuda.synchronize(dev)
@@ -675,7 +686,7 @@ def run_config5(args, local):
 def run_case(args, local):
     """One operator of the path on the benchmarked suspension (N, phi, seed 1):
     the mobility (wave + real space), one application of the learned inner
-    polynomial (k = --poly, fixed interval 0.05) or of the inner-GMRES form
+    polynomial (k = --poly-terms, fixed interval 0.05) or of the inner-GMRES form
     (--inner steps), or one build of the learned preconditioner with the
     shipped network; CUDA-event time per call."""
     import torch
@@ -690,14 +701,14 @@ def run_case(args, local):
     p = torch.as_tensor(pos, device=dev).view(-1).contiguous()
     kw = {}
     if args.case == "poly_apply":
-        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly, poly_interval=0.05)
+        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly_terms, poly_interval=0.05)
     elif args.case == "gmres_apply":
         kw = dict(precond="learned", learned_inner=args.inner)
     elif args.case == "precond_build":
-        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly)
+        kw = dict(precond="learned", learned_inner=0, learned_poly=args.poly_terms)
     s = FSD(N, (L, L, L, 0.0), device=dev, **kw)
-    if args.case == "precond_build" and poly_weights(args.poly).exists():
-        s.learned_set_weights(np.fromfile(poly_weights(args.poly), "<f4"))
+    if args.case == "precond_build" and poly_weights(args.poly_terms).exists():
+        s.learned_set_weights(np.fromfile(poly_weights(args.poly_terms), "<f4"))
     s.build_neighbor_list(p)
     rng = np.random.default_rng(0)
     if args.case == "mobility":

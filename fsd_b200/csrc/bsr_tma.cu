@@ -167,6 +167,22 @@ __global__ void __launch_bounds__(kBsrThreads, 8) k_bsr_tma(BsrTmaArgs a) {
     for (int rl = group; rl < r1 - r0; rl += kBsrThreads / 8) {
         const int r = r0 + rl;
         const int qb = sR[rl], qe = sR[rl + 1];
+        const size_t i6 = 6 * (size_t)r + lane8;
+        // the row's epilogue operands, loaded before the multiply so that
+        // their latency overlaps it
+        float e_a = 0.f, e_b = 0.f, e_c = 0.f;
+        if (lane8 < 6) {
+            if (MODE == 0) {
+                e_a = a.x[i6];
+                e_b = a.x[offU + i6];
+            } else if (MODE == 2) {
+                e_a = a.b[i6];
+            } else if (MODE == 3) {
+                e_a = a.T[i6];
+                e_b = a.B1[i6];
+                e_c = a.B2 ? a.B2[i6] : 0.f;
+            }
+        }
         float acc = 0.f;
         for (int q = qb; q < qe; ++q) {
             const float2* g2 = reinterpret_cast<const float2*>(sG + (size_t)q * 36 + rr * 6);
@@ -180,11 +196,10 @@ __global__ void __launch_bounds__(kBsrThreads, 8) k_bsr_tma(BsrTmaArgs a) {
             acc = fmaf(g45.x, x45.x, acc);
             acc = fmaf(g45.y, x45.y, acc);
         }
-        const size_t i6 = 6 * (size_t)r + lane8;
         if (MODE == 0) {
             if (lane8 < 6) {
                 const float c = a.pc[a.k - 1];
-                const float tv = a.x[i6] - a.x[offU + i6];
+                const float tv = e_a - e_b;
                 a.T[i6] = tv;
                 a.B[i6] = c * tv;
                 a.out[i6] = c * acc;
@@ -193,8 +208,7 @@ __global__ void __launch_bounds__(kBsrThreads, 8) k_bsr_tma(BsrTmaArgs a) {
             if (lane8 < 6) a.out[i6] = acc;
         } else if (MODE == 2) {
             if (lane8 < 6) {
-                const float bq = a.b[i6];
-                a.xs[i6] = bq - acc;
+                a.xs[i6] = e_a - acc;
                 a.xs[offU + i6] = acc;
             }
             if (lane8 < 5) {
@@ -205,8 +219,8 @@ __global__ void __launch_bounds__(kBsrThreads, 8) k_bsr_tma(BsrTmaArgs a) {
             if (lane8 < 6) {
                 const float s2 = 2.0f / a.pc[kMaxPoly];
                 const float f = a.m >= 1 ? 2.0f : 1.0f;
-                float v = fmaf(a.pc[a.m], a.T[i6], f * fmaf(s2, acc, -a.B1[i6]));
-                if (a.B2) v -= a.B2[i6];
+                float v = fmaf(a.pc[a.m], e_a, f * fmaf(s2, acc, -e_b));
+                if (a.B2) v -= e_c;
                 a.out[i6] = v;
             }
         }
