@@ -8,14 +8,20 @@ difference drift (two saddle solves), main saddle solve to relative residual
 Ewald accuracy 1e-3 (xi 0.5, 72^3 grid, P = 6).  Positions from seeded random
 sequential addition followed by overlap relaxation.
 
-The timed preconditioner is the learned one by default (two-hop sparse
-approximate inverse of the lubrication block, inner GMRES steps, flexible outer
-GMRES, and the trained network's correction when fsd_b200/data holds
-weights); the same steps with the plain IChol preconditioner are timed after
-it for the metric's comparison ("ichol" in the JSON line).
+The headline preconditioner is the learned family's fastest form at this
+configuration: the two-hop sparse approximate inverse of the lubrication block
+with six inner GMRES steps and flexible outer GMRES (no network,
+"learned_network": false).  The same steps are then timed with the family's
+other forms -- the inner Chebyshev polynomial whose interval the trained
+network predicts ("learned_interval_polynomial"), a fixed interval, and
+coefficients fitted at every build ("other_forms") -- and with the plain IChol
+preconditioner for the metric's comparison ("ichol").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fsd|reference]
-                  [--precond learned|ichol|none] [--inner k] [--no-ichol] [--no-net]
+                  [--precond learned|ichol|none] [--inner k] [--poly k] [--no-ichol]
+  python bench.py --config5          # held-out dense suspensions, one velocity computation per form
+  python bench.py --case mobility|poly_apply|gmres_apply|precond_build   # one operator (profiling cases)
+  python bench.py --replicas 64      # batched replicas
 
 Under torchrun each rank steps its own independent suspension (the path does
 not shard within one suspension; replicas only).  Prints one JSON line.
@@ -561,8 +567,18 @@ def cpu_baseline(args, pos, L, gpu_out=None, sampler=None):
             iters, src = {"gmres_rfd_plus": 300.0, "gmres_rfd_minus": 300.0, "gmres_main": 300.0,
                           "lanczos_ff": 9.0, "lanczos_nf": 25.0}, "an assumed 300 per solve"
     sec, parts = sampler.step_seconds(iters)
+    # a complete step run end to end at a size the FP64 oracle finishes in seconds
+    from fsd_b200.configs import suspension
+    from oracle.cpu_step import full_step_seconds
+    pos_s, L_s = suspension(1000, float(args.phi), seed=1)
+    fs, fparts, fits = full_step_seconds(pos_s, L_s, ewald_table_golden())
+    full = {"N": 1000, "phi": float(args.phi), "seconds": fs, "steps_per_s": 1.0 / fs,
+            "iterations": fits, "stage_seconds": {k: round(v, 3) for k, v in fparts.items()},
+            "note": "one complete FP64 step measured end to end (oracle.cpu_step.full_step_seconds): "
+                    "Lanczos samplers, two RFD solves and the main solve with GMRES(200) to 1e-4 and SciPy's "
+                    "incomplete LU in the IC(0) slot"}
     return {"value": 1.0 / sec, "unit": "steps/s", "cores": sampler.threads, "kind": "port",
-            "cpu_model": cpu_model(),
+            "cpu_model": cpu_model(), "full_step_measured": full,
             "sample": f"FP64 oracle at N={len(pos)}: every stage of one step timed once on the configuration "
                       f"({time.time() - t0:.0f} s of host time), GMRES/Lanczos stage costs per iteration scaled by "
                       f"the iteration counts of {src}; FFTs on {sampler.threads} threads, pair sums single-threaded",

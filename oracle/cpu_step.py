@@ -26,6 +26,11 @@ assembled from those stage times and the operator counts of the IChol method:
 
 FFTs run on all host cores (scipy.fft workers) and dense BLAS uses its
 default threads; the pair sums are single-threaded NumPy.
+
+`full_step_seconds` runs one complete step end to end instead (Lanczos to
+convergence, the three GMRES solves to 1e-4), at sizes the FP64 oracle
+finishes in seconds (N = 1000); bench.py reports it beside the assembled
+full-size figure.
 """
 from __future__ import annotations
 
@@ -151,3 +156,107 @@ class StepSampler:
             "gmres": g * per_it + 6 * t["saddle_op"], "euler": t["euler"],
         }
         return float(sum(parts.values())), parts
+
+
+def _lanczos_sqrt(op, z, tol=1e-3, max_iter=100):
+    """Chow-Saad Lanczos approximation of op^(1/2) z (Brownian_FarField.cu:597-808,
+    Brownian_NearField.cu:174-464): m-step Lanczos, square root of the small
+    tridiagonal matrix, stopped when the sample changes by less than tol."""
+    from scipy.linalg import eigh_tridiagonal
+    n = len(z)
+    zn = np.linalg.norm(z)
+    V = np.zeros((max_iter + 1, n))
+    V[0] = z / zn
+    alpha, beta = [], []
+    prev = None
+    y = None
+    for m in range(max_iter):
+        w = op(V[m])
+        if m:
+            w -= beta[-1] * V[m - 1]
+        a = float(V[m] @ w)
+        w -= a * V[m]
+        alpha.append(a)
+        b = float(np.linalg.norm(w))
+        ev, Q = eigh_tridiagonal(np.array(alpha), np.array(beta))
+        s = Q @ (np.sqrt(np.maximum(ev, 0.0)) * Q[0])
+        y = zn * (V[: m + 1].T @ s)
+        if prev is not None and np.linalg.norm(y - prev) <= tol * np.linalg.norm(y):
+            return y, m + 1
+        prev = y
+        if b == 0.0:
+            return y, m + 1
+        beta.append(b)
+        V[m + 1] = w / b
+    return y, max_iter
+
+
+def full_step_seconds(pos, L, table, shear_rate=1.0, kT=1.0, dt=1e-4, tol=1e-4, seed=0):
+    """One complete FP64 FSD step with the IChol method's preconditioner
+    (SciPy's incomplete LU of the pruned R_FU + D standing in for csric02),
+    timed end to end on the host cores: neighbour list, pair force,
+    preconditioner build, far-field noise (one wave-space pass for the random
+    field plus Lanczos on the real-space mobility), near-field noise (Lanczos
+    on R_FU), the two random-finite-difference solves and the main solve
+    (GMRES(200) to tol, Saddle.cu:171-264 block preconditioner), stresslet
+    and Euler update.  Returns (seconds, stage seconds, iteration counts)."""
+    import scipy.sparse.linalg as sla
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    st = StepSampler(pos, L, table)
+    N = st.N
+    t = {}
+    rows, t["nlist"] = _timed(st._neighbor_rows)
+    pr = O.Problem(st.pos, st.L, 0.0, table=table, rows=rows)
+    F, t["pair_force"] = _timed(O.pair_force, st.pos, st.L, 0.0, rows)
+
+    def build():
+        A = O.pruned_rfu_sparse(st.pos, st.L, 0.0, pr.tdist, pr.tvals, rows=rows, rp=2.1).tocsc()
+        return sla.spilu(A, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0)
+    ilu, t["precond_build"] = _timed(build)
+    n = 17 * N
+
+    def pc(b):
+        y = ilu.solve(b[: 6 * N] - b[11 * N:])
+        x = b.copy()
+        x[: 6 * N] = b[: 6 * N] - y
+        x[11 * N:] = y
+        return x
+    Aop = sla.LinearOperator((n, n), matvec=pr.saddle_multiply, dtype=np.float64)
+    Mop = sla.LinearOperator((n, n), matvec=pc, dtype=np.float64)
+    its = {}
+
+    def solve(rhs, name):
+        count = [0]
+
+        def cb(_):
+            count[0] += 1
+        x, _ = sla.gmres(Aop, rhs, M=Mop, rtol=tol, restart=200, maxiter=20, callback=cb,
+                         callback_type="pr_norm")
+        its[name] = count[0]
+        return x
+    scale = np.sqrt(2.0 * kT / dt)
+    tb = time.perf_counter()
+    wave = pr.mobility(rng.standard_normal(11 * N), 1)
+    u_ff, its["lanczos_ff"] = _lanczos_sqrt(lambda v: pr.mobility(v, 2), rng.standard_normal(11 * N))
+    f_nf, its["lanczos_nf"] = _lanczos_sqrt(pr.rfu, rng.standard_normal(6 * N))
+    t["brownian"] = time.perf_counter() - tb
+    tr = time.perf_counter()
+    psi = rng.standard_normal(6 * N)
+    rhs = np.zeros(n)
+    rhs[11 * N:] = -psi
+    up = solve(rhs, "gmres_rfd_plus")
+    um = solve(rhs, "gmres_rfd_minus")
+    t["rfd"] = time.perf_counter() - tr
+    tm = time.perf_counter()
+    rhs = O.strain_rhs(shear_rate, N)
+    rhs[: 11 * N] += scale * (wave + u_ff)
+    rhs[11 * N:] += scale * f_nf - F + O.rfe(pr.pos, shear_rate, st.L, 0.0, rows, pr.tdist, pr.tvals)
+    x = solve(rhs, "gmres_main")
+    U = x[11 * N:] + (kT / 1e-3) * 1e-3 * (up[11 * N:] - um[11 * N:])
+    O.rsu(pr.pos, U, st.L, 0.0, rows, pr.tdist, pr.tvals)
+    t["main_solve"] = time.perf_counter() - tm
+    ori = np.tile([0.0, 0.0, 1.0], (N, 1))
+    _, t["euler"] = _timed(O.euler_shear, st.pos, ori, np.zeros((N, 4)), U, np.zeros((N, 3), np.int64), st.L, 0.0,
+                           dt, shear_rate)
+    return time.perf_counter() - t0, t, its
