@@ -321,11 +321,34 @@ __global__ void __launch_bounds__(kInnerThreads) k_inner_orth(float* U, size_t l
     __syncthreads();
     float* w = U + (size_t)nv * ld;
     double s = 0.0;
-    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-        float acc = w[k];
-        for (int q = 0; q < nv; ++q) acc = fmaf(-hc[q], U[(size_t)q * ld + k], acc);
-        w[k] = acc;
-        s += (double)acc * acc;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if ((n & 3) == 0 && (ld & 3) == 0) {  // 16-byte aligned vectors (6N divisible by 4): float4 loads
+        float4* w4 = reinterpret_cast<float4*>(w);
+        const float4* U4 = reinterpret_cast<const float4*>(U);
+        const size_t n4 = n >> 2, ld4 = ld >> 2;
+        for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n4; k += stride) {
+            float4 acc = w4[k];
+            for (int q = 0; q < nv; ++q) {
+                const float4 u = U4[(size_t)q * ld4 + k];
+                const float c = -hc[q];
+                acc.x = fmaf(c, u.x, acc.x);
+                acc.y = fmaf(c, u.y, acc.y);
+                acc.z = fmaf(c, u.z, acc.z);
+                acc.w = fmaf(c, u.w, acc.w);
+            }
+            w4[k] = acc;
+            s += (double)acc.x * acc.x;
+            s += (double)acc.y * acc.y;
+            s += (double)acc.z * acc.z;
+            s += (double)acc.w * acc.w;
+        }
+    } else {
+        for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += stride) {
+            float acc = w[k];
+            for (int q = 0; q < nv; ++q) acc = fmaf(-hc[q], U[(size_t)q * ld + k], acc);
+            w[k] = acc;
+            s += (double)acc * acc;
+        }
     }
     block_partial(s, part);
     if (!last_block(ticket)) return;
