@@ -93,6 +93,9 @@ _SIGS = {
     "fsd_set_temperature": (C.c_int, [H, C.c_float]),
     "fsd_get_pse_info": (C.c_int, [H, C.POINTER(fsd_pse_info)]),
     "fsd_get_solve_info": (C.c_int, [H, C.POINTER(fsd_solve_info)]),
+    "fsd_checkpoint_size": (C.c_size_t, [H]),
+    "fsd_checkpoint_save": (C.c_int, [H, P, C.c_size_t]),
+    "fsd_checkpoint_load": (C.c_int, [H, P, C.c_size_t]),
     "fsd_profile_enable": (C.c_int, [H, C.c_int]),
     "fsd_profile_read": (C.c_int, [H, P, P, C.c_int, C.c_int]),
     "fsd_get_ewald_table": (C.c_int, [H, P, C.c_size_t]),

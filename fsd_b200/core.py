@@ -112,6 +112,21 @@ class FSD:
         check(lib().fsd_get_pse_info(self._h, C.byref(info)), "fsd_get_pse_info")
         return PSEInfo(*[getattr(info, f) for f, _ in info._fields_])
 
+    def checkpoint(self) -> bytes:
+        """The solver state this handle carries into the next step (warm start,
+        Lanczos sizes, IC(0) relaxer), as bytes for fsd_checkpoint_load."""
+        self._sync_stream()
+        n = lib().fsd_checkpoint_size(self._h)
+        buf = C.create_string_buffer(n)
+        check(lib().fsd_checkpoint_save(self._h, buf, n), "fsd_checkpoint_save")
+        return buf.raw
+
+    def restore(self, data: bytes):
+        """Load a checkpoint written by checkpoint() on a handle of the same N."""
+        self._sync_stream()
+        buf = C.create_string_buffer(bytes(data), len(data))
+        check(lib().fsd_checkpoint_load(self._h, buf, len(data)), "fsd_checkpoint_load")
+
     def solve_info(self) -> dict:
         info = _lib.fsd_solve_info()
         check(lib().fsd_get_solve_info(self._h, C.byref(info)), "fsd_get_solve_info")

@@ -411,6 +411,50 @@ int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info) {
     return FSD_OK;
 }
 
+namespace {
+struct CheckpointHeader {
+    uint32_t magic;    // 'FSDC'
+    uint32_t version;  // 1
+    int32_t N;
+    int32_t m_lanczos_ff, m_lanczos_nf;
+    float ichol_relaxer;
+};
+constexpr uint32_t kCheckpointMagic = 0x43445346u;
+}  // namespace
+
+size_t fsd_checkpoint_size(const fsd_handle* h) {
+    if (!h) return 0;
+    return sizeof(CheckpointHeader) + sizeof(float) * 17 * (size_t)h->p.N;
+}
+
+int fsd_checkpoint_save(fsd_handle* h, void* host, size_t bytes) {
+    if (!h || !host || bytes < fsd_checkpoint_size(h)) return FSD_ERR_BAD_PARAMS;
+    CheckpointHeader hd{kCheckpointMagic, 1u, h->p.N, h->m_lanczos_ff, h->m_lanczos_nf, h->ichol_relaxer};
+    std::memcpy(host, &hd, sizeof(hd));
+    float* sol = reinterpret_cast<float*>(static_cast<char*>(host) + sizeof(hd));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(sol, h->w.sol, sizeof(float) * 17 * (size_t)h->p.N, cudaMemcpyDeviceToHost,
+                                   h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    return FSD_OK;
+}
+
+int fsd_checkpoint_load(fsd_handle* h, const void* host, size_t bytes) {
+    if (!h || !host || bytes < fsd_checkpoint_size(h)) return FSD_ERR_BAD_PARAMS;
+    CheckpointHeader hd;
+    std::memcpy(&hd, host, sizeof(hd));
+    if (hd.magic != kCheckpointMagic || hd.version != 1u || hd.N != h->p.N || hd.m_lanczos_ff < 1 ||
+        hd.m_lanczos_nf < 1 || !(hd.ichol_relaxer > 0.f))
+        return FSD_ERR_BAD_PARAMS;
+    const float* sol = reinterpret_cast<const float*>(static_cast<const char*>(host) + sizeof(hd));
+    FSD_CHECK_CUDA(cudaMemcpyAsync(h->w.sol, sol, sizeof(float) * 17 * (size_t)h->p.N, cudaMemcpyHostToDevice,
+                                   h->stream));
+    FSD_CHECK_CUDA(cudaStreamSynchronize(h->stream));
+    h->m_lanczos_ff = hd.m_lanczos_ff;
+    h->m_lanczos_nf = hd.m_lanczos_nf;
+    h->ichol_relaxer = hd.ichol_relaxer;
+    return FSD_OK;
+}
+
 int fsd_get_ewald_table(const fsd_handle* h, float* host_table, size_t n_floats) {
     if (!h || !host_table || n_floats < h->ewald_host.size()) return FSD_ERR_BAD_PARAMS;
     memcpy(host_table, h->ewald_host.data(), sizeof(float) * h->ewald_host.size());

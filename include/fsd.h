@@ -213,6 +213,20 @@ int fsd_get_pse_info(const fsd_handle* h, fsd_pse_info* info);
 int fsd_profile_enable(fsd_handle* h, int on);
 int fsd_profile_read(fsd_handle* h, double* ms, long long* counts, int n, int reset);
 int fsd_get_solve_info(const fsd_handle* h, fsd_solve_info* info);
+
+/* Checkpoint of the solver state one step carries into the next (the carried
+ * state of Stokes::integrateStepOne, Stokes.cc:1658-1666, and the main
+ * solve's warm start, Integrator.cu:777): the saddle solution (17N floats),
+ * the far- and near-field Lanczos sizes and the IC(0) relaxer.  Positions,
+ * orientations, images and the timestep are the caller's; the Brownian
+ * draws are keyed by (seed, timestep), so a handle created with the same
+ * parameters, loaded from a checkpoint and given the same caller arrays
+ * continues the trajectory bit for bit.  fsd_checkpoint_size gives the
+ * bytes; save writes them to host memory, load reads them back (same N;
+ * FSD_ERR_BAD_PARAMS for a checkpoint of another size or format). */
+size_t fsd_checkpoint_size(const fsd_handle* h);
+int fsd_checkpoint_save(fsd_handle* h, void* host, size_t bytes);
+int fsd_checkpoint_load(fsd_handle* h, const void* host, size_t bytes);
 /* Copy the real-space Ewald table (2*(ewald_n+1) float4) to host memory. */
 int fsd_get_ewald_table(const fsd_handle* h, float* host_table, size_t n_floats);
 
