@@ -27,3 +27,15 @@ def test_suspension_is_reproducible():
     b, _ = suspension(500, 0.3, seed=3)
     c, _ = suspension(500, 0.3, seed=4)
     assert np.array_equal(a, b) and not np.array_equal(a, c)
+
+
+def test_cpu_full_step_runs_to_convergence():
+    """The host-core baseline's complete FP64 step (oracle.cpu_step) on a small
+    box: every solve converges within its restart and the stage times add up."""
+    from conftest import ewald_golden
+    from oracle.cpu_step import full_step_seconds
+    pos, L = suspension(200, 0.3, seed=2)
+    sec, parts, its = full_step_seconds(pos, L, ewald_golden())
+    assert sec > 0 and sum(parts.values()) <= sec * 1.01
+    assert 0 < its["gmres_main"] < 200 and 0 < its["gmres_rfd_plus"] < 200
+    assert its["lanczos_ff"] >= 2 and its["lanczos_nf"] >= 2
