@@ -909,7 +909,7 @@ struct __align__(16) StagedParticle {  // read as four float4: (x, y, z, o), v[0
 //                broadcast) and adding it when its node lies in the stencil.
 //                Needs TX % 2 == 0, TY % 4 == 0, TZ % 4 == 0.
 template <bool ROWS>
-__global__ void __launch_bounds__(256, 3) k_spread(SpreadArgs a) {
+__global__ void __launch_bounds__(256, ROWS ? 3 : 4) k_spread(SpreadArgs a) {
     __shared__ StagedParticle sp[kSpreadCap];
     __shared__ int so[ROWS ? 1 : kSpreadCap];  // packed origins, contiguous for the ballot
     __shared__ unsigned scan_sh[32];
