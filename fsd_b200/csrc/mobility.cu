@@ -740,7 +740,7 @@ struct DigitSlot {
 
 // The fused x-pass for Nx = N1 * N2: one shared buffer, rows padded to N + 1.
 template <int N1, int N2>
-__global__ void __launch_bounds__(256, 2) k_fft_x_green_t(float2* __restrict__ grid, const float4* __restrict__ gridk,
+__global__ void __launch_bounds__(256, 3) k_fft_x_green_t(float2* __restrict__ grid, const float4* __restrict__ gridk,
                                                           int Ny, int Nz, int B, int nzc,
                                                           const float2* __restrict__ tw_global) {
     constexpr int n = N1 * N2, LS = n + 1;
