@@ -39,3 +39,24 @@ def test_cpu_full_step_runs_to_convergence():
     assert sec > 0 and sum(parts.values()) <= sec * 1.01
     assert 0 < its["gmres_main"] < 200 and 0 < its["gmres_rfd_plus"] < 200
     assert its["lanczos_ff"] >= 2 and its["lanczos_nf"] >= 2
+
+
+def test_smoothed_interval_target_avoids_a_cliff():
+    """The interval-network training target with --smooth: the candidate whose
+    iteration count, averaged in log with its neighbours, is lowest -- so a
+    lone minimum next to a steep rise loses to a flat valley."""
+    from fsd_b200.train_precond import smoothed_best
+    its = {0.01: 900, 0.02: 60, 0.03: 400, 0.045: 80, 0.07: 78, 0.1: 82, 0.15: 120}
+    assert min(its, key=its.get) == 0.02
+    assert smoothed_best(its) == 0.07
+    its[0.03] = 10 ** 9  # a candidate that never converged counts as infinitely bad
+    assert smoothed_best(its) == 0.07
+
+
+def test_configuration_cache_round_trip(tmp_path):
+    from fsd_b200.train_precond import configuration
+    a, La = configuration(300, 0.3, 5, tmp_path)
+    assert (tmp_path / "susp_N300_phi0.3_s5.npz").exists()
+    b, Lb = configuration(300, 0.3, 5, tmp_path)
+    c, _ = suspension(300, 0.3, seed=5)
+    assert La == Lb and np.array_equal(a, b) and np.array_equal(a, c)
