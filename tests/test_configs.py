@@ -60,3 +60,20 @@ def test_configuration_cache_round_trip(tmp_path):
     b, Lb = configuration(300, 0.3, 5, tmp_path)
     c, _ = suspension(300, 0.3, seed=5)
     assert La == Lb and np.array_equal(a, b) and np.array_equal(a, c)
+
+
+def test_cpu_lanczos_square_root_matches_dense():
+    """The Chow-Saad Lanczos square root of the host-core baseline against a
+    dense eigendecomposition, on a small SPD matrix with the spread of
+    eigenvalues of a lubrication block (1e-3 to 1)."""
+    from oracle.cpu_step import _lanczos_sqrt
+    rng = np.random.default_rng(4)
+    n = 60
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    ev = np.geomspace(1e-3, 1.0, n)
+    A = (Q * ev) @ Q.T
+    z = rng.standard_normal(n)
+    y, m = _lanczos_sqrt(lambda v: A @ v, z, tol=1e-10, max_iter=n)
+    ref = (Q * np.sqrt(ev)) @ (Q.T @ z)
+    assert np.linalg.norm(y - ref) < 1e-6 * np.linalg.norm(ref)
+    assert m <= n
