@@ -213,6 +213,22 @@ def make_solver(args, precond, N, L, dev, seed, form=None, interval=0.05):
     return s, net
 
 
+def max_over_ranks(value: float, dev, ws: int) -> float:
+    """The largest of the ranks' values (every rank takes part; a no-op on one
+    rank): the device time of a multi-GPU run is its slowest rank's."""
+    if ws <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(ws: int, steps: int, ms: float) -> float:
+    """Steps per second of the whole job: every rank steps its own replica."""
+    return ws * steps / (ms / 1e3)
+
+
 def timed_steps(args, s, state, steps, warmup, dev, ws, clocks=False, profile=False):
     """Warm-up, then `steps` steps each bracketed by CUDA events on the launching
     stream with a 256 MiB L2 flush before it (outside the events)."""
@@ -264,11 +280,7 @@ def timed_steps(args, s, state, steps, warmup, dev, ws, clocks=False, profile=Fa
     if ws > 1:
         torch.distributed.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = float(sum(step_ms))
-    if ws > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(sum(step_ms)), dev, ws)
     regions = None
     if profile:
         lib.fsd_profile_read(s._h, ms_regions.ctypes.data_as(C.c_void_p), cnt_regions.ctypes.data_as(C.c_void_p),
@@ -313,7 +325,7 @@ def run_fsd(args, ws, rank, local):
     state = fresh_state()
     # Headline: device time of the steps with the library's region profiler off.
     main = timed_steps(args, s, state, args.steps, args.warmup, dev, ws, clocks=True, profile=False)
-    value = ws * args.steps / (main["total_ms"] / 1e3)
+    value = whole_job_rate(ws, args.steps, main["total_ms"])
     # Per-region breakdown and the roofline's launch times: a separate pass over
     # the next steps of the same trajectory with the CUDA-event profiler on.
     prof = timed_steps(args, s, state, max(1, min(3, args.steps)), 0, dev, ws, profile=True)
@@ -362,12 +374,8 @@ def run_fsd(args, ws, rank, local):
             si = s.solve_info()
             e2e_iters.append(si["gmres_iters"] + [si["lanczos_ff_iters"], si["lanczos_nf_iters"]])
         torch.cuda.synchronize(dev)
-        e2e_ms = float(sum(a.elapsed_time(b) for a, b in evs))
-        if ws > 1:
-            t = torch.tensor([e2e_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": "steps/s",
+        e2e_ms = max_over_ranks(float(sum(a.elapsed_time(b) for a, b in evs)), dev, ws)
+        e2e = {"value": whole_job_rate(ws, args.steps, e2e_ms), "unit": "steps/s",
                "h2d_bytes_per_step": int(4 * (h_pos.numel() + h_ori.numel() + h_img.numel())),
                "d2h_bytes_per_step": int(4 * (h_V.numel() + h_pos.numel() + h_ori.numel() + h_img.numel())),
                "ms_per_step": e2e_ms / args.steps,
