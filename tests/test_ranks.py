@@ -36,7 +36,7 @@ def _rank(rank, ws, port, out):
 
 def test_max_over_ranks_and_whole_job_rate_on_two_ranks():
     ws = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_rank, args=(ws, _free_port(), out), nprocs=ws, join=True, start_method="spawn")
         res = dict(out)
