@@ -19,15 +19,16 @@ its solution satisfies the FP64 oracle's saddle system to 1.1e-4 (the FP32
 residual target 1e-4 plus the FP32 operator's rounding against FP64); over
 the three suspensions the network's interval takes fewer outer iterations
 than the fixed one; at phi = 0.45 and 0.5 it takes fewer outer iterations
-than the inner-GMRES form (measured 66 against 81, and 181 against 210;
-the fixed interval took 77, 183 and 94 against the network's 66, 181 and 96).  At phi = 0.55 the boxes relaxed to a minimum gap of 1e-3 make the
-two-hop sets large (G about 130 MB) and the inner-GMRES form needs fewer
-iterations (87 against 96); there it is not compared.  Device times (preconditioner build plus solve,
-second run) are printed: each application of the degree-nine polynomial
-(10 products with G, 9 with A) costs about as much as six inner GMRES steps,
-and the network's forward pass adds a few milliseconds per build, so the wall
-time is close to the inner-GMRES form's at phi = 0.45 and 0.5 and above it at
-phi = 0.55.
+than the inner-GMRES form (measured 66 against 81, and 181 against 210; the
+fixed interval took 77, 183 and 94 against the network's 66, 181 and 96).
+At phi = 0.55 the boxes relaxed to a minimum gap of 1e-3 make the two-hop
+sets large (G about 130 MB) and the inner-GMRES form needs fewer iterations
+(87 against 96); there it is not compared.  Device times (preconditioner
+build plus solve, second run) are printed: each application of the
+degree-nine polynomial (10 products with G, 9 with A) costs about as much as
+six inner GMRES steps, and the network's forward pass adds a few
+milliseconds per build, so the wall time is close to the inner-GMRES form's
+at phi = 0.45 and 0.5 and above it at phi = 0.55.
 """
 from __future__ import annotations
 
